@@ -1,0 +1,330 @@
+"""Benchmark: hash join + high-cardinality group-by + top-k on one B200.
+
+Workload (the join configuration of the benchmark set): build side 15M rows
+(unique int32 keys from a seeded permutation, order_day, segment), probe
+side 60M rows (fk, ship_day, price, discount); build filter segment==1 AND
+order_day<1170, probe filter ship_day>1170, group by build key summing
+price*(100-discount) exactly in int64, top 10 by (sum desc, key asc).
+Synthetic seeded data of the stated shapes; inputs (1.575 GB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+One step = one full query: bitmap semi-join build, exact group-count sizing
+(host read of the distinct counter), probe + hash group-by, top-k.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs an independent replica on its own GPU
+(replicas only: the query does not shard); the timed region is bracketed by
+a barrier, and the slowest rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BUILD_ROWS = 15_000_000
+PROBE_ROWS = 60_000_000
+K_TOP = 10
+SPEC = f"template=join_topk;k={K_TOP}"
+PROBE_BYTES_PER_ROW = 24   # fk i32 + ship_day i32 + price i64 + discount i64
+BUILD_BYTES_PER_ROW = 9    # key i32 + order_day i32 + segment u8
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = []
+        smax = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_info():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def gen_data():
+    from gpudbmetalcodegen_b200 import workloads as W
+    dim = W.gen_dim(BUILD_ROWS, seed=W.SEED)
+    probe = W.gen_probe(PROBE_ROWS, dim_rows=BUILD_ROWS, seed=W.SEED)
+    return dim, probe
+
+
+def run_reference(args):
+    """CPU restatement of the reference's operator semantics (the oracle
+    port: bitmap semi-join, direct-address atomic aggregation, top-k) on all
+    host cores, same workload, rows/s."""
+    from oracle import oracle_py as O
+    dim, probe = gen_data()
+    threads = os.cpu_count() or 1
+    O.join_topk(dim, probe, k=K_TOP, threads=threads)  # warm caches / page in
+    for _ in range(max(0, args.warmup - 1)):
+        O.join_topk(dim, probe, k=K_TOP, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.join_topk(dim, probe, k=K_TOP, threads=threads)
+        times.append(time.perf_counter() - t0)
+    step = statistics.mean(times)
+    rows = BUILD_ROWS + PROBE_ROWS
+    value = rows / step
+    line = {
+        "metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": "join_topk: build 15M + probe 60M rows, top-10", "build_rows": BUILD_ROWS,
+                   "probe_rows": PROBE_ROWS, "k": K_TOP},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                         "sample": f"full workload ({rows} rows) per step, {args.steps} steps"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(dim, probe, budget_s: float = 12.0):
+    from oracle import oracle_py as O
+    threads = os.cpu_count() or 1
+    O.join_topk(dim, probe, k=K_TOP, threads=threads)
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 20):
+        t0 = time.perf_counter()
+        O.join_topk(dim, probe, k=K_TOP, threads=threads)
+        times.append(time.perf_counter() - t0)
+    step = statistics.median(times)
+    return {"value": (BUILD_ROWS + PROBE_ROWS) / step, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"full workload ({BUILD_ROWS + PROBE_ROWS} rows) x {len(times)} runs, median"}
+
+
+def load_traffic():
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("JT_probe_group")
+        except Exception:
+            return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tune", default="")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--build-rows", type=int, default=BUILD_ROWS, help="smaller cases for profiling only")
+    ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS, help="smaller cases for profiling only")
+    args = ap.parse_args()
+    global BUILD_ROWS, PROBE_ROWS
+    BUILD_ROWS, PROBE_ROWS = args.build_rows, args.probe_rows
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_info()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args)
+        return
+
+    import ctypes as C
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from gpudbmetalcodegen_b200 import Context, _lib
+    from oracle import oracle_py as O
+
+    dim, probe = gen_data()
+    ctx = Context(local)
+    ctx.upload_table("dim", dim)
+    ctx.upload_table("probe", probe)
+    q = ctx.prepare(SPEC, args.tune)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    # correctness of this exact configuration
+    res, t = ctx.run(q)
+    expect, groups, distinct = O.join_topk(dim, probe, k=K_TOP)
+    verified = res.rows == expect
+
+    for _ in range(args.warmup):
+        ctx.run(q, collect=False)
+    phase_acc = {}
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            _, t = ctx.run(q, collect=False)
+            launches += t.launches
+            for i, ms in enumerate(t.phase_ms):
+                phase_acc[i] = phase_acc.get(i, 0.0) + ms
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    step_ms = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        tt = torch.tensor([step_ms], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        step_ms = float(tt.item())
+        pg.barrier()
+    rows_total = (BUILD_ROWS + PROBE_ROWS) * world
+    value = rows_total / (step_ms / 1e3)
+
+    # roofline of the dominant kernel (probe + group-by), per launch
+    names = ["JT_build", "JT_probe_group", "JT_topk"]
+    phase_ms = {names[i] if i < len(names) else str(i): v / args.steps for i, v in phase_acc.items()}
+    probe_ms = phase_ms.get("JT_probe_group")
+    peak, peak_kind = peaks()
+    alg_bytes = PROBE_ROWS * PROBE_BYTES_PER_ROW
+    achieved = alg_bytes / (probe_ms / 1e3) / 1e9 if probe_ms else None
+    roofline = {"bound": "hbm", "kernel": "JT_probe_group", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "algorithmic_bytes": alg_bytes, "traffic": load_traffic()}
+
+    # end to end through the C-ABI with pinned host buffers: H2D of every
+    # input column, the query, D2H of the top-k result, per step
+    e2e = None
+    if not args.no_e2e:
+        lib = _lib.load()
+        pinned = {}
+        host_bytes = 0
+        for tname, table in (("dim", dim), ("probe", probe)):
+            for cname, arr in table.items():
+                ptr = lib.gpudb_host_alloc(arr.nbytes)
+                buf = np.ctypeslib.as_array((C.c_uint8 * arr.nbytes).from_address(ptr))
+                buf[:] = arr.view(np.uint8)
+                pinned[(tname, cname)] = (ptr, arr)
+                host_bytes += arr.nbytes
+        def e2e_step():
+            for (tname, cname), (ptr, arr) in pinned.items():
+                _lib.check(lib.gpudb_upload_column(ctx.handle, tname.encode(), cname.encode(), C.c_void_p(ptr),
+                                                   arr.shape[0], arr.itemsize), ctx.handle)
+            r, _ = ctx.run(q, collect=True)
+            return r
+        for _ in range(2):
+            e2e_step()
+        ctx.synchronize()
+        e_steps = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            r = e2e_step()
+        ctx.synchronize()
+        e_ms = (time.perf_counter() - t0) / e_steps * 1e3
+        verified = verified and r.rows == expect
+        if pg:
+            tt = torch.tensor([e_ms], device="cuda")
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            e_ms = float(tt.item())
+        e2e = {"value": rows_total / (e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": host_bytes,
+               "d2h_bytes_per_step": K_TOP * 16 + 8, "ms_per_step": e_ms}
+        for ptr, _ in pinned.values():
+            lib.gpudb_host_free(C.c_void_p(ptr))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dim, probe)
+
+    if rank == 0:
+        line = {
+            "metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+            "config": {"workload": "join_topk: build 15M + probe 60M rows, top-10", "build_rows": BUILD_ROWS,
+                       "probe_rows": PROBE_ROWS, "k": K_TOP, "groups": groups, "build_distinct": distinct,
+                       "l2": "inputs 1.575 GB > 126 MB L2; no flush", "tune": q.tune or "default",
+                       "parallelism": f"replicas x{world}"},
+            "verified": verified,
+            "phase_ms": phase_ms,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

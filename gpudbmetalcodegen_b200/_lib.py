@@ -1,0 +1,164 @@
+"""ctypes bindings for libgpudb.so (include/gpudb_rt.h, gpudb_engine.h, gpudb_datagen.h).
+
+The shared library is built in-tree by ``build_native.build()``. Loading fails
+loudly when it is missing: there is no Python or CPU fallback for any
+operation of the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgpudb.so"
+
+GPUDB_OK = 0
+STATUS_NAMES = {0: "OK", -1: "INVALID", -2: "PLAN", -3: "ALLOC", -4: "LAUNCH", -5: "COMPILE", -6: "CUDA",
+                -7: "DEVICE", -8: "NOGPU"}
+DEVERR_HASH_OVERFLOW = 0x1
+DEVERR_WAIT_TIMEOUT = 0x2
+DEVERR_BOUNDS = 0x4
+DEVERR_SENTINEL_KEY = 0x8
+DEVERR_CAPACITY = 0x10
+
+PARAM_TABLE_DATA, PARAM_TABLE_SIZE, PARAM_DEVICE_BUFFER, PARAM_CONSTANT_SCALAR, PARAM_CONSTANT_DATA, \
+    PARAM_ERROR_WORD, PARAM_BUFFER_LENGTH = range(7)
+COL_INT, COL_DOUBLE, COL_STRING = 0, 1, 2
+MAX_PHASES = 32
+
+
+class BindingDesc(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("kind", C.c_int), ("elem_type", C.c_char_p), ("table", C.c_char_p),
+                ("size_expr", C.c_char_p), ("zero_init", C.c_int), ("fill_byte", C.c_int), ("read_only", C.c_int)]
+
+
+class PhaseDesc(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("scanned_table", C.c_char_p), ("block_size", C.c_int),
+                ("max_blocks", C.c_int), ("single_thread", C.c_int), ("dynamic_smem_bytes", C.c_int),
+                ("tile_rows", C.c_int), ("rows_per_thread", C.c_int), ("bindings", C.POINTER(BindingDesc)),
+                ("nbindings", C.c_int)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("nphases", C.c_int), ("phase_ms", C.c_double * MAX_PHASES),
+                ("phase_grid", C.c_int * MAX_PHASES), ("phase_block", C.c_int * MAX_PHASES),
+                ("device_error", C.c_uint), ("launches", C.c_longlong), ("alloc_ms", C.c_double),
+                ("plan_ms", C.c_double), ("codegen_ms", C.c_double), ("compile_ms", C.c_double),
+                ("collect_ms", C.c_double)]
+
+
+# (name, restype, argtypes) for every exported entry point.
+_SIGNATURES = [
+    # gpudb_rt.h
+    ("gpudb_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("gpudb_destroy", None, [C.c_void_p]),
+    ("gpudb_last_error", C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("gpudb_stream", C.c_void_p, [C.c_void_p]),
+    ("gpudb_device_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("gpudb_synchronize", C.c_int, [C.c_void_p]),
+    ("gpudb_compile", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_void_p)]),
+    ("gpudb_module_free", None, [C.c_void_p]),
+    ("gpudb_compile_check", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_double)]),
+    ("gpudb_set_fast_math", None, [C.c_int]),
+    ("gpudb_set_kernel_cache_dir", None, [C.c_char_p]),
+    ("gpudb_register_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
+    ("gpudb_upload_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
+    ("gpudb_register_rows", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
+    ("gpudb_register_buffer", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
+    ("gpudb_register_symbol", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
+    ("gpudb_get_symbol", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_uint64)]),
+    ("gpudb_register_scalar_i64", C.c_int, [C.c_void_p, C.c_char_p, C.c_longlong]),
+    ("gpudb_register_scalar_f64", C.c_int, [C.c_void_p, C.c_char_p, C.c_double]),
+    ("gpudb_execute", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PhaseDesc), C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_int, C.POINTER(Timing)]),
+    ("gpudb_set_skip_zero_init", C.c_int, [C.c_void_p, C.c_int]),
+    ("gpudb_set_use_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("gpudb_read_buffer", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64]),
+    ("gpudb_buffer_ptr", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    ("gpudb_release_buffers", C.c_int, [C.c_void_p]),
+    ("gpudb_host_alloc", C.c_void_p, [C.c_uint64]),
+    ("gpudb_host_free", None, [C.c_void_p]),
+    # gpudb_engine.h
+    ("gpudb_query_prepare", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("gpudb_query_free", None, [C.c_void_p]),
+    ("gpudb_query_source", C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("gpudb_query_describe", C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("gpudb_query_compile_log", C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("gpudb_query_algorithmic_bytes", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("gpudb_query_run", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p),
+                                  C.POINTER(Timing)]),
+    ("gpudb_result_shape", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    ("gpudb_result_column", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_int)]),
+    ("gpudb_result_get_int", C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64)]),
+    ("gpudb_result_get_f64", C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_double)]),
+    ("gpudb_result_get_str", C.c_size_t, [C.c_void_p, C.c_longlong, C.c_int, C.c_char_p, C.c_size_t]),
+    ("gpudb_result_export_i64", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]),
+    ("gpudb_result_canonical", C.c_size_t, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
+    ("gpudb_result_free", None, [C.c_void_p]),
+    ("gpudb_compare_canonical", C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_char_p,
+                                          C.c_size_t]),
+    ("gpudb_register_max_key", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_longlong)]),
+    ("gpudb_list_templates", C.c_size_t, [C.c_char_p, C.c_size_t]),
+    ("gpudb_version", C.c_char_p, []),
+    # gpudb_datagen.h
+    ("gpudb_gen_fact", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 7 + [C.c_int]),
+    ("gpudb_gen_dim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 3 + [C.c_int]),
+    ("gpudb_gen_probe", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 4 + [C.c_int]),
+    ("gpudb_gen_order_day", C.c_int32, [C.c_uint64, C.c_int64]),
+    ("gpudb_gen_zbuild", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_zprobe", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_void_p,
+                                   C.c_void_p, C.c_int]),
+    ("gpudb_gen_zkey", C.c_int64, [C.c_uint64, C.c_uint64]),
+    ("gpudb_gen_mix", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
+     + [C.c_void_p] * 5 + [C.c_int]),
+    ("gpudb_gen_mixdim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+]
+
+EXPORTED = [s[0] for s in _SIGNATURES]
+
+_lib = None
+
+
+class GpudbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"gpudb {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def load() -> C.CDLL:
+    """Load libgpudb.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run gpudbmetalcodegen_b200.build_native.build() "
+                           "(there is no fallback implementation)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
+    for name, res, args in _SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error(ctx) -> str:
+    lib = load()
+    n = lib.gpudb_last_error(ctx, None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib.gpudb_last_error(ctx, buf, n + 1)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, ctx=None) -> None:
+    if status != GPUDB_OK:
+        raise GpudbError(status, last_error(ctx))
+
+
+def get_string(fn, *args) -> str:
+    n = fn(*args, None, 0)
+    buf = C.create_string_buffer(n + 1)
+    fn(*args, buf, n + 1)
+    return buf.value.decode(errors="replace")

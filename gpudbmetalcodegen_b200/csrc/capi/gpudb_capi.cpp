@@ -1,0 +1,467 @@
+// C-ABI of libgpudb.so: include/gpudb_rt.h and include/gpudb_engine.h.
+// Every entry point catches C++ exceptions and turns them into a status +
+// context error text; nothing C++ crosses the boundary.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../../include/gpudb_engine.h"
+#include "../../../include/gpudb_rt.h"
+#include "../execution/query_engine.h"
+
+struct gpudb_ctx {
+    std::unique_ptr<gpudb::QueryContext> qc;
+    std::string lastError;
+};
+struct gpudb_module {
+    std::shared_ptr<gpudb::RuntimeCompiler::CompiledQuery> cq;
+};
+struct gpudb_query {
+    std::shared_ptr<gpudb::PreparedQuery> q;
+};
+struct gpudb_result {
+    gpudb::GenericResult r;
+};
+
+namespace {
+
+thread_local std::string tlCreateError;
+
+size_t copyOut(const std::string& s, char* buf, size_t cap) {
+    if (buf && cap) {
+        const size_t n = s.size() < cap - 1 ? s.size() : cap - 1;
+        std::memcpy(buf, s.data(), n);
+        buf[n] = '\0';
+    }
+    return s.size();
+}
+
+int fail(gpudb_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->lastError = msg;
+    else tlCreateError = msg;
+    return code;
+}
+
+int mapStatus(int rc) {
+    switch (rc) {
+        case 0: return GPUDB_OK;
+        case -2: return GPUDB_E_PLAN;
+        case -3: return GPUDB_E_ALLOC;
+        case -4: return GPUDB_E_LAUNCH;
+        case -5: return GPUDB_E_CUDA;
+        case -6: return GPUDB_E_LAUNCH;
+        case -7: return GPUDB_E_DEVICE;
+        default: return GPUDB_E_CUDA;
+    }
+}
+
+void fillTiming(const gpudb::ExecutionResult& r, gpudb_timing* t) {
+    if (!t) return;
+    std::memset(t, 0, sizeof *t);
+    t->total_ms = r.totalKernelTimeMs;
+    t->nphases = (int)std::min<size_t>(r.phaseNames.size(), GPUDB_MAX_PHASES);
+    for (int i = 0; i < t->nphases; i++) {
+        t->phase_ms[i] = r.phaseTimesMs[i];
+        t->phase_grid[i] = r.phaseGrid[i];
+        t->phase_block[i] = r.phaseBlock[i];
+    }
+    t->device_error = r.deviceError;
+    t->launches = r.launches;
+    t->alloc_ms = r.bufferAllocTimeMs;
+    t->plan_ms = r.planTimeMs;
+    t->codegen_ms = r.codegenTimeMs;
+    t->compile_ms = r.compileTimeMs;
+    t->collect_ms = r.collectTimeMs;
+}
+
+#define GPUDB_GUARD(ctx, ...)                                    \
+    try {                                                        \
+        __VA_ARGS__                                              \
+    } catch (const std::exception& e) {                          \
+        return fail(ctx, GPUDB_E_INVALID, e.what());             \
+    } catch (...) {                                              \
+        return fail(ctx, GPUDB_E_INVALID, "unknown C++ exception"); \
+    }
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+int gpudb_create(int device, gpudb_ctx** out) {
+    if (!out) return fail(nullptr, GPUDB_E_INVALID, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(nullptr, GPUDB_E_NOGPU, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return fail(nullptr, GPUDB_E_INVALID, "device index out of range");
+    try {
+        auto c = std::make_unique<gpudb_ctx>();
+        c->qc = std::make_unique<gpudb::QueryContext>(device);
+        *out = c.release();
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(nullptr, GPUDB_E_CUDA, e.what());
+    }
+}
+
+void gpudb_destroy(gpudb_ctx* ctx) { delete ctx; }
+
+size_t gpudb_last_error(gpudb_ctx* ctx, char* buf, size_t cap) {
+    return copyOut(ctx ? ctx->lastError : tlCreateError, buf, cap);
+}
+
+void* gpudb_stream(gpudb_ctx* ctx) { return ctx ? (void*)ctx->qc->ex.stream() : nullptr; }
+
+int gpudb_device_info(gpudb_ctx* ctx, int* num_sms, int* cc_major, int* cc_minor) {
+    if (!ctx) return GPUDB_E_INVALID;
+    const int d = ctx->qc->ex.device();
+    if (num_sms) *num_sms = ctx->qc->ex.numSMs();
+    if (cc_major) cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, d);
+    if (cc_minor) cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, d);
+    return GPUDB_OK;
+}
+
+int gpudb_synchronize(gpudb_ctx* ctx) {
+    if (!ctx) return GPUDB_E_INVALID;
+    const cudaError_t e = cudaStreamSynchronize(ctx->qc->ex.stream());
+    return e == cudaSuccess ? GPUDB_OK : fail(ctx, GPUDB_E_CUDA, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// compile
+// ---------------------------------------------------------------------------
+int gpudb_compile(gpudb_ctx* ctx, const char* src, const char* const* kernels, int nkernels, gpudb_module** out) {
+    if (!ctx || !src || !out || (nkernels > 0 && !kernels)) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        std::vector<std::string> names;
+        for (int i = 0; i < nkernels; i++) names.push_back(kernels[i]);
+        std::string err;
+        cudaSetDevice(ctx->qc->ex.device());
+        auto cq = gpudb::RuntimeCompiler::compileAndLoad(src, names, err);
+        if (!cq) return fail(ctx, GPUDB_E_COMPILE, err);
+        *out = new gpudb_module{cq};
+        return GPUDB_OK;
+    })
+}
+
+void gpudb_module_free(gpudb_module* m) { delete m; }
+
+int gpudb_compile_check(const char* src, char* log, size_t cap, double* compile_ms) {
+    if (!src) return GPUDB_E_INVALID;
+    try {
+        gpudb::CubinArtifact art;
+        std::string err;
+        const bool ok = gpudb::RuntimeCompiler::compileToCubin(src, art, err);
+        copyOut(ok ? art.log : err, log, cap);
+        if (compile_ms) *compile_ms = art.compileMs;
+        return ok ? GPUDB_OK : GPUDB_E_COMPILE;
+    } catch (const std::exception& e) {
+        copyOut(e.what(), log, cap);
+        return GPUDB_E_COMPILE;
+    }
+}
+
+void gpudb_set_fast_math(int on) { gpudb::RuntimeCompiler::setFastMathEnabled(on != 0); }
+void gpudb_set_kernel_cache_dir(const char* dir) { gpudb::RuntimeCompiler::setCacheDir(dir ? dir : ""); }
+
+// ---------------------------------------------------------------------------
+// registration
+// ---------------------------------------------------------------------------
+int gpudb_register_column(gpudb_ctx* ctx, const char* table, const char* column, const void* dptr, uint64_t rows,
+                          int elem_bytes) {
+    if (!ctx || !table || !column || (!dptr && rows) || elem_bytes <= 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        ctx->qc->ex.registerTableBuffer(column, dptr, rows, (size_t)elem_bytes);
+        ctx->qc->ex.registerTableRowCount(table, rows);
+        return GPUDB_OK;
+    })
+}
+
+int gpudb_upload_column(gpudb_ctx* ctx, const char* table, const char* column, const void* host, uint64_t rows,
+                        int elem_bytes) {
+    if (!ctx || !table || !column || (!host && rows) || elem_bytes <= 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    try {
+        ctx->qc->ex.uploadColumn(column, table, host, rows, (size_t)elem_bytes);
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, GPUDB_E_ALLOC, e.what());
+    }
+}
+
+int gpudb_register_rows(gpudb_ctx* ctx, const char* table, uint64_t rows) {
+    if (!ctx || !table) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    ctx->qc->ex.registerTableRowCount(table, rows);
+    return GPUDB_OK;
+}
+
+int gpudb_register_buffer(gpudb_ctx* ctx, const char* name, void* dptr, uint64_t bytes, int elem_bytes) {
+    if (!ctx || !name || !dptr) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    ctx->qc->ex.registerAllocatedBuffer(name, dptr, bytes, elem_bytes > 0 ? (size_t)elem_bytes : 1);
+    return GPUDB_OK;
+}
+
+int gpudb_register_symbol(gpudb_ctx* ctx, const char* name, uint64_t value) {
+    if (!ctx || !name) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    ctx->qc->ex.registerSymbol(name, value);
+    return GPUDB_OK;
+}
+
+int gpudb_get_symbol(gpudb_ctx* ctx, const char* name, uint64_t* value) {
+    if (!ctx || !name || !value) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    return ctx->qc->ex.tryGetSymbol(name, *value) ? GPUDB_OK
+                                                  : fail(ctx, GPUDB_E_INVALID, std::string("unknown symbol ") + name);
+}
+
+int gpudb_register_scalar_i64(gpudb_ctx* ctx, const char* name, long long value) {
+    if (!ctx || !name) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    ctx->qc->ex.registerScalarInt(name, value);
+    return GPUDB_OK;
+}
+
+int gpudb_register_scalar_f64(gpudb_ctx* ctx, const char* name, double value) {
+    if (!ctx || !name) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    ctx->qc->ex.registerScalarFloat(name, value);
+    return GPUDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// execute
+// ---------------------------------------------------------------------------
+int gpudb_execute(gpudb_ctx* ctx, gpudb_module* m, const gpudb_phase_desc* phases, int nphases, int first, int last,
+                  int warmup, int measured, gpudb_timing* timing) {
+    if (!ctx || !m || !phases || nphases <= 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        std::vector<gpudb::CudaCodegen::PhaseInfo> ph(nphases);
+        for (int i = 0; i < nphases; i++) {
+            const auto& d = phases[i];
+            auto& p = ph[i];
+            if (!d.name) return fail(ctx, GPUDB_E_INVALID, "phase without a name");
+            p.name = d.name;
+            p.scannedTable = d.scanned_table ? d.scanned_table : "";
+            p.threadgroupSize = d.block_size > 0 ? d.block_size : 256;
+            p.maxThreadgroups = d.max_blocks;
+            p.isSingleThread = d.single_thread != 0;
+            p.dynamicSmemBytes = d.dynamic_smem_bytes;
+            p.tileRows = d.tile_rows;
+            p.rowsPerThread = d.rows_per_thread > 0 ? d.rows_per_thread : 1;
+            for (int k = 0; k < d.nbindings; k++) {
+                const auto& bd = d.bindings[k];
+                if (!bd.name || bd.kind < 0 || bd.kind > GPUDB_PARAM_BUFFER_LENGTH)
+                    return fail(ctx, GPUDB_E_INVALID, "bad binding in phase " + p.name);
+                gpudb::CudaParamBinding b;
+                b.name = bd.name;
+                b.kind = (gpudb::CudaParamKind)bd.kind;
+                b.elementType = bd.elem_type ? bd.elem_type : "unsigned";
+                b.tableName = bd.table ? bd.table : "";
+                b.sizeExpr = bd.size_expr ? bd.size_expr : "";
+                b.zeroInit = bd.zero_init != 0;
+                b.fillByte = bd.fill_byte;
+                b.readOnly = bd.read_only != 0;
+                b.argIndex = k;
+                p.bindings.push_back(b);
+            }
+        }
+        gpudb::ExecutionResult r;
+        std::string err;
+        const int rc = ctx->qc->ex.execute(*m->cq, ph, warmup, measured, first, last, r, err);
+        fillTiming(r, timing);
+        if (rc != 0) return fail(ctx, mapStatus(rc), err);
+        if (r.deviceError) return fail(ctx, GPUDB_E_DEVICE, "device error word set");
+        return GPUDB_OK;
+    })
+}
+
+int gpudb_set_skip_zero_init(gpudb_ctx* ctx, int skip) {
+    if (!ctx) return GPUDB_E_INVALID;
+    ctx->qc->ex.setSkipZeroInit(skip != 0);
+    return GPUDB_OK;
+}
+
+int gpudb_set_use_graphs(gpudb_ctx* ctx, int on) {
+    if (!ctx) return GPUDB_E_INVALID;
+    ctx->qc->ex.setUseGraphs(on != 0);
+    return GPUDB_OK;
+}
+
+int gpudb_read_buffer(gpudb_ctx* ctx, const char* name, void* host, uint64_t bytes) {
+    if (!ctx || !name || (!host && bytes)) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    return ctx->qc->ex.readBuffer(name, host, bytes) ? GPUDB_OK
+                                                     : fail(ctx, GPUDB_E_INVALID, std::string("cannot read buffer ") + name);
+}
+
+int gpudb_buffer_ptr(gpudb_ctx* ctx, const char* name, void** dptr, uint64_t* bytes) {
+    if (!ctx || !name || !dptr) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    size_t b = 0;
+    *dptr = ctx->qc->ex.bufferPtr(name, &b);
+    if (bytes) *bytes = b;
+    return *dptr ? GPUDB_OK : fail(ctx, GPUDB_E_INVALID, std::string("unknown buffer ") + name);
+}
+
+int gpudb_release_buffers(gpudb_ctx* ctx) {
+    if (!ctx) return GPUDB_E_INVALID;
+    ctx->qc->ex.releaseAllocatedBuffers();
+    return GPUDB_OK;
+}
+
+void* gpudb_host_alloc(uint64_t bytes) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void gpudb_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
+// ---------------------------------------------------------------------------
+// queries
+// ---------------------------------------------------------------------------
+int gpudb_query_prepare(gpudb_ctx* ctx, const char* spec, const char* tune, gpudb_query** out) {
+    if (!spec || !out) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    *out = nullptr;
+    try {
+        if (ctx) cudaSetDevice(ctx->qc->ex.device());
+        auto q = gpudb::prepareQuery(spec, tune ? tune : "", true, ctx != nullptr);
+        *out = new gpudb_query{q};
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        const bool compile = m.find("NVRTC") != std::string::npos || m.find("cuModule") != std::string::npos;
+        return fail(ctx, compile ? GPUDB_E_COMPILE : GPUDB_E_PLAN, m);
+    }
+}
+
+void gpudb_query_free(gpudb_query* q) { delete q; }
+
+size_t gpudb_query_source(gpudb_query* q, char* buf, size_t cap) { return q ? copyOut(q->q->source, buf, cap) : 0; }
+size_t gpudb_query_describe(gpudb_query* q, char* buf, size_t cap) { return q ? copyOut(q->q->describe, buf, cap) : 0; }
+size_t gpudb_query_compile_log(gpudb_query* q, char* buf, size_t cap) {
+    return q ? copyOut(q->q->compileLog, buf, cap) : 0;
+}
+
+int gpudb_query_algorithmic_bytes(gpudb_ctx* ctx, gpudb_query* q, long long* bytes) {
+    if (!ctx || !q || !bytes) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        std::map<std::string, long long> rows;
+        for (const auto& t : q->q->plan.tables) rows[t] = (long long)ctx->qc->ex.tableRows(t);
+        *bytes = gpudb::planAlgorithmicBytes(q->q->plan, rows);
+        return GPUDB_OK;
+    })
+}
+
+int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gpudb_result** result,
+                    gpudb_timing* timing) {
+    if (!ctx || !q) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    if (result) *result = nullptr;
+    GPUDB_GUARD(ctx, {
+        cudaSetDevice(ctx->qc->ex.device());
+        gpudb::ExecutionResult r;
+        std::string err;
+        ctx->qc->ex.setSkipZeroInit(false);
+        const int rc = gpudb::runQuery(*ctx->qc, *q->q, warmup, measured, result != nullptr, r, err);
+        fillTiming(r, timing);
+        if (rc != 0) return fail(ctx, mapStatus(rc), err);
+        if (result) *result = new gpudb_result{std::move(r.result)};
+        return GPUDB_OK;
+    })
+}
+
+// ---------------------------------------------------------------------------
+// results
+// ---------------------------------------------------------------------------
+int gpudb_result_shape(gpudb_result* r, int* ncols, long long* nrows) {
+    if (!r) return GPUDB_E_INVALID;
+    if (ncols) *ncols = (int)r->r.columns.size();
+    if (nrows) *nrows = (long long)r->r.rows.size();
+    return GPUDB_OK;
+}
+
+int gpudb_result_column(gpudb_result* r, int col, char* name, size_t cap, int* type) {
+    if (!r || col < 0 || col >= (int)r->r.columns.size()) return GPUDB_E_INVALID;
+    copyOut(r->r.columns[col].name, name, cap);
+    if (type) {
+        const auto& t = r->r.columns[col].type;
+        *type = t == "int" ? GPUDB_COL_INT : t == "double" ? GPUDB_COL_DOUBLE : GPUDB_COL_STRING;
+    }
+    return GPUDB_OK;
+}
+
+int gpudb_result_get_int(gpudb_result* r, long long row, int col, int64_t* lo, int64_t* hi) {
+    if (!r || row < 0 || row >= (long long)r->r.rows.size() || col < 0 || col >= (int)r->r.rows[row].size())
+        return GPUDB_E_INVALID;
+    const auto* v = std::get_if<gpudb::int128>(&r->r.rows[row][col]);
+    if (!v) return GPUDB_E_INVALID;
+    if (lo) *lo = (int64_t)(unsigned long long)(*v);
+    if (hi) *hi = (int64_t)(*v >> 64);
+    return GPUDB_OK;
+}
+
+int gpudb_result_get_f64(gpudb_result* r, long long row, int col, double* out) {
+    if (!r || row < 0 || row >= (long long)r->r.rows.size() || col < 0 || col >= (int)r->r.rows[row].size())
+        return GPUDB_E_INVALID;
+    const auto* v = std::get_if<double>(&r->r.rows[row][col]);
+    if (!v) return GPUDB_E_INVALID;
+    if (out) *out = *v;
+    return GPUDB_OK;
+}
+
+size_t gpudb_result_get_str(gpudb_result* r, long long row, int col, char* buf, size_t cap) {
+    if (!r || row < 0 || row >= (long long)r->r.rows.size() || col < 0 || col >= (int)r->r.rows[row].size()) return 0;
+    const auto* v = std::get_if<std::string>(&r->r.rows[row][col]);
+    return v ? copyOut(*v, buf, cap) : 0;
+}
+
+int gpudb_result_export_i64(gpudb_result* r, int col, int64_t* out, long long n) {
+    if (!r || !out || col < 0 || col >= (int)r->r.columns.size() || n < (long long)r->r.rows.size())
+        return GPUDB_E_INVALID;
+    for (size_t i = 0; i < r->r.rows.size(); i++) {
+        const auto* v = std::get_if<gpudb::int128>(&r->r.rows[i][col]);
+        if (!v || *v > (gpudb::int128)INT64_MAX || *v < (gpudb::int128)INT64_MIN) return GPUDB_E_INVALID;
+        out[i] = (int64_t)*v;
+    }
+    return GPUDB_OK;
+}
+
+size_t gpudb_result_canonical(gpudb_result* r, int exact, char* buf, size_t cap) {
+    if (!r) return 0;
+    return copyOut(exact ? r->r.toExact() : r->r.toCanonical(), buf, cap);
+}
+
+void gpudb_result_free(gpudb_result* r) { delete r; }
+
+int gpudb_compare_canonical(const char* got, const char* expected, double abs_tol, double rel_tol, char* buf,
+                            size_t cap) {
+    if (!got || !expected) return 0;
+    const std::string why = gpudb::compareCanonical(got, expected, abs_tol, rel_tol);
+    copyOut(why, buf, cap);
+    return why.empty() ? 1 : 0;
+}
+
+int gpudb_register_max_key(gpudb_ctx* ctx, const char* column, long long* max_out) {
+    if (!ctx || !column) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        const long long m = gpudb::registerMaxKey(*ctx->qc, column);
+        if (max_out) *max_out = m;
+        return GPUDB_OK;
+    })
+}
+
+size_t gpudb_list_templates(char* buf, size_t cap) {
+    std::string s;
+    for (const auto& t : gpudb::planTemplates()) s += (s.empty() ? "" : ",") + t;
+    return copyOut(s, buf, cap);
+}
+
+const char* gpudb_version(void) { return "gpudb-b200 0.1 (sm_100a, NVRTC)"; }
+
+}  // extern "C"

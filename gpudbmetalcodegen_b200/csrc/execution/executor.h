@@ -1,0 +1,148 @@
+#pragma once
+// ===================================================================
+// CudaGenericExecutor — data-driven launch of generated phases.
+//
+// Replaces the reference's MetalGenericExecutor
+// (codegen/execution/metal_generic_executor.h:46-164) with the same
+// responsibilities and lifetimes: register non-owned columns / row counts /
+// buffers / symbols / scalars, allocate phase buffers from symbolic sizes,
+// zero/0xFF-fill them every iteration (unless skip-zero-init), launch the
+// phases in order, time them, and hand buffers to the collector.
+// B200 design:
+//   * one CUDA stream per executor; all fills and launches are
+//     stream-ordered, the host synchronises once per execute();
+//   * per-phase CUDA events (the reference's GPU timestamps);
+//   * launch = min(work, SMs x occupancy) persistent CTAs, with the
+//     dynamic shared memory each phase declares (TMA ring, smem tables);
+//   * the device error word is cleared before and read after each run;
+//   * optional CUDA-graph replay of a whole iteration (fills + kernels).
+// ===================================================================
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../core/cuda_codegen.h"
+#include "result_collector.h"
+#include "runtime_compiler.h"
+
+namespace gpudb {
+
+struct ExecutionResult {
+    GenericResult result;
+    double totalKernelTimeMs = 0.0;        // device time of one iteration (fills + kernels), mean over measured
+    std::vector<double> phaseTimesMs;      // per phase, mean over measured iterations
+    std::vector<std::string> phaseNames;
+    std::vector<int> phaseGrid, phaseBlock, phaseSmem;
+    unsigned deviceError = 0;              // OR of GPUDB_ERR_* bits seen
+    long long launches = 0;                // kernels launched per iteration
+    double bufferAllocTimeMs = 0.0;
+    // filled by the query driver
+    double planTimeMs = 0.0, codegenTimeMs = 0.0, compileTimeMs = 0.0, collectTimeMs = 0.0;
+};
+
+class CudaGenericExecutor {
+public:
+    explicit CudaGenericExecutor(int device);
+    ~CudaGenericExecutor();
+    CudaGenericExecutor(const CudaGenericExecutor&) = delete;
+    CudaGenericExecutor& operator=(const CudaGenericExecutor&) = delete;
+
+    // --- registration (non-owning) ---------------------------------------
+    void registerTableBuffer(const std::string& column, const void* dptr, size_t rows, size_t elemBytes);
+    void registerTableRowCount(const std::string& table, size_t rows);
+    void registerAllocatedBuffer(const std::string& name, void* dptr, size_t bytes, size_t elemBytes = 1);
+    void registerSymbol(const std::string& name, uint64_t value);
+    bool tryGetSymbol(const std::string& name, uint64_t& out) const;
+    void registerScalarInt(const std::string& name, long long value);
+    void registerScalarFloat(const std::string& name, double value);
+    CudaSizeResolver& sizeResolver() { return resolver_; }
+
+    // Owned column: copy `rows*elemBytes` host bytes into an executor-owned
+    // device buffer (reused across calls when large enough) on the stream.
+    void uploadColumn(const std::string& column, const std::string& table, const void* host, size_t rows,
+                      size_t elemBytes);
+
+    // --- execution -----------------------------------------------------------
+    // Run phases [first, last) (last < 0 = all) `warmup` + `measured` times.
+    // Returns 0, or a negative status with `error` filled.
+    int execute(const RuntimeCompiler::CompiledQuery& cq, const std::vector<CudaCodegen::PhaseInfo>& phases,
+                int warmup, int measured, int first, int last, ExecutionResult& out, std::string& error);
+
+    void setSkipZeroInit(bool skip) { skipZeroInit_ = skip; }
+    void setUseGraphs(bool on) { useGraphs_ = on; }
+
+    // --- buffers -------------------------------------------------------------
+    bool readBuffer(const std::string& name, void* host, size_t bytes);
+    void* bufferPtr(const std::string& name, size_t* bytes = nullptr) const;
+    void releaseAllocatedBuffers();
+    GenericResult collectResult(const CudaResultSchema& schema);
+
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
+    int numSMs() const { return numSMs_; }
+    size_t tableRows(const std::string& table) const;
+    const void* columnPtr(const std::string& column, size_t* rows = nullptr) const;
+    // Bumped on every (re)registration or upload of the column; caches of
+    // column-derived values (max-key symbols) compare it.
+    uint64_t columnGeneration(const std::string& column) const;
+
+private:
+    struct Buffer {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+        size_t elemBytes = 1;
+        bool owned = false;
+    };
+    struct Column {
+        const void* ptr = nullptr;
+        size_t rows = 0;
+        size_t elemBytes = 0;
+        uint64_t generation = 0;
+    };
+    uint64_t generationCounter_ = 0;
+    struct Launch {
+        CUfunction fn;
+        unsigned grid, block, smem;
+        std::vector<uint64_t> slots;
+        std::string name;
+    };
+    struct Fill {
+        void* ptr;
+        size_t bytes;
+        int value;
+    };
+
+    int device_ = 0;
+    int numSMs_ = 148;
+    cudaStream_t stream_ = nullptr;
+    unsigned* errWord_ = nullptr;
+    unsigned* errHost_ = nullptr;
+    bool skipZeroInit_ = false;
+    bool useGraphs_ = false;
+    CudaSizeResolver resolver_;
+    std::unordered_map<std::string, Column> columns_;
+    std::unordered_map<std::string, size_t> tableRows_;
+    std::unordered_map<std::string, Buffer> buffers_;
+    std::unordered_map<std::string, Buffer> ownedColumns_;
+    std::unordered_map<std::string, long long> scalarInts_;
+    std::unordered_map<std::string, double> scalarFloats_;
+    std::map<CUfunction, int> smemConfigured_;
+    std::vector<cudaEvent_t> events_;
+    struct GraphEntry {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::map<std::string, GraphEntry> graphs_;
+
+    void ensureEvents(size_t n);
+    bool allocateBuffers(const CudaCodegen::PhaseInfo& phase, std::string& error);
+    bool buildLaunch(const RuntimeCompiler::CompiledQuery& cq, const CudaCodegen::PhaseInfo& phase, Launch& l,
+                     std::string& error);
+    void clearGraphs();
+};
+
+}  // namespace gpudb

@@ -1,0 +1,956 @@
+#include "cuda_operators.h"
+
+#include <sstream>
+#include <stdexcept>
+
+namespace gpudb {
+
+namespace {
+
+std::string S(long long v) { return std::to_string(v); }
+
+// Key type -> (unsigned storage type, insert fn, find fn, empty literal).
+struct KeyOps {
+    std::string store, ins, find, empty, cast;
+};
+KeyOps keyOps(const std::string& keyType, HashLayout layout) {
+    if (keyType == "int" || keyType == "unsigned") {
+        if (layout == HashLayout::Bucket8)
+            throw std::runtime_error("Bucket8 hash layout needs 64-bit keys");
+        return {"unsigned", "gpudb_ht_insert32", "gpudb_ht_find32", "GPUDB_EMPTY32", "(unsigned)"};
+    }
+    if (keyType == "long long" || keyType == "unsigned long long") {
+        if (layout == HashLayout::Bucket8)
+            return {"unsigned long long", "gpudb_htb_insert64", "gpudb_htb_find64", "GPUDB_EMPTY64",
+                    "(unsigned long long)"};
+        return {"unsigned long long", "gpudb_ht_insert64", "gpudb_ht_find64", "GPUDB_EMPTY64",
+                "(unsigned long long)"};
+    }
+    throw std::runtime_error("hash key type must be int or long long, got '" + keyType + "'");
+}
+
+// Bucket8 probes count buckets of 8 slots; keep the same slot budget.
+int probeArg(HashLayout layout, int maxProbe) {
+    return layout == HashLayout::Bucket8 ? (maxProbe + 7) / 8 : maxProbe;
+}
+
+}  // namespace
+
+std::string hashSlotsExpr(const std::string& capacityExpr) { return "pow2ceil(max(" + capacityExpr + ", 16))"; }
+std::string hashLog2Expr(const std::string& capacityExpr) { return "log2ceil(max(" + capacityExpr + ", 16))"; }
+
+std::string CudaUnaryOperator::describeChain() const { return child_ ? child_->describe() : ""; }
+
+// ===================================================================
+// CudaGridStrideScan
+// ===================================================================
+CudaGridStrideScan::CudaGridStrideScan(const std::string& table, const std::string& rowVar,
+                                       const std::string& idxVar)
+    : tableName_(table), rowVar_(rowVar), idxVar_(idxVar) {}
+
+void CudaGridStrideScan::addColumn(const std::string& paramName, const std::string& cudaType) {
+    for (const auto& c : columns_)
+        if (c.paramName == paramName) return;
+    columns_.push_back({paramName, cudaType});
+}
+
+void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.setPhaseScannedTable(tableName_);
+    if (columns_.empty())
+        throw std::runtime_error("CudaGridStrideScan(" + tableName_ + "): no columns registered; call addColumn()");
+    for (const auto& c : columns_) cg.addColumnParam(c.paramName, c.cudaType, tableName_);
+    cg.addTableSizeParam(tableName_);
+    const std::string n = tableSizeName(tableName_);
+    const std::string& i = idxVar_;
+
+    if (cfg_.mode == ScanConfig::Direct) {
+        cg.addComment("grid-stride scan of " + tableName_ + " (direct coalesced loads)");
+        cg.addBlock("for (long long " + i + " = tid; " + i + " < " + n + "; " + i + " += tpg)", [&]() {
+            cg.addLine("const long long _row = " + i + "; (void)_row;");
+            consume();
+        });
+        return;
+    }
+
+    // ---- TMA bulk staged tile loop ------------------------------------
+    const int bs = cg.currentThreadgroupSize();
+    const int tile = cfg_.tileRows;
+    const int stages = cfg_.stages;
+    if (tile <= 0 || tile % 16 != 0 || tile % bs != 0)
+        throw std::runtime_error("CudaGridStrideScan: tileRows must be a positive multiple of 16 and of the block size");
+    if (stages < 1 || stages > 8) throw std::runtime_error("CudaGridStrideScan: stages must be in [1,8]");
+    std::vector<long long> off;
+    long long stageBytes = 0, txBytes = 0;
+    for (const auto& c : columns_) {
+        const long long w = (long long)cudaTypeBytes(c.cudaType);
+        off.push_back(stageBytes);
+        stageBytes += ((long long)tile * w + 127) / 128 * 128;
+        txBytes += (long long)tile * w;
+    }
+    if (txBytes >= (1 << 20)) throw std::runtime_error("CudaGridStrideScan: tile too large for one mbarrier transaction");
+    const int barOff = cg.allocDynamicSmem(128);
+    const int ringOff = cg.allocDynamicSmem((int)(stageBytes * stages));
+    cg.setPhaseTileRows(tile);
+
+    const std::string SB = S(stageBytes);
+    cg.addComment("TMA-bulk staged scan of " + tableName_ + ": " + S(tile) + "-row tiles, " + S(stages) +
+                  "-stage cp.async.bulk ring, " + S(txBytes) + " B per tile");
+    cg.addBlock("", [&]() {
+        cg.addLine("unsigned long long* _sb_bar = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(barOff) +
+                   ");");
+        cg.addLine("unsigned char* _sb_ring = gpudb_smem + " + S(ringOff) + ";");
+        cg.addLine("const long long _sb_n = " + n + ";");
+        std::string alignExpr;
+        for (size_t k = 0; k < columns_.size(); k++)
+            alignExpr += (k ? " | " : "") + std::string("(unsigned long long)") + columns_[k].paramName;
+        cg.addLine("const bool _sb_aligned = ((" + alignExpr + ") & 15ull) == 0ull;");
+        cg.addLine("const long long _sb_ntiles = _sb_aligned ? (_sb_n / " + S(tile) + "ll) : 0ll;");
+        cg.addIf("threadIdx.x == 0", [&]() {
+            cg.addLine("for (int _s = 0; _s < " + S(stages) + "; ++_s) gpudb_mbar_init(_sb_bar + _s, 1u);");
+            cg.addLine("gpudb_mbar_init_fence();");
+        });
+        cg.addLine("__syncthreads();");
+        cg.addLine("const unsigned long long _sb_pol = gpudb_policy_evict_first();");
+        cg.addBlock("auto _sb_issue = [&](long long _t, int _s)", [&]() {
+            cg.addLine("unsigned char* _st = _sb_ring + (long long)_s * " + SB + "ll;");
+            cg.addLine("gpudb_mbar_expect_tx(_sb_bar + _s, " + S(txBytes) + "u);");
+            for (size_t k = 0; k < columns_.size(); k++) {
+                const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
+                cg.addLine("gpudb_bulk_g2s_stream(_st + " + S(off[k]) + ", " + columns_[k].paramName + " + _t * " +
+                           S(tile) + "ll, " + S(tile * w) + "u, _sb_bar + _s, _sb_pol);");
+            }
+        }, ";");
+        cg.addIf("threadIdx.x == 0", [&]() {
+            cg.addBlock("for (int _s = 0; _s < " + S(stages) + "; ++_s)", [&]() {
+                cg.addLine("const long long _t = (long long)blockIdx.x + (long long)_s * gridDim.x;");
+                cg.addLine("if (_t < _sb_ntiles) _sb_issue(_t, _s);");
+            });
+        });
+        cg.addLine("unsigned _sb_par = 0u;");
+        cg.addLine("int _sb_s = 0;");
+        cg.addLine("bool _sb_ok = true;");
+        cg.addBlock("for (long long _sb_t = blockIdx.x; _sb_t < _sb_ntiles; _sb_t += gridDim.x)", [&]() {
+            cg.addLine("const bool _sb_got = gpudb_mbar_wait(_sb_bar + _sb_s, (_sb_par >> _sb_s) & 1u, gpudb_err);");
+            cg.addLine("_sb_par ^= (1u << _sb_s);");
+            cg.addIf("_sb_got", [&]() {
+                cg.addLine("const long long _sb_base = _sb_t * " + S(tile) + "ll;");
+                cg.addLine("const unsigned char* _sb_st = _sb_ring + (long long)_sb_s * " + SB + "ll;");
+                for (size_t k = 0; k < columns_.size(); k++)
+                    cg.addLine("const " + columns_[k].cudaType + "* " + columns_[k].paramName + " = reinterpret_cast<const " +
+                               columns_[k].cudaType + "*>(_sb_st + " + S(off[k]) + ");");
+                cg.addBlock("for (int " + i + " = threadIdx.x; " + i + " < " + S(tile) + "; " + i + " += " + S(bs) + ")",
+                            [&]() {
+                                cg.addLine("const long long _row = _sb_base + " + i + "; (void)_row;");
+                                consume();
+                            });
+            });
+            cg.addIf("!__syncthreads_and(_sb_got)", [&]() {
+                cg.addLine("_sb_ok = false;");
+                cg.addLine("break;");
+            });
+            cg.addIf("threadIdx.x == 0", [&]() {
+                cg.addLine("const long long _nt = _sb_t + (long long)" + S(stages) + " * gridDim.x;");
+                cg.addIf("_nt < _sb_ntiles", [&]() {
+                    cg.addLine("gpudb_fence_proxy_async();");
+                    cg.addLine("_sb_issue(_nt, _sb_s);");
+                });
+            });
+            cg.addLine("_sb_s = (_sb_s + 1 == " + S(stages) + ") ? 0 : _sb_s + 1;");
+        });
+        cg.addComment("rows of the partial last tile (all rows if a column is not 16-byte aligned)");
+        cg.addBlock("if (_sb_ok) for (long long " + i + " = _sb_ntiles * " + S(tile) + "ll + tid; " + i + " < _sb_n; " + i +
+                        " += tpg)",
+                    [&]() {
+                        cg.addLine("const long long _row = " + i + "; (void)_row;");
+                        consume();
+                    });
+    });
+}
+
+std::string CudaGridStrideScan::describe() const {
+    return std::string(cfg_.mode == ScanConfig::TmaBulk ? "TmaScan(" : "GridStrideScan(") + tableName_ + ")";
+}
+
+// ===================================================================
+// CudaBufferScan
+// ===================================================================
+CudaBufferScan::CudaBufferScan(const std::string& countName, const std::string& countExpr, const std::string& idxVar)
+    : countName_(countName), countExpr_(countExpr), idxVar_(idxVar) {}
+
+void CudaBufferScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addSizeScalarParam(countName_, "long long", countExpr_);
+    const std::string& i = idxVar_;
+    cg.addBlock("for (long long " + i + " = tid; " + i + " < " + countName_ + "; " + i + " += tpg)", [&]() {
+        cg.addLine("const long long _row = " + i + "; (void)_row;");
+        consume();
+    });
+}
+
+std::string CudaBufferScan::describe() const { return "BufferScan(" + countName_ + " = " + countExpr_ + ")"; }
+
+// ===================================================================
+// Selection / ComputeExpr
+// ===================================================================
+CudaSelection::CudaSelection(std::unique_ptr<CudaOperator> child, const std::string& predicate)
+    : CudaUnaryOperator(std::move(child)), predicate_(predicate) {}
+
+void CudaSelection::produce(CudaCodegen& cg, ConsumerFn consume) {
+    child_->produce(cg, [&]() { cg.addIf(predicate_, [&]() { consume(); }); });
+}
+
+std::string CudaSelection::describe() const { return "Selection(" + predicate_ + ")"; }
+
+CudaComputeExpr::CudaComputeExpr(std::unique_ptr<CudaOperator> child, const std::string& varName,
+                                 const std::string& varType, const std::string& expression)
+    : CudaUnaryOperator(std::move(child)), varName_(varName), varType_(varType), expression_(expression) {}
+
+void CudaComputeExpr::produce(CudaCodegen& cg, ConsumerFn consume) {
+    child_->produce(cg, [&]() {
+        cg.addLine("const " + varType_ + " " + varName_ + " = " + expression_ + ";");
+        consume();
+    });
+}
+
+std::string CudaComputeExpr::describe() const { return "ComputeExpr(" + varName_ + " = " + expression_ + ")"; }
+
+// ===================================================================
+// Bitmaps
+// ===================================================================
+CudaBitmapBuild::CudaBitmapBuild(std::unique_ptr<CudaOperator> child, const std::string& bitmapName,
+                                 const std::string& keyExpr, const std::string& sizeExpr)
+    : CudaUnaryOperator(std::move(child)), bitmapName_(bitmapName), keyExpr_(keyExpr), sizeExpr_(sizeExpr) {}
+
+void CudaBitmapBuild::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addBitmapWriteParam(bitmapName_, sizeExpr_);
+    cg.addBufferLengthParam("len_" + bitmapName_, bitmapName_);
+    if (!counter_.empty()) cg.addAtomicBufferParam(counter_, "unsigned long long", "1");
+    child_->produce(cg, [&]() {
+        cg.addLine("const long long _bk = (long long)(" + keyExpr_ + ");");
+        cg.addBlock("if ((unsigned long long)(_bk >> 5) >= (unsigned long long)len_" + bitmapName_ + ")", [&]() {
+            cg.addLine("gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+        }, " else {");
+        cg.increaseIndent();
+        if (counter_.empty()) {
+            cg.addLine("gpudb_bitmap_set(" + bitmapName_ + ", _bk);");
+        } else {
+            cg.addLine("const unsigned _bbit = 1u << (unsigned)(_bk & 31);");
+            cg.addLine("if ((atomicOr(" + bitmapName_ + " + (_bk >> 5), _bbit) & _bbit) == 0u) atomicAdd(" + counter_ +
+                       ", 1ull);");
+        }
+        consume();
+        cg.decreaseIndent();
+        cg.addLine("}");
+    });
+}
+
+std::string CudaBitmapBuild::describe() const { return "BitmapBuild(" + bitmapName_ + ", key=" + keyExpr_ + ")"; }
+
+CudaBitmapProbe::CudaBitmapProbe(std::unique_ptr<CudaOperator> child, const std::string& bitmapName,
+                                 const std::string& keyExpr, bool anti)
+    : CudaUnaryOperator(std::move(child)), bitmapName_(bitmapName), keyExpr_(keyExpr), anti_(anti) {}
+
+void CudaBitmapProbe::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addBitmapReadParam(bitmapName_, "");
+    cg.addBufferLengthParam("len_" + bitmapName_, bitmapName_);
+    child_->produce(cg, [&]() {
+        const std::string k = cg.fresh("_pk");
+        cg.addLine("const long long " + k + " = (long long)(" + keyExpr_ + ");");
+        // Keys beyond the bitmap are simply absent (not an error on probe).
+        const std::string inb = "(unsigned long long)(" + k + " >> 5) < (unsigned long long)len_" + bitmapName_;
+        const std::string t = "gpudb_bitmap_test(" + bitmapName_ + ", " + k + ")";
+        cg.addIf(anti_ ? "!(" + inb + " && " + t + ")" : "(" + inb + ") && " + t, [&]() { consume(); });
+    });
+}
+
+std::string CudaBitmapProbe::describe() const {
+    return std::string(anti_ ? "AntiBitmapProbe(" : "BitmapProbe(") + bitmapName_ + ", key=" + keyExpr_ + ")";
+}
+
+// ===================================================================
+// Direct-address maps
+// ===================================================================
+CudaArrayStore::CudaArrayStore(std::unique_ptr<CudaOperator> child, const std::string& arrayName,
+                               const std::string& keyExpr, const std::string& valueExpr,
+                               const std::string& valueType, const std::string& sizeExpr)
+    : CudaUnaryOperator(std::move(child)),
+      arrayName_(arrayName), keyExpr_(keyExpr), valueExpr_(valueExpr), valueType_(valueType), sizeExpr_(sizeExpr) {}
+
+void CudaArrayStore::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addBufferParam(arrayName_, valueType_, sizeExpr_, true, 0xFF);
+    cg.addBufferLengthParam("len_" + arrayName_, arrayName_);
+    child_->produce(cg, [&]() {
+        const std::string k = cg.fresh("_ak");
+        cg.addLine("const long long " + k + " = (long long)(" + keyExpr_ + ");");
+        cg.addBlock("if ((unsigned long long)" + k + " >= (unsigned long long)len_" + arrayName_ + ")", [&]() {
+            cg.addLine("gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+        }, " else {");
+        cg.increaseIndent();
+        cg.addLine(arrayName_ + "[" + k + "] = (" + valueType_ + ")(" + valueExpr_ + ");");
+        consume();
+        cg.decreaseIndent();
+        cg.addLine("}");
+    });
+}
+
+std::string CudaArrayStore::describe() const {
+    return "ArrayStore(" + arrayName_ + "[" + keyExpr_ + "] = " + valueExpr_ + ")";
+}
+
+CudaArrayLookup::CudaArrayLookup(std::unique_ptr<CudaOperator> child, const std::string& arrayName,
+                                 const std::string& keyExpr, const std::string& resultVar,
+                                 const std::string& resultType, long long sentinel)
+    : CudaUnaryOperator(std::move(child)),
+      arrayName_(arrayName), keyExpr_(keyExpr), resultVar_(resultVar), resultType_(resultType), sentinel_(sentinel) {}
+
+void CudaArrayLookup::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addReadBufferParam(arrayName_, resultType_);
+    cg.addBufferLengthParam("len_" + arrayName_, arrayName_);
+    child_->produce(cg, [&]() {
+        const std::string k = cg.fresh("_lk");
+        cg.addLine("const long long " + k + " = (long long)(" + keyExpr_ + ");");
+        cg.addLine("const " + resultType_ + " " + resultVar_ + " = ((unsigned long long)" + k +
+                   " < (unsigned long long)len_" + arrayName_ + ") ? " + arrayName_ + "[" + k + "] : (" + resultType_ +
+                   ")(" + S(sentinel_) + "ll);");
+        cg.addIf(resultVar_ + " != (" + resultType_ + ")(" + S(sentinel_) + "ll)", [&]() { consume(); });
+    });
+}
+
+std::string CudaArrayLookup::describe() const {
+    return "ArrayLookup(" + resultVar_ + " = " + arrayName_ + "[" + keyExpr_ + "])";
+}
+
+// ===================================================================
+// CudaTGReduce
+// ===================================================================
+CudaTGReduce::CudaTGReduce(std::unique_ptr<CudaOperator> child, const std::string& outputPrefix)
+    : CudaUnaryOperator(std::move(child)), outputPrefix_(outputPrefix) {}
+
+void CudaTGReduce::addAccumulator(const std::string& name, const std::string& valueExpr, const std::string& type,
+                                  const std::string& buffer) {
+    if (type != "wide" && type != "long" && type != "umax")
+        throw std::runtime_error("CudaTGReduce: type must be 'wide', 'long' or 'umax'");
+    accumulators_.push_back({name, buffer.empty() ? outputPrefix_ + "_" + name : buffer, valueExpr, type});
+}
+
+void CudaTGReduce::setResultAlias(const std::string& displayName, int scaleDown) {
+    resultInfos_.push_back({displayName, scaleDown});
+}
+
+void CudaTGReduce::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const int na = (int)accumulators_.size();
+    if (na == 0) throw std::runtime_error("CudaTGReduce: no accumulators");
+    for (const auto& a : accumulators_)
+        cg.addAtomicBufferParam(a.buffer, "unsigned long long", a.type == "wide" ? "2" : "1");
+    cg.addLine("unsigned long long _tr_acc[" + S(na) + "];");
+    cg.addLine("#pragma unroll");
+    cg.addLine("for (int _a = 0; _a < " + S(na) + "; ++_a) _tr_acc[_a] = 0ull;");
+    child_->produce(cg, [&]() {
+        for (int a = 0; a < na; a++) {
+            const auto& acc = accumulators_[a];
+            if (acc.type == "umax")
+                cg.addLine("_tr_acc[" + S(a) + "] = max(_tr_acc[" + S(a) + "], (unsigned long long)(" + acc.valueExpr + "));");
+            else
+                cg.addLine("_tr_acc[" + S(a) + "] += (unsigned long long)(long long)(" + acc.valueExpr + ");");
+        }
+        consume();
+    });
+    cg.addComment("block reduction (warp shuffles + smem), one RED per accumulator per block");
+    cg.addLine("__shared__ unsigned long long _tr_red[32 * " + S(na) + "];");
+    cg.addLine("#pragma unroll");
+    cg.addBlock("for (int _a = 0; _a < " + S(na) + "; ++_a)", [&]() {
+        cg.addLine("unsigned long long _v = _tr_acc[_a];");
+        cg.addBlock("switch (_a)", [&]() {
+            for (int a = 0; a < na; a++)
+                cg.addLine("case " + S(a) + ": _v = " +
+                           (accumulators_[a].type == "umax" ? "gpudb_warp_max_u64(_v)" : "gpudb_warp_sum_u64(_v)") +
+                           "; break;");
+            cg.addLine("default: break;");
+        });
+        cg.addLine("if ((threadIdx.x & 31u) == 0u) _tr_red[(threadIdx.x >> 5) * " + S(na) + " + _a] = _v;");
+    });
+    cg.addLine("__syncthreads();");
+    cg.addBlock("for (int _a = threadIdx.x; _a < " + S(na) + "; _a += blockDim.x)", [&]() {
+        cg.addLine("unsigned long long _tot = 0ull;");
+        cg.addBlock("switch (_a)", [&]() {
+            for (int a = 0; a < na; a++) {
+                const auto& acc = accumulators_[a];
+                const std::string comb = acc.type == "umax" ? "_tot = max(_tot, _tr_red[_w * " + S(na) + " + _a]);"
+                                                            : "_tot += _tr_red[_w * " + S(na) + " + _a];";
+                std::string emit;
+                if (acc.type == "umax") emit = "if (_tot) atomicMax(" + acc.buffer + ", _tot);";
+                else if (acc.type == "wide") emit = "if (_tot) gpudb_acc128_add(" + acc.buffer + ", (long long)_tot);";
+                else emit = "if (_tot) gpudb_acc64_add(" + acc.buffer + ", (long long)_tot);";
+                cg.addLine("case " + S(a) + ": for (int _w = 0; _w < (int)(blockDim.x >> 5); ++_w) " + comb + " " + emit +
+                           " break;");
+            }
+            cg.addLine("default: break;");
+        });
+    });
+    for (size_t i = 0; i < accumulators_.size(); i++) {
+        const auto& a = accumulators_[i];
+        const std::string disp = i < resultInfos_.size() ? resultInfos_[i].displayName : a.name;
+        const int sd = i < resultInfos_.size() ? resultInfos_[i].scaleDown : 0;
+        cg.registerScalarAggColumn(disp, a.buffer, a.type == "wide", sd);
+    }
+}
+
+std::string CudaTGReduce::describe() const {
+    return "TGReduce(" + S((long long)accumulators_.size()) + " accumulators) <- " + describeChain();
+}
+
+// ===================================================================
+// CudaKeyedAgg
+// ===================================================================
+CudaKeyedAgg::CudaKeyedAgg(std::unique_ptr<CudaOperator> child, const std::string& outputArrayName,
+                           const std::string& bucketExpr, int numBuckets, int valuesPerBucket,
+                           const std::string& sizeExpr)
+    : CudaUnaryOperator(std::move(child)),
+      outputArrayName_(outputArrayName), bucketExpr_(bucketExpr), numBuckets_(numBuckets),
+      valuesPerBucket_(valuesPerBucket), sizeExpr_(sizeExpr) {}
+
+void CudaKeyedAgg::addAggregate(const std::string& name, int offset, const std::string& valueExpr,
+                                const std::string& atomicOp, bool isWide, int scaleDown) {
+    if (atomicOp != "add" && atomicOp != "min" && atomicOp != "max")
+        throw std::runtime_error("CudaKeyedAgg: atomicOp must be add/min/max");
+    if (isWide && atomicOp != "add") throw std::runtime_error("CudaKeyedAgg: wide aggregates must be adds");
+    if (offset < 0 || offset + (isWide ? 2 : 1) > valuesPerBucket_)
+        throw std::runtime_error("CudaKeyedAgg: aggregate '" + name + "' does not fit in valuesPerBucket");
+    aggregates_.push_back({name, offset, valueExpr, atomicOp, isWide, scaleDown});
+}
+
+CudaKeyedAgg::Strategy CudaKeyedAgg::chosenStrategy() const {
+    bool allAdds = true;
+    for (const auto& a : aggregates_)
+        if (a.atomicOp != "add") allAdds = false;
+    if (strategy_ != Strategy::Auto) {
+        if (!allAdds && strategy_ != Strategy::Global)
+            throw std::runtime_error("CudaKeyedAgg: min/max aggregates need the Global strategy");
+        return strategy_;
+    }
+    if (!allAdds) return Strategy::Global;
+    if (numBuckets_ * (int)aggregates_.size() <= 64 && numBuckets_ <= 16) return Strategy::Registers;
+    if ((long long)numBuckets_ * valuesPerBucket_ <= 16384) return Strategy::Shared;
+    return Strategy::Global;
+}
+
+void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const std::string sz = sizeExpr_.empty() ? S((long long)numBuckets_ * valuesPerBucket_) : sizeExpr_;
+    cg.addAtomicBufferParam(outputArrayName_, "unsigned long long", sz);
+    const int nb = numBuckets_, vpb = valuesPerBucket_, na = (int)aggregates_.size();
+    const Strategy st = chosenStrategy();
+    const std::string out = outputArrayName_;
+
+    auto emitValues = [&]() {
+        cg.addLine("const int _bucket = (int)(" + bucketExpr_ + ");");
+        for (int j = 0; j < na; j++)
+            cg.addLine("const long long _kv" + S(j) + " = (long long)(" + aggregates_[j].valueExpr + ");");
+    };
+
+    if (st == Strategy::Registers) {
+        cg.addComment("keyed aggregation: per-thread register accumulators (" + S(nb) + " buckets x " + S(na) +
+                      " aggregates), predicated on the bucket id");
+        for (int j = 0; j < na; j++) {
+            std::string init;
+            for (int b = 0; b < nb; b++) init += (b ? ", " : "") + std::string("0ll");
+            cg.addLine("long long _ka" + S(j) + "[" + S(nb) + "] = {" + init + "};");
+        }
+        child_->produce(cg, [&]() {
+            emitValues();
+            cg.addLine("#pragma unroll");
+            cg.addBlock("for (int _b = 0; _b < " + S(nb) + "; ++_b)", [&]() {
+                cg.addLine("const bool _hit = (_bucket == _b);");
+                for (int j = 0; j < na; j++) cg.addLine("_ka" + S(j) + "[_b] += _hit ? _kv" + S(j) + " : 0ll;");
+            });
+            consume();
+        });
+        const int nacc = nb * na;
+        cg.addComment("block reduction, then one RED per non-zero (bucket, aggregate) per block");
+        cg.addLine("long long _ka_all[" + S(nacc) + "];");
+        cg.addLine("#pragma unroll");
+        cg.addBlock("for (int _b = 0; _b < " + S(nb) + "; ++_b)", [&]() {
+            for (int j = 0; j < na; j++) cg.addLine("_ka_all[_b * " + S(na) + " + " + S(j) + "] = _ka" + S(j) + "[_b];");
+        });
+        cg.addLine("__shared__ long long _ka_red[32 * " + S(nacc) + "];");
+        cg.addLine("gpudb_block_partials<" + S(nacc) + ">(_ka_all, _ka_red);");
+        cg.addBlock("for (int _a = threadIdx.x; _a < " + S(nacc) + "; _a += blockDim.x)", [&]() {
+            cg.addLine("const long long _tot = gpudb_block_total(_ka_red, " + S(nacc) + ", _a);");
+            cg.addLine("if (_tot == 0ll) continue;");
+            cg.addLine("const int _b = _a / " + S(na) + ", _j = _a % " + S(na) + ";");
+            cg.addBlock("switch (_j)", [&]() {
+                for (int j = 0; j < na; j++) {
+                    const auto& ag = aggregates_[j];
+                    cg.addLine("case " + S(j) + ": " + (ag.isWide ? "gpudb_acc128_add(" : "gpudb_acc64_add(") + out +
+                               " + _b * " + S(vpb) + " + " + S(ag.offset) + ", _tot); break;");
+                }
+                cg.addLine("default: break;");
+            });
+        });
+    } else if (st == Strategy::Shared) {
+        const int words = nb * vpb;
+        const int soff = cg.allocDynamicSmem(words * 8);
+        cg.addComment("keyed aggregation: per-block shared-memory table of " + S(words) + " words");
+        cg.addLine("unsigned long long* _ks = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(soff) + ");");
+        cg.addLine("for (int _w = threadIdx.x; _w < " + S(words) + "; _w += blockDim.x) _ks[_w] = 0ull;");
+        cg.addLine("__syncthreads();");
+        child_->produce(cg, [&]() {
+            emitValues();
+            cg.addBlock("if ((unsigned)_bucket < " + S(nb) + "u)", [&]() {
+                for (int j = 0; j < na; j++) {
+                    const auto& ag = aggregates_[j];
+                    const std::string base = "_ks + _bucket * " + S(vpb) + " + " + S(ag.offset);
+                    if (ag.isWide)
+                        cg.addLine("gpudb_acc128_add(" + base + ", _kv" + S(j) + ");");
+                    else
+                        cg.addLine("atomicAdd(" + base + ", (unsigned long long)_kv" + S(j) + ");");
+                }
+            }, " else { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); }");
+            consume();
+        });
+        cg.addLine("__syncthreads();");
+        cg.addBlock("for (int _w = threadIdx.x; _w < " + S(words) + "; _w += blockDim.x)", [&]() {
+            cg.addLine("const unsigned long long _v = _ks[_w];");
+            cg.addLine("if (_v != 0ull) atomicAdd(" + out + " + _w, _v);");
+        });
+    } else {
+        cg.addComment("keyed aggregation: per-row global atomics");
+        child_->produce(cg, [&]() {
+            emitValues();
+            cg.addBlock("if ((unsigned)_bucket < " + S(nb) + "u)", [&]() {
+                for (int j = 0; j < na; j++) {
+                    const auto& ag = aggregates_[j];
+                    const std::string addr = out + " + _bucket * " + S(vpb) + " + " + S(ag.offset);
+                    if (ag.atomicOp == "add")
+                        cg.addLine(std::string(ag.isWide ? "gpudb_acc128_add(" : "gpudb_acc64_add(") + addr + ", _kv" +
+                                   S(j) + ");");
+                    else
+                        cg.addLine(std::string(ag.atomicOp == "min" ? "atomicMin(" : "atomicMax(") +
+                                   "reinterpret_cast<long long*>(" + addr + "), _kv" + S(j) + ");");
+                }
+            }, " else { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); }");
+            consume();
+        });
+    }
+
+    std::vector<CudaResultSchema::KeyedAggSlot> slots;
+    for (const auto& a : aggregates_) slots.push_back({a.name, a.offset, a.isWide, a.scaleDown});
+    cg.registerKeyedAggOutput(outputArrayName_, numBuckets_, valuesPerBucket_, slots);
+}
+
+std::string CudaKeyedAgg::describe() const {
+    static const char* names[] = {"auto", "registers", "shared", "global"};
+    return "KeyedAgg(" + outputArrayName_ + ", " + S(numBuckets_) + " buckets, " + S((long long)aggregates_.size()) +
+           " aggs, " + names[(int)chosenStrategy()] + ") <- " + describeChain();
+}
+
+// ===================================================================
+// CudaAtomicAgg
+// ===================================================================
+CudaAtomicAgg::CudaAtomicAgg(std::unique_ptr<CudaOperator> child, const std::string& arrayName,
+                             const std::string& bucketExpr, const std::string& valueExpr,
+                             const std::string& sizeExpr, const std::string& elemType)
+    : CudaUnaryOperator(std::move(child)),
+      arrayName_(arrayName), bucketExpr_(bucketExpr), valueExpr_(valueExpr), sizeExpr_(sizeExpr), elemType_(elemType) {}
+
+void CudaAtomicAgg::addAggregate(const std::string& arrayName, const std::string& valueExpr) {
+    extra_.push_back({arrayName, valueExpr});
+}
+
+void CudaAtomicAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
+    if (elemType_ != "unsigned long long")
+        throw std::runtime_error("CudaAtomicAgg: only 64-bit integer accumulators are supported");
+    std::vector<std::pair<std::string, std::string>> arrs{{arrayName_, valueExpr_}};
+    for (const auto& e : extra_) arrs.push_back(e);
+    const int na = (int)arrs.size();
+    for (const auto& a : arrs) {
+        if (zeroInit_)
+            cg.addAtomicBufferParam(a.first, elemType_, sizeExpr_);
+        else
+            cg.addBufferParam(a.first, elemType_, sizeExpr_, false);
+    }
+    const std::string len = "len_" + arrayName_;
+    cg.addBufferLengthParam(len, arrayName_);
+    const int L = smemLog2_;
+    const int slots = 1 << L;
+    if (L > 0) {
+        const int ko = cg.allocDynamicSmem(slots * 8);
+        const int vo = cg.allocDynamicSmem(slots * 8 * na);
+        cg.addComment("per-block shared-memory cache of hot buckets (" + S(slots) + " slots)");
+        cg.addLine("unsigned long long* _ac_k = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(ko) + ");");
+        cg.addLine("unsigned long long* _ac_v = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(vo) + ");");
+        cg.addLine("for (int _w = threadIdx.x; _w < " + S(slots) + "; _w += blockDim.x) _ac_k[_w] = GPUDB_EMPTY64;");
+        cg.addLine("for (int _w = threadIdx.x; _w < " + S(slots * na) + "; _w += blockDim.x) _ac_v[_w] = 0ull;");
+        cg.addLine("__syncthreads();");
+    }
+    child_->produce(cg, [&]() {
+        cg.addLine("const long long _ab = (long long)(" + bucketExpr_ + ");");
+        for (int j = 0; j < na; j++) cg.addLine("long long _av" + S(j) + " = (long long)(" + arrs[j].second + ");");
+        auto update = [&]() {
+            cg.addBlock("if ((unsigned long long)_ab >= (unsigned long long)" + len + ")", [&]() {
+                cg.addLine("gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+            }, " else {");
+            cg.increaseIndent();
+            if (L > 0) {
+                cg.addLine("const int _as = gpudb_smem_ht_slot64(_ac_k, " + S(L) + ", (unsigned long long)_ab, 16);");
+                cg.addBlock("if (_as >= 0)", [&]() {
+                    for (int j = 0; j < na; j++)
+                        cg.addLine("atomicAdd(_ac_v + " + S(j * slots) + " + _as, (unsigned long long)_av" + S(j) + ");");
+                }, " else {");
+                cg.increaseIndent();
+                for (int j = 0; j < na; j++)
+                    cg.addLine("atomicAdd(" + arrs[j].first + " + _ab, (unsigned long long)_av" + S(j) + ");");
+                cg.decreaseIndent();
+                cg.addLine("}");
+            } else {
+                for (int j = 0; j < na; j++)
+                    cg.addLine("atomicAdd(" + arrs[j].first + " + _ab, (unsigned long long)_av" + S(j) + ");");
+            }
+            cg.decreaseIndent();
+            cg.addLine("}");
+        };
+        if (warpAgg_) {
+            cg.addLine("const unsigned _am = __activemask();");
+            cg.addLine("const unsigned _peers = __match_any_sync(_am, (unsigned long long)_ab);");
+            for (int j = 0; j < na; j++) cg.addLine("_av" + S(j) + " = gpudb_peer_sum(_am, _peers, _av" + S(j) + ");");
+            cg.addIf("(int)(threadIdx.x & 31u) == __ffs(_peers) - 1", update);
+        } else {
+            update();
+        }
+        consume();
+    });
+    if (L > 0) {
+        cg.addLine("__syncthreads();");
+        cg.addBlock("for (int _w = threadIdx.x; _w < " + S(slots) + "; _w += blockDim.x)", [&]() {
+            cg.addLine("const unsigned long long _k = _ac_k[_w];");
+            cg.addLine("if (_k == GPUDB_EMPTY64) continue;");
+            for (int j = 0; j < na; j++)
+                cg.addLine("if (_ac_v[" + S(j * slots) + " + _w] != 0ull) atomicAdd(" + arrs[j].first + " + _k, _ac_v[" +
+                           S(j * slots) + " + _w]);");
+        });
+    }
+}
+
+std::string CudaAtomicAgg::describe() const {
+    return "AtomicAgg(" + arrayName_ + "[" + bucketExpr_ + "]" + (warpAgg_ ? ", warp-agg" : "") +
+           (smemLog2_ ? ", smem-cache" : "") + ") <- " + describeChain();
+}
+
+// ===================================================================
+// CudaAtomicCount
+// ===================================================================
+CudaAtomicCount::CudaAtomicCount(std::unique_ptr<CudaOperator> child, const std::string& arrayName,
+                                 const std::string& bucketExpr, const std::string& sizeExpr)
+    : CudaUnaryOperator(std::move(child)), arrayName_(arrayName), bucketExpr_(bucketExpr), sizeExpr_(sizeExpr) {}
+
+void CudaAtomicCount::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addAtomicBufferParam(arrayName_, "unsigned long long", sizeExpr_);
+    cg.addBufferLengthParam("len_" + arrayName_, arrayName_);
+    long long staticSize = 0;
+    try {
+        size_t used = 0;
+        staticSize = std::stoll(sizeExpr_, &used);
+        if (used != sizeExpr_.size()) staticSize = 0;
+    } catch (...) {
+        staticSize = 0;
+    }
+    const std::string arr = arrayName_;
+    if (staticSize > 0 && staticSize <= 8192) {
+        const std::string sz = S(staticSize);
+        cg.addComment("shared-memory histogram of " + sz + " bins");
+        cg.addLine("__shared__ unsigned _hist[" + sz + "];");
+        cg.addLine("for (int _h = threadIdx.x; _h < " + sz + "; _h += blockDim.x) _hist[_h] = 0u;");
+        cg.addLine("__syncthreads();");
+        child_->produce(cg, [&]() {
+            cg.addLine("const long long _hb = (long long)(" + bucketExpr_ + ");");
+            cg.addLine("if ((unsigned long long)_hb < " + sz + "ull) atomicAdd(_hist + _hb, 1u); else "
+                       "gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+            consume();
+        });
+        cg.addLine("__syncthreads();");
+        cg.addLine("for (int _h = threadIdx.x; _h < " + sz + "; _h += blockDim.x) if (_hist[_h]) atomicAdd(" + arr +
+                   " + _h, (unsigned long long)_hist[_h]);");
+    } else {
+        child_->produce(cg, [&]() {
+            cg.addLine("const long long _hb = (long long)(" + bucketExpr_ + ");");
+            cg.addLine("if ((unsigned long long)_hb < (unsigned long long)len_" + arr + ") atomicAdd(" + arr +
+                       " + _hb, 1ull); else gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+            consume();
+        });
+    }
+}
+
+std::string CudaAtomicCount::describe() const { return "AtomicCount(" + arrayName_ + "[" + bucketExpr_ + "])"; }
+
+// ===================================================================
+// CudaMaterialize
+// ===================================================================
+CudaMaterialize::CudaMaterialize(std::unique_ptr<CudaOperator> child, const std::string& counterName,
+                                 const std::string& capacityExpr)
+    : CudaUnaryOperator(std::move(child)), counterName_(counterName), capacityExpr_(capacityExpr) {}
+
+void CudaMaterialize::addColumn(const std::string& arrayName, const std::string& type, const std::string& valueExpr,
+                                const std::string& displayName) {
+    columns_.push_back({arrayName, type, valueExpr, displayName.empty() ? arrayName : displayName});
+}
+
+void CudaMaterialize::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addAtomicBufferParam(counterName_, "unsigned long long", "1");
+    for (const auto& c : columns_) cg.addBufferParam(c.arrayName, c.type, capacityExpr_, false);
+    cg.addSizeScalarParam("cap_" + counterName_, "long long", capacityExpr_);
+    cg.registerMaterializeOutput(counterName_);
+    for (const auto& c : columns_) cg.registerOutputColumn(c.displayName, c.arrayName, c.type);
+    child_->produce(cg, [&]() {
+        cg.addLine("const unsigned long long _pos = gpudb_warp_reserve(" + counterName_ + ", true);");
+        cg.addBlock("if (_pos < (unsigned long long)cap_" + counterName_ + ")", [&]() {
+            for (const auto& c : columns_)
+                cg.addLine(c.arrayName + "[_pos] = (" + c.type + ")(" + c.valueExpr + ");");
+        }, " else { gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY); }");
+        consume();
+    });
+}
+
+std::string CudaMaterialize::describe() const {
+    return "Materialize(" + S((long long)columns_.size()) + " columns) <- " + describeChain();
+}
+
+// ===================================================================
+// Hash build / probe / group-by
+// ===================================================================
+CudaHashBuild::CudaHashBuild(std::unique_ptr<CudaOperator> child, const std::string& tableName,
+                             const std::string& keyExpr, const std::string& keyType, const std::string& capacityExpr,
+                             HashLayout layout, int maxProbe)
+    : CudaUnaryOperator(std::move(child)),
+      table_(tableName), keyExpr_(keyExpr), keyType_(keyType), capExpr_(capacityExpr), layout_(layout),
+      maxProbe_(maxProbe) {}
+
+void CudaHashBuild::addPayload(const std::string& column, const std::string& type, const std::string& valueExpr) {
+    payloads_.push_back({column, type, valueExpr});
+}
+
+void CudaHashBuild::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const KeyOps ko = keyOps(keyType_, layout_);
+    const std::string cap = hashSlotsExpr(capExpr_);
+    cg.addHashMapParam(table_ + "_keys", ko.store, cap);
+    for (const auto& p : payloads_) cg.addBufferParam(table_ + "_" + p.column, p.type, cap, false);
+    cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    child_->produce(cg, [&]() {
+        cg.addLine("const long long _hslot = " + ko.ins + "(" + table_ + "_keys, " + table_ + "_log2cap, " + ko.cast + "(" +
+                   keyExpr_ + "), " + S(probeArg(layout_, maxProbe_)) + "u, gpudb_err);");
+        cg.addIf("_hslot >= 0", [&]() {
+            for (const auto& p : payloads_)
+                cg.addLine(table_ + "_" + p.column + "[_hslot] = (" + p.type + ")(" + p.valueExpr + ");");
+            consume();
+        });
+    });
+}
+
+std::string CudaHashBuild::describe() const { return "HashBuild(" + table_ + ", key=" + keyExpr_ + ") <- " + describeChain(); }
+
+CudaHashProbe::CudaHashProbe(std::unique_ptr<CudaOperator> child, const std::string& tableName,
+                             const std::string& keyExpr, const std::string& keyType, const std::string& capacityExpr,
+                             const std::string& slotVar, HashLayout layout, int maxProbe)
+    : CudaUnaryOperator(std::move(child)),
+      table_(tableName), keyExpr_(keyExpr), keyType_(keyType), capExpr_(capacityExpr), slotVar_(slotVar),
+      layout_(layout), maxProbe_(maxProbe) {}
+
+void CudaHashProbe::addPayloadRead(const std::string& column, const std::string& type) {
+    payloadReads_.push_back({column, type});
+}
+
+void CudaHashProbe::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const KeyOps ko = keyOps(keyType_, layout_);
+    cg.addHashMapReadParam(table_ + "_keys", ko.store);
+    for (const auto& p : payloadReads_) cg.addReadBufferParam(table_ + "_" + p.first, p.second);
+    cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    child_->produce(cg, [&]() {
+        cg.addLine("const long long " + slotVar_ + " = " + ko.find + "(" + table_ + "_keys, " + table_ + "_log2cap, " +
+                   ko.cast + "(" + keyExpr_ + "), " + S(probeArg(layout_, maxProbe_)) + "u);");
+        cg.addIf(slotVar_ + " >= 0", [&]() { consume(); });
+    });
+}
+
+std::string CudaHashProbe::describe() const { return "HashProbe(" + table_ + ", key=" + keyExpr_ + ") <- " + describeChain(); }
+
+CudaHashGroupBy::CudaHashGroupBy(std::unique_ptr<CudaOperator> child, const std::string& tableName,
+                                 const std::string& keyExpr, const std::string& keyType,
+                                 const std::string& capacityExpr, HashLayout layout, int maxProbe)
+    : CudaUnaryOperator(std::move(child)),
+      table_(tableName), keyExpr_(keyExpr), keyType_(keyType), capExpr_(capacityExpr), layout_(layout),
+      maxProbe_(maxProbe) {}
+
+void CudaHashGroupBy::addAggregate(const std::string& name, const std::string& valueExpr) {
+    aggs_.push_back({name, valueExpr});
+}
+
+void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
+    if (aggs_.empty()) throw std::runtime_error("CudaHashGroupBy: no aggregates");
+    const KeyOps ko = keyOps(keyType_, layout_);
+    const std::string cap = hashSlotsExpr(capExpr_);
+    const std::string keys = table_ + "_keys";
+    cg.addHashMapParam(keys, ko.store, cap);
+    for (const auto& a : aggs_) cg.addAtomicBufferParam(table_ + "_" + a.name, "unsigned long long", cap);
+    cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    const int na = (int)aggs_.size();
+    const int L = smemLog2_;
+    const bool smem = L > 0 && ko.store == "unsigned long long";
+    if (smem) {
+        const int slots = 1 << L;
+        const int ko_off = cg.allocDynamicSmem(slots * 8);
+        const int vo_off = cg.allocDynamicSmem(slots * 8 * na);
+        cg.addComment("per-block shared-memory pre-aggregation table (" + S(slots) + " slots) for heavy hitters");
+        cg.addLine("unsigned long long* _gs_k = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(ko_off) + ");");
+        cg.addLine("unsigned long long* _gs_v = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(vo_off) + ");");
+        cg.addBlock("for (int _w = threadIdx.x; _w < " + S(slots) + "; _w += blockDim.x)", [&]() {
+            cg.addLine("_gs_k[_w] = GPUDB_EMPTY64;");
+            for (int j = 0; j < na; j++) cg.addLine("_gs_v[" + S(j) + " * " + S(slots) + " + _w] = 0ull;");
+        });
+        cg.addLine("__syncthreads();");
+    }
+    auto globalUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
+        cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + table_ + "_log2cap, " + ko.cast + keyVar + ", " +
+                   S(probeArg(layout_, maxProbe_)) + "u, gpudb_err);");
+        cg.addBlock("if (_gslot >= 0)", [&]() {
+            for (int j = 0; j < na; j++)
+                cg.addLine("atomicAdd(" + table_ + "_" + aggs_[j].name + " + _gslot, (unsigned long long)" + vals[j] + ");");
+        });
+    };
+    child_->produce(cg, [&]() {
+        cg.addLine("const long long _gk = (long long)(" + keyExpr_ + ");");
+        std::vector<std::string> vals;
+        for (int j = 0; j < na; j++) {
+            cg.addLine("long long _gv" + S(j) + " = (long long)(" + aggs_[j].valueExpr + ");");
+            vals.push_back("_gv" + S(j));
+        }
+        auto update = [&]() {
+            if (smem) {
+                cg.addLine("const int _gss = gpudb_smem_ht_slot64(_gs_k, " + S(L) + ", (unsigned long long)_gk, 8);");
+                cg.addBlock("if (_gss >= 0)", [&]() {
+                    for (int j = 0; j < na; j++)
+                        cg.addLine("atomicAdd(_gs_v + " + S(j) + " * " + S(1 << L) + " + _gss, (unsigned long long)_gv" +
+                                   S(j) + ");");
+                }, " else {");
+                cg.increaseIndent();
+                globalUpdate("(_gk)", vals);
+                cg.decreaseIndent();
+                cg.addLine("}");
+            } else {
+                globalUpdate("(_gk)", vals);
+            }
+        };
+        if (warpAgg_) {
+            cg.addLine("const unsigned _gm = __activemask();");
+            cg.addLine("const unsigned _gpeers = __match_any_sync(_gm, (unsigned long long)_gk);");
+            for (int j = 0; j < na; j++) cg.addLine("_gv" + S(j) + " = gpudb_peer_sum(_gm, _gpeers, _gv" + S(j) + ");");
+            cg.addIf("(int)(threadIdx.x & 31u) == __ffs(_gpeers) - 1", update);
+        } else {
+            update();
+        }
+        consume();
+    });
+    if (smem) {
+        cg.addComment("flush the shared-memory table into the global table");
+        cg.addLine("__syncthreads();");
+        cg.addBlock("for (int _w = threadIdx.x; _w < " + S(1 << L) + "; _w += blockDim.x)", [&]() {
+            cg.addLine("const unsigned long long _fk = _gs_k[_w];");
+            cg.addLine("if (_fk == GPUDB_EMPTY64) continue;");
+            std::vector<std::string> vals;
+            for (int j = 0; j < na; j++) vals.push_back("_gs_v[" + S(j) + " * " + S(1 << L) + " + _w]");
+            globalUpdate("(_fk)", vals);
+        });
+    }
+    auto& hs = cg.resultSchema();
+    hs.kind = CudaResultSchema::HASH_AGG;
+    hs.hashAgg.keyBuffer = keys;
+    hs.hashAgg.keyType = ko.store;
+    hs.hashAgg.capacitySymbol = cap;
+    hs.hashAgg.aggs.clear();
+    for (const auto& a : aggs_) hs.hashAgg.aggs.push_back({a.name, table_ + "_" + a.name});
+}
+
+std::string CudaHashGroupBy::describe() const {
+    return "HashGroupBy(" + table_ + ", key=" + keyExpr_ + (layout_ == HashLayout::Bucket8 ? ", bucket8" : ", linear") +
+           (warpAgg_ ? ", warp-agg" : "") + (smemLog2_ ? ", smem-preagg" : "") + ") <- " + describeChain();
+}
+
+// ===================================================================
+// CudaTopK
+// ===================================================================
+CudaTopK::CudaTopK(std::unique_ptr<CudaOperator> child, const std::string& outPrefix, const std::string& keyExpr,
+                   const std::string& valueExpr, int k, int maxBlocks)
+    : CudaUnaryOperator(std::move(child)), out_(outPrefix), keyExpr_(keyExpr), valueExpr_(valueExpr), k_(k),
+      maxBlocks_(maxBlocks) {}
+
+void CudaTopK::produce(CudaCodegen& cg, ConsumerFn consume) {
+    if (k_ < 1 || k_ > 32) throw std::runtime_error("CudaTopK: k must be in [1,32]");
+    const std::string K = S(k_);
+    cg.setPhaseMaxThreadgroups(maxBlocks_);
+    cg.addBufferParam(out_ + "_keys", "long long", K, true, 0);
+    cg.addBufferParam(out_ + "_vals", "long long", K, true, 0);
+    cg.addAtomicBufferParam(out_ + "_count", "unsigned long long", "1");
+    cg.addBufferParam(out_ + "_pkeys", "long long", S((long long)k_ * maxBlocks_), false);
+    cg.addBufferParam(out_ + "_pvals", "long long", S((long long)k_ * maxBlocks_), false);
+    cg.addAtomicBufferParam(out_ + "_ticket", "unsigned", "1");
+    cg.addLine("long long _tk_v[" + K + "], _tk_k[" + K + "];");
+    cg.addLine("#pragma unroll");
+    cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _tk_v[_q] = GPUDB_TOPK_NONE_VAL; _tk_k[_q] = GPUDB_TOPK_NONE_KEY; }");
+    child_->produce(cg, [&]() {
+        cg.addLine("gpudb_topk_push<" + K + ">(_tk_v, _tk_k, (long long)(" + valueExpr_ + "), (long long)(" + keyExpr_ +
+                   "));");
+        consume();
+    });
+    cg.addComment("warp merge -> block merge -> last-block merge of the per-block lists");
+    cg.addLine("long long _tw_v[" + K + "], _tw_k[" + K + "];");
+    cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
+    cg.addLine("__shared__ long long _ts_v[32 * " + K + "], _ts_k[32 * " + K + "];");
+    cg.addLine("__shared__ bool _t_last;");
+    cg.addBlock("if ((threadIdx.x & 31u) == 0u)", [&]() {
+        cg.addLine("#pragma unroll");
+        cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _ts_v[(threadIdx.x >> 5) * " + K + " + _q] = _tw_v[_q]; "
+                   "_ts_k[(threadIdx.x >> 5) * " + K + " + _q] = _tw_k[_q]; }");
+    });
+    cg.addLine("__syncthreads();");
+    // merges n entries of (vals, keys) held in memory into the first warp's list
+    auto warpMerge = [&](const std::string& vsrc, const std::string& ksrc, const std::string& n, bool coherent) {
+        cg.addLine("#pragma unroll");
+        cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _tk_v[_q] = GPUDB_TOPK_NONE_VAL; _tk_k[_q] = GPUDB_TOPK_NONE_KEY; }");
+        const std::string ld_v = coherent ? "__ldcg(" + vsrc + " + _e)" : vsrc + "[_e]";
+        const std::string ld_k = coherent ? "__ldcg(" + ksrc + " + _e)" : ksrc + "[_e]";
+        cg.addLine("for (int _e = (int)threadIdx.x; _e < " + n + "; _e += 32) gpudb_topk_push<" + K + ">(_tk_v, _tk_k, " + ld_v +
+                   ", " + ld_k + ");");
+        cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
+    };
+    cg.addBlock("if (threadIdx.x < 32u)", [&]() {
+        warpMerge("_ts_v", "_ts_k", "(int)(blockDim.x >> 5) * " + K, false);
+        cg.addBlock("if (threadIdx.x == 0u)", [&]() {
+            cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { " + out_ + "_pvals[blockIdx.x * " + K + " + _q] = _tw_v[_q]; " +
+                       out_ + "_pkeys[blockIdx.x * " + K + " + _q] = _tw_k[_q]; }");
+            cg.addLine("__threadfence();");
+            cg.addLine("_t_last = (atomicAdd(" + out_ + "_ticket, 1u) == gridDim.x - 1u);");
+        });
+    });
+    cg.addLine("__syncthreads();");
+    cg.addBlock("if (_t_last && threadIdx.x < 32u)", [&]() {
+        cg.addLine("__threadfence();");
+        warpMerge(out_ + "_pvals", out_ + "_pkeys", "(int)gridDim.x * " + K, true);
+        cg.addBlock("if (threadIdx.x == 0u)", [&]() {
+            cg.addLine("unsigned long long _cnt = 0ull;");
+            cg.addBlock("for (int _q = 0; _q < " + K + "; ++_q)", [&]() {
+                cg.addLine("if (_tw_k[_q] == GPUDB_TOPK_NONE_KEY && _tw_v[_q] == GPUDB_TOPK_NONE_VAL) break;");
+                cg.addLine(out_ + "_vals[_q] = _tw_v[_q]; " + out_ + "_keys[_q] = _tw_k[_q]; ++_cnt;");
+            });
+            cg.addLine(out_ + "_count[0] = _cnt;");
+            cg.addLine(out_ + "_ticket[0] = 0u;  // self-reset for the next launch");
+        });
+    });
+    auto& rs = cg.resultSchema();
+    rs.kind = CudaResultSchema::TOPK;
+    rs.topk.keyBuffer = out_ + "_keys";
+    rs.topk.valueBuffer = out_ + "_vals";
+    rs.topk.countBuffer = out_ + "_count";
+    rs.topk.k = k_;
+}
+
+std::string CudaTopK::describe() const {
+    return "TopK(k=" + S(k_) + ", key=" + keyExpr_ + ", value=" + valueExpr_ + ") <- " + describeChain();
+}
+
+}  // namespace gpudb

@@ -1,0 +1,405 @@
+#pragma once
+// ===================================================================
+// CUDA operators — composable producer/consumer code generation.
+//
+// Same operator API as the reference (codegen/operators/metal_operators.h:
+// MetalOperator::produce(MetalCodegen&, ConsumerFn) :26-31): each operator's
+// produce() registers its parameters, emits code around its child's
+// produce() and wraps the consumer callback. Operators and their argument
+// meanings follow the reference one for one (Scan, Selection, ComputeExpr,
+// BitmapBuild/Probe/AntiProbe, ArrayStore/Lookup, TGReduce, KeyedAgg,
+// AtomicAgg, AtomicCount, Materialize); the emitted text is CUDA for
+// sm_100a. New operators the reference lacks: BufferScan, HashBuild,
+// HashProbe, HashGroupBy (GPU open addressing with 64-bit CAS) and TopK.
+//
+// Expressions are CUDA C++ strings over the column names, indexed by the
+// scan's index variable (default "i"), exactly like the reference's
+// exprToMetal output (metal_plan_builder.cpp:64-117). `_row` always holds
+// the global 64-bit row index.
+// ===================================================================
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../core/cuda_codegen.h"
+
+namespace gpudb {
+
+class CudaOperator {
+public:
+    virtual ~CudaOperator() = default;
+    virtual void produce(CudaCodegen& cg, ConsumerFn consume) = 0;
+    virtual std::string describe() const = 0;
+};
+
+class CudaUnaryOperator : public CudaOperator {
+protected:
+    std::unique_ptr<CudaOperator> child_;
+
+public:
+    explicit CudaUnaryOperator(std::unique_ptr<CudaOperator> child) : child_(std::move(child)) {}
+    std::string describeChain() const;
+};
+
+// How a scan moves column bytes from HBM to the row loop.
+struct ScanConfig {
+    enum Mode { Direct, TmaBulk };
+    Mode mode = TmaBulk;
+    int tileRows = 1024;   // rows per TMA tile (multiple of 16 and of the block size)
+    int stages = 4;        // TMA ring depth
+};
+
+// ------------------------------------------------------------------
+// Leaf: grid-stride / TMA-staged scan over a resident columnar table.
+// Reference: MetalGridStrideScan (metal_operators.cpp:28-49).
+// Direct mode emits the reference's grid-stride loop with 64-bit indices.
+// TmaBulk mode runs a persistent tile loop: thread 0 streams each tile's
+// columns into a shared-memory ring with cp.async.bulk (evict-first L2
+// hint, CTA-local destination only) signalled by per-stage mbarriers; all threads
+// consume rows from shared memory; rows of a partial last tile (and all
+// rows when a column is not 16-byte aligned) take the direct loop.
+// ------------------------------------------------------------------
+class CudaGridStrideScan : public CudaOperator {
+public:
+    struct ColumnDesc {
+        std::string paramName;
+        std::string cudaType;
+    };
+    CudaGridStrideScan(const std::string& table, const std::string& rowVar = "row",
+                       const std::string& idxVar = "i");
+    void addColumn(const std::string& paramName, const std::string& cudaType);
+    void setConfig(const ScanConfig& c) { cfg_ = c; }
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+    const std::string& tableName() const { return tableName_; }
+    const std::vector<ColumnDesc>& columns() const { return columns_; }
+
+private:
+    std::string tableName_, rowVar_, idxVar_;
+    std::vector<ColumnDesc> columns_;
+    ScanConfig cfg_;
+};
+
+// Leaf: grid-stride loop over executor buffers of `countExpr` elements
+// (e.g. the slots of a hash table). Consumers register the buffers.
+class CudaBufferScan : public CudaOperator {
+public:
+    CudaBufferScan(const std::string& countName, const std::string& countExpr, const std::string& idxVar = "i");
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string countName_, countExpr_, idxVar_;
+};
+
+// Selection: if (predicate) consume(). Reference: metal_operators.cpp:63-69.
+class CudaSelection : public CudaUnaryOperator {
+public:
+    CudaSelection(std::unique_ptr<CudaOperator> child, const std::string& predicate);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string predicate_;
+};
+
+// ComputeExpr: T var = expr; consume(). Reference: metal_operators.cpp:86-91.
+class CudaComputeExpr : public CudaUnaryOperator {
+public:
+    CudaComputeExpr(std::unique_ptr<CudaOperator> child, const std::string& varName, const std::string& varType,
+                    const std::string& expression);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string varName_, varType_, expression_;
+};
+
+// Bitmap build / probe / anti-probe over 32-bit words.
+// Reference: metal_operators.cpp:108-165. Optional counter of newly set
+// bits gives the exact number of distinct build keys (sizing pass).
+class CudaBitmapBuild : public CudaUnaryOperator {
+public:
+    CudaBitmapBuild(std::unique_ptr<CudaOperator> child, const std::string& bitmapName, const std::string& keyExpr,
+                    const std::string& sizeExpr);
+    void setDistinctCounter(const std::string& counterName) { counter_ = counterName; }
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string bitmapName_, keyExpr_, sizeExpr_, counter_;
+};
+
+class CudaBitmapProbe : public CudaUnaryOperator {
+public:
+    CudaBitmapProbe(std::unique_ptr<CudaOperator> child, const std::string& bitmapName, const std::string& keyExpr,
+                    bool anti = false);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string bitmapName_, keyExpr_;
+    bool anti_;
+};
+
+class CudaAntiBitmapProbe : public CudaBitmapProbe {
+public:
+    CudaAntiBitmapProbe(std::unique_ptr<CudaOperator> child, const std::string& bitmapName,
+                        const std::string& keyExpr)
+        : CudaBitmapProbe(std::move(child), bitmapName, keyExpr, true) {}
+};
+
+// Direct-address maps. Reference: metal_operators.cpp:185-225 (0xFF fill =
+// sentinel -1 for int maps).
+class CudaArrayStore : public CudaUnaryOperator {
+public:
+    CudaArrayStore(std::unique_ptr<CudaOperator> child, const std::string& arrayName, const std::string& keyExpr,
+                   const std::string& valueExpr, const std::string& valueType = "int",
+                   const std::string& sizeExpr = "");
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string arrayName_, keyExpr_, valueExpr_, valueType_, sizeExpr_;
+};
+
+class CudaArrayLookup : public CudaUnaryOperator {
+public:
+    CudaArrayLookup(std::unique_ptr<CudaOperator> child, const std::string& arrayName, const std::string& keyExpr,
+                    const std::string& resultVar, const std::string& resultType = "int", long long sentinel = -1);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string arrayName_, keyExpr_, resultVar_, resultType_;
+    long long sentinel_;
+};
+
+// ------------------------------------------------------------------
+// Scalar reduction. Reference: MetalTGReduce (metal_operators.cpp:258-346):
+// per-thread local sums, SIMD + threadgroup reduce, one atomic per TG.
+// Here: per-thread int64, warp shuffle + smem block reduce, then one
+// global RED per accumulator per block ("wide" = exact 128-bit split
+// pair, "long" = one 64-bit word).
+// ------------------------------------------------------------------
+class CudaTGReduce : public CudaUnaryOperator {
+public:
+    struct Accumulator {
+        std::string name, buffer, valueExpr, type;  // type: "wide" | "long" | "umax"
+    };
+    CudaTGReduce(std::unique_ptr<CudaOperator> child, const std::string& outputPrefix);
+    void addAccumulator(const std::string& name, const std::string& valueExpr, const std::string& type = "wide",
+                        const std::string& buffer = "");
+    void setResultAlias(const std::string& displayName, int scaleDown = 0);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string outputPrefix_;
+    std::vector<Accumulator> accumulators_;
+    struct ResultInfo {
+        std::string displayName;
+        int scaleDown = 0;
+    };
+    std::vector<ResultInfo> resultInfos_;
+};
+
+// ------------------------------------------------------------------
+// Few-group keyed aggregation. Reference: MetalKeyedAgg
+// (metal_operators.cpp:375-502): thread-local arrays + TG reduction when
+// all aggregates are adds and buckets <= 64, else per-row atomics.
+// Here three strategies, chosen by size:
+//   registers : buckets*aggs <= 64 — per-thread register accumulators
+//               updated branch-free (predicated on the bucket id), block
+//               reduce, one RED per non-zero (bucket, agg) per block;
+//   shared    : buckets*valuesPerBucket <= 16384 words — per-block smem
+//               table with shared 64-bit atomics, flushed non-zero words;
+//   global    : per-row global atomics (add / min / max).
+// Output: numBuckets x valuesPerBucket u64 words; a "wide" aggregate
+// occupies words offset and offset+1 (exact 128-bit split pair).
+// ------------------------------------------------------------------
+class CudaKeyedAgg : public CudaUnaryOperator {
+public:
+    struct Aggregate {
+        std::string name;
+        int offset = 0;
+        std::string valueExpr;
+        std::string atomicOp;  // add | min | max
+        bool isWide = false;
+        int scaleDown = 0;
+    };
+    enum class Strategy { Auto, Registers, Shared, Global };
+    CudaKeyedAgg(std::unique_ptr<CudaOperator> child, const std::string& outputArrayName,
+                 const std::string& bucketExpr, int numBuckets, int valuesPerBucket,
+                 const std::string& sizeExpr = "");
+    void addAggregate(const std::string& name, int offset, const std::string& valueExpr,
+                      const std::string& atomicOp = "add", bool isWide = false, int scaleDown = 0);
+    void setStrategy(Strategy s) { strategy_ = s; }
+    Strategy chosenStrategy() const;
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string outputArrayName_, bucketExpr_;
+    int numBuckets_, valuesPerBucket_;
+    std::string sizeExpr_;
+    std::vector<Aggregate> aggregates_;
+    Strategy strategy_ = Strategy::Auto;
+};
+
+// ------------------------------------------------------------------
+// Direct-address atomic aggregation. Reference: MetalAtomicAgg
+// (metal_operators.cpp:525-533). Options for skew: warp aggregation of
+// equal buckets (__match_any_sync + peer tree sum, one atomic per distinct
+// bucket per warp) and a per-block shared-memory cache of hot buckets.
+// ------------------------------------------------------------------
+class CudaAtomicAgg : public CudaUnaryOperator {
+public:
+    CudaAtomicAgg(std::unique_ptr<CudaOperator> child, const std::string& arrayName, const std::string& bucketExpr,
+                  const std::string& valueExpr, const std::string& sizeExpr = "",
+                  const std::string& elemType = "unsigned long long");
+    // Further arrays updated at the same bucket (share warp aggregation
+    // and the shared-memory cache), e.g. a count beside a sum.
+    void addAggregate(const std::string& arrayName, const std::string& valueExpr);
+    void setWarpAggregate(bool on) { warpAgg_ = on; }
+    void setSharedCache(int log2Slots) { smemLog2_ = log2Slots; }
+    void setZeroInit(bool on) { zeroInit_ = on; }
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string arrayName_, bucketExpr_, valueExpr_, sizeExpr_, elemType_;
+    std::vector<std::pair<std::string, std::string>> extra_;
+    bool warpAgg_ = false;
+    int smemLog2_ = 0;
+    bool zeroInit_ = true;
+};
+
+// Histogram. Reference: MetalAtomicCount (metal_operators.cpp:550-594):
+// TG-local histogram when the static size is <= 256. Here <= 8192 bins go
+// to a shared-memory histogram flushed non-zero bins.
+class CudaAtomicCount : public CudaUnaryOperator {
+public:
+    CudaAtomicCount(std::unique_ptr<CudaOperator> child, const std::string& arrayName,
+                    const std::string& bucketExpr, const std::string& sizeExpr = "");
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string arrayName_, bucketExpr_, sizeExpr_;
+};
+
+// Materialize selected rows. Reference: MetalMaterialize
+// (metal_operators.cpp:618-643, one atomic per row). Here positions are
+// reserved per warp from a ballot of the selection (one atomic per warp);
+// rows beyond the capacity raise GPUDB_ERR_CAPACITY and are dropped.
+class CudaMaterialize : public CudaUnaryOperator {
+public:
+    struct Column {
+        std::string arrayName, type, valueExpr, displayName;
+    };
+    CudaMaterialize(std::unique_ptr<CudaOperator> child, const std::string& counterName,
+                    const std::string& capacityExpr);
+    void addColumn(const std::string& arrayName, const std::string& type, const std::string& valueExpr,
+                   const std::string& displayName = "");
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string counterName_, capacityExpr_;
+    std::vector<Column> columns_;
+};
+
+// ------------------------------------------------------------------
+// GPU hash tables (new; the reference builds its tables on the host).
+// ------------------------------------------------------------------
+enum class HashLayout { Linear, Bucket8 };
+
+// Slot count / log2 of a hash table requested with `capacityExpr` slots:
+// rounded up to a power of two, at least 16 (one bucket8 group twice).
+std::string hashSlotsExpr(const std::string& capacityExpr);
+std::string hashLog2Expr(const std::string& capacityExpr);
+
+// Build: insert keyExpr (64-bit or 32-bit keys) and store payloads at the
+// key's slot. Capacity is a power of two (sizeExpr rounded up).
+class CudaHashBuild : public CudaUnaryOperator {
+public:
+    CudaHashBuild(std::unique_ptr<CudaOperator> child, const std::string& tableName, const std::string& keyExpr,
+                  const std::string& keyType, const std::string& capacityExpr, HashLayout layout = HashLayout::Linear,
+                  int maxProbe = 128);
+    void addPayload(const std::string& column, const std::string& type, const std::string& valueExpr);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    struct Payload {
+        std::string column, type, valueExpr;
+    };
+    std::string table_, keyExpr_, keyType_, capExpr_;
+    HashLayout layout_;
+    int maxProbe_;
+    std::vector<Payload> payloads_;
+};
+
+// Probe: long long slotVar = find(keyExpr); if (slotVar >= 0) consume().
+class CudaHashProbe : public CudaUnaryOperator {
+public:
+    CudaHashProbe(std::unique_ptr<CudaOperator> child, const std::string& tableName, const std::string& keyExpr,
+                  const std::string& keyType, const std::string& capacityExpr, const std::string& slotVar = "_slot",
+                  HashLayout layout = HashLayout::Linear, int maxProbe = 128);
+    void addPayloadRead(const std::string& column, const std::string& type);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string table_, keyExpr_, keyType_, capExpr_, slotVar_;
+    HashLayout layout_;
+    int maxProbe_;
+    std::vector<std::pair<std::string, std::string>> payloadReads_;
+};
+
+// High-cardinality hash group-by with 64-bit sums / counts per group.
+// Options: warp aggregation (match_any on the key) and a per-block
+// shared-memory table (2^log2 slots) absorbing heavy hitters before the
+// global table; the block flushes it at the end.
+class CudaHashGroupBy : public CudaUnaryOperator {
+public:
+    CudaHashGroupBy(std::unique_ptr<CudaOperator> child, const std::string& tableName, const std::string& keyExpr,
+                    const std::string& keyType, const std::string& capacityExpr,
+                    HashLayout layout = HashLayout::Linear, int maxProbe = 128);
+    void addAggregate(const std::string& name, const std::string& valueExpr);  // "1" = count
+    void setWarpAggregate(bool on) { warpAgg_ = on; }
+    void setSharedPreAgg(int log2Slots) { smemLog2_ = log2Slots; }
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    struct Agg {
+        std::string name, valueExpr;
+    };
+    std::string table_, keyExpr_, keyType_, capExpr_;
+    HashLayout layout_;
+    int maxProbe_;
+    std::vector<Agg> aggs_;
+    bool warpAgg_ = true;
+    int smemLog2_ = 0;
+};
+
+// Top-k (value desc, key asc) of the consumed (key, value) pairs.
+// Per-thread register lists, warp shuffle merge, block merge in smem,
+// last-block-done merge of the per-block lists (one launch).
+// Reference: host top-k in codegen_main.cpp:1211-1248.
+class CudaTopK : public CudaUnaryOperator {
+public:
+    CudaTopK(std::unique_ptr<CudaOperator> child, const std::string& outPrefix, const std::string& keyExpr,
+             const std::string& valueExpr, int k, int maxBlocks = 296);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string out_, keyExpr_, valueExpr_;
+    int k_, maxBlocks_;
+};
+
+}  // namespace gpudb

@@ -1,0 +1,508 @@
+#include "plan_builder.h"
+
+#include <set>
+#include <sstream>
+#include <stdexcept>
+
+namespace gpudb {
+
+// ===================================================================
+// Catalog
+// ===================================================================
+namespace {
+
+std::vector<TableDef> buildCatalog() {
+    return {
+        // Fact table (lineitem role): config-0 schema.
+        {"fact",
+         {{"f_ship_day", "int"},
+          {"f_quantity", "long long"},
+          {"f_price", "long long"},
+          {"f_discount", "long long"},
+          {"f_tax", "long long"},
+          {"f_flag_a", "unsigned char"},
+          {"f_flag_b", "unsigned char"}}},
+        // Build side (orders role): unique int keys.
+        {"dim", {{"b_key", "int"}, {"b_order_day", "int"}, {"b_segment", "unsigned char"}}},
+        // Probe side (lineitem role for the join).
+        {"probe", {{"p_fk", "int"}, {"p_ship_day", "int"}, {"p_price", "long long"}, {"p_discount", "long long"}}},
+        // Skewed-key probe / group-by input.
+        {"zprobe", {{"z_key", "long long"}, {"z_value", "long long"}}},
+        // Skewed-key build side: every distinct key once.
+        {"zbuild", {{"zb_key", "long long"}, {"zb_payload", "int"}}},
+        // Mixed-workload table: keys by rank (uniform / Zipf), filter, value.
+        {"mix",
+         {{"m_rank_u", "int"},
+          {"m_rank_z", "int"},
+          {"m_filter", "int"},
+          {"m_value", "long long"},
+          {"m_fk", "int"}}},
+        // Mixed-workload dimension (join-agg build side).
+        {"mixdim", {{"md_key", "int"}, {"md_attr", "int"}}},
+    };
+}
+
+const std::vector<TableDef>& catalog() {
+    static const std::vector<TableDef> c = buildCatalog();
+    return c;
+}
+
+}  // namespace
+
+const ColumnDef& TableDef::col(const std::string& n) const {
+    for (const auto& c : columns)
+        if (c.name == n) return c;
+    throw std::runtime_error("catalog: table '" + name + "' has no column '" + n + "'");
+}
+
+const TableDef& catalogTable(const std::string& table) {
+    for (const auto& t : catalog())
+        if (t.name == table) return t;
+    throw std::runtime_error("catalog: unknown table '" + table + "'");
+}
+
+std::vector<std::string> catalogTables() {
+    std::vector<std::string> out;
+    for (const auto& t : catalog()) out.push_back(t.name);
+    return out;
+}
+
+// ===================================================================
+// Spec / tune parsing
+// ===================================================================
+SpecMap parseSpec(const std::string& spec) {
+    SpecMap m;
+    std::stringstream ss(spec);
+    std::string item;
+    while (std::getline(ss, item, ';')) {
+        const auto b = item.find_first_not_of(" \t");
+        if (b == std::string::npos) continue;
+        item = item.substr(b, item.find_last_not_of(" \t") - b + 1);
+        const auto eq = item.find('=');
+        if (eq == std::string::npos) throw std::runtime_error("spec: expected key=value, got '" + item + "'");
+        m[item.substr(0, eq)] = item.substr(eq + 1);
+    }
+    return m;
+}
+
+std::string canonicalSpec(const SpecMap& m) {
+    std::string s;
+    for (const auto& [k, v] : m) s += (s.empty() ? "" : ";") + k + "=" + v;
+    return s;
+}
+
+std::string TuneConfig::toString() const {
+    std::ostringstream o;
+    o << "bs=" << blockSize << ";scan=" << (scan.mode == ScanConfig::TmaBulk ? "tma" : "direct")
+      << ";tile=" << scan.tileRows << ";stages=" << scan.stages
+      << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
+      << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe;
+    return o.str();
+}
+
+TuneConfig TuneConfig::parse(const std::string& s) {
+    TuneConfig t;
+    for (const auto& [k, v] : parseSpec(s)) {
+        if (k == "bs") t.blockSize = std::stoi(v);
+        else if (k == "scan") {
+            if (v == "tma") t.scan.mode = ScanConfig::TmaBulk;
+            else if (v == "direct") t.scan.mode = ScanConfig::Direct;
+            else throw std::runtime_error("tune: scan must be tma|direct");
+        } else if (k == "tile") t.scan.tileRows = std::stoi(v);
+        else if (k == "stages") t.scan.stages = std::stoi(v);
+        else if (k == "layout") {
+            if (v == "linear") t.hashLayout = HashLayout::Linear;
+            else if (v == "bucket8") t.hashLayout = HashLayout::Bucket8;
+            else throw std::runtime_error("tune: layout must be linear|bucket8");
+        } else if (k == "smem") t.smemPreAggLog2 = std::stoi(v);
+        else if (k == "warp") t.warpAggregate = std::stoi(v) != 0;
+        else if (k == "keyed") t.keyedStrategy = std::stoi(v);
+        else if (k == "probe") t.maxProbe = std::stoi(v);
+        else throw std::runtime_error("tune: unknown key '" + k + "'");
+    }
+    if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
+        throw std::runtime_error("tune: bs must be a multiple of 32 in [32,1024]");
+    if (t.scan.tileRows % t.blockSize) t.scan.tileRows = ((t.scan.tileRows + t.blockSize - 1) / t.blockSize) * t.blockSize;
+    return t;
+}
+
+// ===================================================================
+// Builders
+// ===================================================================
+namespace {
+
+struct Spec {
+    SpecMap m;
+    std::set<std::string> used;
+    std::string str(const std::string& k, const std::string& def) {
+        used.insert(k);
+        auto it = m.find(k);
+        return it == m.end() ? def : it->second;
+    }
+    long long num(const std::string& k, long long def) {
+        used.insert(k);
+        auto it = m.find(k);
+        if (it == m.end()) return def;
+        size_t p = 0;
+        long long v = std::stoll(it->second, &p);
+        if (p != it->second.size()) throw std::runtime_error("spec: '" + k + "' is not an integer");
+        return v;
+    }
+    bool has(const std::string& k) const { return m.count(k) != 0; }
+    void finish() {
+        for (const auto& [k, v] : m)
+            if (!used.count(k)) throw std::runtime_error("spec: unknown key '" + k + "' for this template");
+    }
+};
+
+std::string L(long long v) { return std::to_string(v) + "ll"; }
+
+std::unique_ptr<CudaGridStrideScan> makeScan(CudaQueryPlan& plan, const std::string& table,
+                                             const std::vector<std::string>& cols, const TuneConfig& tune,
+                                             bool allowTma = true) {
+    const TableDef& td = catalogTable(table);
+    auto scan = std::make_unique<CudaGridStrideScan>(table, "row", "i");
+    for (const auto& c : cols) scan->addColumn(c, td.col(c).cudaType);
+    ScanConfig sc = tune.scan;
+    if (!allowTma) sc.mode = ScanConfig::Direct;
+    scan->setConfig(sc);
+    bool seen = false;
+    for (const auto& t : plan.tables) seen |= (t == table);
+    if (!seen) plan.tables.push_back(table);
+    return scan;
+}
+
+CudaQueryPlan::Phase& appendPhase(CudaQueryPlan& plan, const std::string& name, std::unique_ptr<CudaOperator> root,
+                                  const TuneConfig& tune) {
+    CudaQueryPlan::Phase ph;
+    ph.name = name;
+    ph.root = std::move(root);
+    ph.threadgroupSize = tune.blockSize;
+    plan.phases.push_back(std::move(ph));
+    return plan.phases.back();
+}
+
+// ---- q1: scan -> filter -> few-group aggregate (reference buildQ1Plan,
+// metal_plan_builder.cpp:309-354). Buckets follow the reference's order:
+// (flag_a=='A'?0 : flag_a=='N'?2 : 4) + (flag_b=='F'?0:1).
+CudaQueryPlan buildQ1(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "Q1";
+    const long long shipLe = s.num("ship_le", 2436);
+    const std::string i = "i";
+    auto scan = makeScan(plan, "fact",
+                         {"f_ship_day", "f_quantity", "f_price", "f_discount", "f_tax", "f_flag_a", "f_flag_b"}, tune);
+    auto filtered = std::make_unique<CudaSelection>(std::move(scan), "f_ship_day[i] <= " + std::to_string(shipLe));
+    const std::string bucket =
+        "((f_flag_a[i] == 'A' ? 0 : (f_flag_a[i] == 'N' ? 2 : 4)) + (f_flag_b[i] == 'F' ? 0 : 1))";
+    auto agg = std::make_unique<CudaKeyedAgg>(std::move(filtered), "d_q1_aggs", bucket, 6, 7, "42");
+    agg->addAggregate("sum_qty", 0, "f_quantity[i]", "add", false);
+    agg->addAggregate("sum_base_price", 1, "f_price[i]", "add", false);
+    agg->addAggregate("sum_disc_price", 2, "f_price[i] * (100ll - f_discount[i])", "add", false);
+    agg->addAggregate("sum_charge", 3, "f_price[i] * (100ll - f_discount[i]) * (100ll + f_tax[i])", "add", true);
+    agg->addAggregate("sum_disc", 5, "f_discount[i]", "add", false);
+    agg->addAggregate("count_order", 6, "1", "add", false);
+    if (tune.keyedStrategy) agg->setStrategy((CudaKeyedAgg::Strategy)tune.keyedStrategy);
+    appendPhase(plan, "Q1_reduce", std::move(agg), tune);
+    plan.chunkable = true;
+    plan.decorate.push_back([](CudaResultSchema& rs) {
+        rs.keyedAgg.keys = {{"flag_a", 2, 3, {"A", "N", "R"}}, {"flag_b", 1, 2, {"F", "O"}}};
+        rs.keyedAgg.derived = {{"avg_qty", "sum_qty", "count_order"},
+                               {"avg_price", "sum_base_price", "count_order"},
+                               {"avg_disc", "sum_disc", "count_order"}};
+    });
+    return plan;
+}
+
+// ---- q6: scan -> filter -> scalar sum (reference buildQ6Plan,
+// metal_plan_builder.cpp:253-303).
+CudaQueryPlan buildQ6(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "Q6";
+    const long long ge = s.num("ship_ge", 365), lt = s.num("ship_lt", 730);
+    const long long dlo = s.num("disc_lo", 5), dhi = s.num("disc_hi", 7), qlt = s.num("qty_lt", 24);
+    auto scan = makeScan(plan, "fact", {"f_ship_day", "f_quantity", "f_price", "f_discount"}, tune);
+    const std::string pred = "(f_ship_day[i] >= " + std::to_string(ge) + " && f_ship_day[i] < " + std::to_string(lt) +
+                             ") && (f_discount[i] >= " + L(dlo) + " && f_discount[i] <= " + L(dhi) +
+                             ") && (f_quantity[i] < " + L(qlt) + ")";
+    auto filtered = std::make_unique<CudaSelection>(std::move(scan), pred);
+    auto reduce = std::make_unique<CudaTGReduce>(std::move(filtered), "d_q6");
+    reduce->addAccumulator("revenue", "f_price[i] * f_discount[i]", "wide");
+    reduce->setResultAlias("revenue", 0);
+    appendPhase(plan, "Q6_reduce", std::move(reduce), tune);
+    plan.chunkable = true;
+    return plan;
+}
+
+// ---- join_topk: bitmap semi-join build -> probe + hash group-by ->
+// top-k (reference Q3 shape: metal_plan_builder.cpp:1170-1239 + host top-k
+// codegen_main.cpp:1211-1248). The build's distinct counter is the exact
+// sizing pass for the group table; `groups=N` supplies it instead.
+CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "JOIN_TOPK";
+    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
+    const long long k = s.num("k", 10);
+    const bool given = s.has("groups");
+    const long long groups = s.num("groups", 0);
+    {
+        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
+                                                                      " && b_order_day[i] < " + std::to_string(odLt));
+        auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "jb_bitmap", "b_key[i]", "max_b_key / 32 + 1");
+        bm->setDistinctCounter("jb_distinct");
+        appendPhase(plan, "JT_build", std::move(bm), tune);
+    }
+    const std::string cap = "2 * max(jt_groups, 1)";
+    {
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day", "p_price", "p_discount"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
+        auto gb = std::make_unique<CudaHashGroupBy>(std::move(pr), "jg", "p_fk[i]", "int", cap, HashLayout::Linear,
+                                                    tune.maxProbe);
+        gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
+        gb->setWarpAggregate(tune.warpAggregate);
+        appendPhase(plan, "JT_probe_group", std::move(gb), tune);
+    }
+    {
+        auto bscan = std::make_unique<CudaBufferScan>("n_jg_slots", hashSlotsExpr(cap));
+        auto f = std::make_unique<CudaSelection>(std::move(bscan), "jg_keys[i] != GPUDB_EMPTY32");
+        auto tk = std::make_unique<CudaTopK>(std::move(f), "jt_top", "(long long)(int)jg_keys[i]",
+                                             "(long long)jg_revenue[i]", (int)k);
+        auto& ph = appendPhase(plan, "JT_topk", std::move(tk), tune);
+        ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});
+        ph.extraBuffers.push_back({"jg_revenue", "unsigned long long", true, false});
+    }
+    CudaQueryPlan::SizingStep st;
+    st.symbol = "jt_groups";
+    st.afterPhase = 1;
+    if (given) st.fallbackExpr = std::to_string(groups);
+    else st.counterBuffer = "jb_distinct";
+    plan.sizing.push_back(st);
+    plan.decorate.push_back([](CudaResultSchema& rs) {
+        rs.topk.keyName = "key";
+        rs.topk.valueName = "revenue";
+    });
+    plan.cpuSort = CudaQueryPlan::CpuSort{{{"revenue", true}, {"key", false}}, (int)k};
+    return plan;
+}
+
+// ---- groupby: high-cardinality hash group-by, count + sum (reference
+// Q18 shape metal_plan_builder.cpp:1529-1545, which aggregates into a
+// direct-address array; here an open-addressing table keyed by int64).
+CudaQueryPlan buildGroupBy(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "GROUPBY";
+    const std::string groupsExpr = s.str("groups", "zgroups");
+    auto scan = makeScan(plan, "zprobe", {"z_key", "z_value"}, tune);
+    auto gb = std::make_unique<CudaHashGroupBy>(std::move(scan), "zg", "z_key[i]", "long long",
+                                                "2 * (" + groupsExpr + ")", tune.hashLayout, tune.maxProbe);
+    gb->addAggregate("count", "1");
+    gb->addAggregate("sum", "z_value[i]");
+    gb->setWarpAggregate(tune.warpAggregate);
+    gb->setSharedPreAgg(tune.smemPreAggLog2);
+    appendPhase(plan, "GB_aggregate", std::move(gb), tune);
+    return plan;
+}
+
+// ---- hashjoin: GPU hash build (64-bit CAS) -> probe -> per-key sum of
+// the build payload over matches (reference Q9/Q20 hash tables:
+// query_preprocessing.cpp:352-386/443-479 built on the host, probed by
+// metal_plan_builder.cpp:1598-1610/1968-1982).
+CudaQueryPlan buildHashJoin(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "HASHJOIN";
+    (void)s;
+    const std::string cap = "2 * n_zbuild";
+    {
+        auto scan = makeScan(plan, "zbuild", {"zb_key", "zb_payload"}, tune);
+        auto hb = std::make_unique<CudaHashBuild>(std::move(scan), "hj", "zb_key[i]", "long long", cap, tune.hashLayout,
+                                                  tune.maxProbe);
+        hb->addPayload("payload", "int", "zb_payload[i]");
+        appendPhase(plan, "HJ_build", std::move(hb), tune);
+    }
+    {
+        auto scan = makeScan(plan, "zprobe", {"z_key"}, tune);
+        auto pr = std::make_unique<CudaHashProbe>(std::move(scan), "hj", "z_key[i]", "long long", cap, "_slot",
+                                                  tune.hashLayout, tune.maxProbe);
+        pr->addPayloadRead("payload", "int");
+        auto ag = std::make_unique<CudaAtomicAgg>(std::move(pr), "hj_sum", "_slot", "(long long)hj_payload[_slot]",
+                                                  hashSlotsExpr(cap));
+        ag->addAggregate("hj_count", "1");
+        ag->setWarpAggregate(tune.warpAggregate);
+        ag->setSharedCache(tune.smemPreAggLog2);
+        auto& ph = appendPhase(plan, "HJ_probe_sum", std::move(ag), tune);
+        ph.extraBuffers.push_back({"hj_keys", "unsigned long long", true, false});
+    }
+    plan.decorate.push_back([cap](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::HASH_AGG;
+        rs.hashAgg.keyBuffer = "hj_keys";
+        rs.hashAgg.keyType = "unsigned long long";
+        rs.hashAgg.capacitySymbol = hashSlotsExpr(cap);
+        rs.hashAgg.aggs = {{"count", "hj_count"}, {"sum", "hj_sum"}};
+    });
+    return plan;
+}
+
+// ---- colmax: exact max of an integer column (the reference's max-key
+// sizing pass, max_key_symbols.cpp:188-235, run on the GPU).
+CudaQueryPlan buildColMax(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    const std::string table = s.str("table", "");
+    const std::string col = s.str("col", "");
+    plan.name = "COLMAX";
+    auto scan = makeScan(plan, table, {col}, tune);
+    // max over signed values as an unsigned max of (v ^ sign bit); the
+    // zero fill of the output word is then the identity.
+    auto r = std::make_unique<CudaTGReduce>(std::move(scan), "d_colmax");
+    r->addAccumulator("max_biased", "(unsigned long long)(long long)" + col + "[i] ^ 0x8000000000000000ull", "umax");
+    auto ag = std::move(r);
+    appendPhase(plan, "COLMAX_" + col, std::move(ag), tune);
+    return plan;
+}
+
+// ---- distinct: exact distinct count of (key % card) over rows passing a
+// filter; the exact count pass of the mixed group-by templates.
+CudaQueryPlan buildDistinct(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "DISTINCT";
+    const std::string keyCol = s.str("key", "m_rank_u");
+    const long long card = s.num("card", 1024), thr = s.num("thr", 10000);
+    auto scan = makeScan(plan, "mix", {keyCol, "m_filter"}, tune);
+    auto f = std::make_unique<CudaSelection>(std::move(scan), "m_filter[i] < " + std::to_string(thr));
+    auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "dc_bitmap", "(long long)" + keyCol + "[i] % " + L(card),
+                                                std::to_string(card / 32 + 1));
+    bm->setDistinctCounter("dc_distinct");
+    appendPhase(plan, "DC_count", std::move(bm), tune);
+    plan.decorate.push_back([](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::SCALAR_AGG;
+        rs.scalarAggs = {{"distinct", "dc_distinct", false, 0}};
+    });
+    return plan;
+}
+
+// ---- mixed-workload templates (batched mixed-query form) ----------------
+// mix_agg:     filter -> count + sum(value)
+// mix_groupby: filter -> hash group-by on (rank % card): count + sum
+// mix_topk:    mix_groupby -> top-k groups by sum
+// mix_join:    bitmap semi-join on fk against mixdim(attr < a) -> count + sum
+CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = tmpl;
+    const long long thr = s.num("thr", 10000);
+    const std::string filt = "m_filter[i] < " + std::to_string(thr);
+    if (tmpl == "mix_agg") {
+        auto scan = makeScan(plan, "mix", {"m_filter", "m_value"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
+        auto r = std::make_unique<CudaTGReduce>(std::move(f), "d_mix");
+        r->addAccumulator("count", "1", "long");
+        r->addAccumulator("sum", "m_value[i]", "wide");
+        appendPhase(plan, "MIX_agg", std::move(r), tune);
+        return plan;
+    }
+    if (tmpl == "mix_join") {
+        const long long attrLt = s.num("attr_lt", 500);
+        {
+            auto scan = makeScan(plan, "mixdim", {"md_key", "md_attr"}, tune);
+            auto f = std::make_unique<CudaSelection>(std::move(scan), "md_attr[i] < " + std::to_string(attrLt));
+            auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "mj_bitmap", "md_key[i]", "max_md_key / 32 + 1");
+            appendPhase(plan, "MIXJ_build", std::move(bm), tune);
+        }
+        auto scan = makeScan(plan, "mix", {"m_fk", "m_filter", "m_value"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
+        auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "mj_bitmap", "m_fk[i]");
+        auto r = std::make_unique<CudaTGReduce>(std::move(pr), "d_mixj");
+        r->addAccumulator("count", "1", "long");
+        r->addAccumulator("sum", "m_value[i]", "wide");
+        appendPhase(plan, "MIXJ_probe", std::move(r), tune);
+        return plan;
+    }
+    const std::string keyCol = s.str("key", "m_rank_u");
+    const long long card = s.num("card", 1024);
+    const long long k = s.num("k", 10);
+    const std::string groups = s.str("groups", "mix_groups");
+    const std::string cap = "2 * max(" + groups + ", 1)";
+    auto scan = makeScan(plan, "mix", {keyCol, "m_filter", "m_value"}, tune);
+    auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
+    auto gb = std::make_unique<CudaHashGroupBy>(std::move(f), "mg", "(long long)" + keyCol + "[i] % " + L(card),
+                                                "long long", cap, tune.hashLayout, tune.maxProbe);
+    gb->addAggregate("count", "1");
+    gb->addAggregate("sum", "m_value[i]");
+    gb->setWarpAggregate(tune.warpAggregate);
+    gb->setSharedPreAgg(tune.smemPreAggLog2);
+    appendPhase(plan, "MIXG_group", std::move(gb), tune);
+    if (tmpl == "mix_topk") {
+        auto bscan = std::make_unique<CudaBufferScan>("n_mg_slots", hashSlotsExpr(cap));
+        auto sel = std::make_unique<CudaSelection>(std::move(bscan), "mg_keys[i] != GPUDB_EMPTY64");
+        auto tk = std::make_unique<CudaTopK>(std::move(sel), "mt_top", "(long long)mg_keys[i]", "(long long)mg_sum[i]",
+                                             (int)k);
+        auto& ph = appendPhase(plan, "MIXG_topk", std::move(tk), tune);
+        ph.extraBuffers.push_back({"mg_keys", "unsigned long long", true, false});
+        ph.extraBuffers.push_back({"mg_sum", "unsigned long long", true, false});
+        plan.decorate.push_back([](CudaResultSchema& rs) { rs.topk.valueName = "sum"; });
+    }
+    return plan;
+}
+
+}  // namespace
+
+std::vector<std::string> planTemplates() {
+    return {"q1", "q6", "join_topk", "groupby", "hashjoin", "colmax", "distinct",
+            "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
+}
+
+CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) {
+    Spec s{parseSpec(specStr), {}};
+    const std::string tmpl = s.str("template", "");
+    CudaQueryPlan plan;
+    if (tmpl == "q1" || tmpl == "scan_filter_groupagg") plan = buildQ1(s, tune);
+    else if (tmpl == "q6" || tmpl == "scan_filter_sum") plan = buildQ6(s, tune);
+    else if (tmpl == "join_topk") plan = buildJoinTopK(s, tune);
+    else if (tmpl == "groupby") plan = buildGroupBy(s, tune);
+    else if (tmpl == "hashjoin") plan = buildHashJoin(s, tune);
+    else if (tmpl == "colmax") plan = buildColMax(s, tune);
+    else if (tmpl == "distinct") plan = buildDistinct(s, tune);
+    else if (tmpl == "mix_agg" || tmpl == "mix_groupby" || tmpl == "mix_topk" || tmpl == "mix_join")
+        plan = buildMix(tmpl, s, tune);
+    else throw std::runtime_error("buildCudaPlan: unknown template '" + tmpl + "'");
+    s.finish();
+    plan.spec = canonicalSpec(s.m);
+    return plan;
+}
+
+CudaCodegen generateFromPlan(const CudaQueryPlan& plan) {
+    CudaCodegen cg;
+    for (const auto& h : plan.helpers) cg.addHelper(h);
+    for (const auto& ph : plan.phases) {
+        cg.beginPhase(ph.name);
+        cg.setPhaseThreadgroupSize(ph.threadgroupSize);
+        cg.setPhaseSingleThread(ph.singleThread);
+        cg.setPhaseMinBlocksPerSM(ph.minBlocksPerSM);
+        for (const auto& [n, sz] : ph.bitmapReads) cg.addBitmapReadParam(n, sz);
+        for (const auto& [n, t] : ph.scalarParams) cg.addScalarParam(n, t);
+        for (const auto& eb : ph.extraBuffers) {
+            if (eb.readOnly) cg.addReadBufferParam(eb.name, eb.type);
+            else cg.addBufferParam(eb.name, eb.type, "", eb.zeroInit);
+        }
+        if (ph.root) ph.root->produce(cg, []() {});
+        cg.endPhase();
+    }
+    for (const auto& d : plan.decorate) d(cg.resultSchema());
+    return cg;
+}
+
+long long planAlgorithmicBytes(const CudaQueryPlan& plan, const std::map<std::string, long long>& rows) {
+    CudaCodegen cg = generateFromPlan(plan);
+    long long bytes = 0;
+    for (const auto& ph : cg.getPhases()) {
+        std::set<std::string> seen;
+        for (const auto& b : ph.bindings) {
+            if (b.kind != CudaParamKind::TableData || !seen.insert(b.name).second) continue;
+            auto it = rows.find(b.tableName);
+            if (it != rows.end()) bytes += it->second * (long long)b.elemSizeBytes();
+        }
+    }
+    return bytes;
+}
+
+}  // namespace gpudb

@@ -1,0 +1,127 @@
+#pragma once
+// ===================================================================
+// Query plans and plan builders.
+//
+// CudaQueryPlan mirrors the reference's MetalQueryPlan
+// (codegen/planning/metal_plan_builder.h:22-68): an ordered list of phases,
+// each one operator tree = one kernel, plus helpers, the chunkable flag and
+// the CPU post-sort descriptor. B200 additions:
+//   * `sizing`: symbols a later phase's buffers depend on, produced by an
+//     earlier phase (exact count pass) or supplied by the caller (learned
+//     sizer); the driver splits execution at `afterPhase`.
+//   * `decorate`: post-generation edits of the result schema (group-key
+//     labels, FP64 derived columns).
+//
+// The reference builds plans from an AnalyzedQuery produced by its SQL
+// front end (buildMetalPlan, metal_plan_builder.cpp:2035); the SQL parser
+// is out of scope here, so plans are built from a `key=value;...` spec
+// naming a pipeline template and its constants (buildCudaPlan).
+// ===================================================================
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <optional>
+#include <string>
+#include <vector>
+
+#include "../operators/cuda_operators.h"
+
+namespace gpudb {
+
+// ------------------------------------------------------------------
+// Synthetic schema catalog (the role of tpch_schema.h for the workloads
+// this backend is measured on). Decimals are scaled int64 fixed point.
+// ------------------------------------------------------------------
+struct ColumnDef {
+    std::string name;
+    std::string cudaType;  // "int", "long long", "unsigned char"
+};
+struct TableDef {
+    std::string name;
+    std::vector<ColumnDef> columns;
+    const ColumnDef& col(const std::string& n) const;
+};
+const TableDef& catalogTable(const std::string& table);
+std::vector<std::string> catalogTables();
+
+struct CudaQueryPlan {
+    std::string name;
+    struct Phase {
+        std::string name;
+        std::unique_ptr<CudaOperator> root;
+        int threadgroupSize = 256;
+        int minBlocksPerSM = 1;
+        bool singleThread = false;
+        std::vector<std::pair<std::string, std::string>> bitmapReads;   // (name, sizeExpr)
+        std::vector<std::pair<std::string, std::string>> scalarParams;  // (name, type)
+        struct ExtraBuffer {
+            std::string name, type;
+            bool readOnly = true;
+            bool zeroInit = false;
+        };
+        std::vector<ExtraBuffer> extraBuffers;
+    };
+    std::vector<Phase> phases;
+    std::vector<std::string> helpers;
+    bool chunkable = false;
+
+    struct CpuSort {
+        struct SortKey {
+            std::string column;
+            bool descending;
+        };
+        std::vector<SortKey> keys;
+        int limit = -1;
+    };
+    std::optional<CpuSort> cpuSort;
+
+    struct SizingStep {
+        std::string symbol;       // symbol registered before phase `afterPhase`
+        int afterPhase = 0;       // phases [0, afterPhase) produce it
+        std::string counterBuffer;// u64 buffer holding the exact value
+        std::string fallbackExpr; // when no counter: a size expression
+    };
+    std::vector<SizingStep> sizing;
+
+    std::vector<std::function<void(CudaResultSchema&)>> decorate;
+
+    // Tables the plan scans (for registration checks and algorithmic bytes).
+    std::vector<std::string> tables;
+    std::string spec;  // canonical spec string the plan was built from
+};
+
+// Tunables the autotuner sweeps. Every field changes the generated source
+// (hence the compile-cache key) but never an answer.
+struct TuneConfig {
+    int blockSize = 512;
+    ScanConfig scan;
+    HashLayout hashLayout = HashLayout::Linear;
+    int smemPreAggLog2 = 0;     // hash group-by shared-memory table (0 = off)
+    bool warpAggregate = true;  // match_any pre-aggregation in hash / atomic aggregation
+    int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
+    int maxProbe = 128;
+    std::string toString() const;
+    static TuneConfig parse(const std::string& s);  // "bs=512;scan=tma;tile=1024;stages=4;..."
+};
+
+using SpecMap = std::map<std::string, std::string>;
+SpecMap parseSpec(const std::string& spec);
+std::string canonicalSpec(const SpecMap& m);
+
+// Build a plan for `spec` (template=...; constants). Throws
+// std::runtime_error on an unknown template / bad constant.
+CudaQueryPlan buildCudaPlan(const std::string& spec, const TuneConfig& tune = {});
+
+// Generate CUDA source metadata from a plan. Reference:
+// generateFromPlan (metal_plan_builder.cpp:2115-2154).
+CudaCodegen generateFromPlan(const CudaQueryPlan& plan);
+
+// Algorithmic bytes of one execution of the plan (each referenced column
+// read once, at its declared width), given registered row counts.
+long long planAlgorithmicBytes(const CudaQueryPlan& plan, const std::map<std::string, long long>& rows);
+
+// Template names understood by buildCudaPlan.
+std::vector<std::string> planTemplates();
+
+}  // namespace gpudb

@@ -1,0 +1,213 @@
+"""GPU parity: every generated pipeline, called through the C-ABI, against
+the CPU oracle on the same seeded inputs. Integers must match bit-exactly;
+FP64 derived averages to 1e-12 relative (they are the same IEEE division of
+the same exact integers, so they are in fact identical)."""
+import numpy as np
+import pytest
+
+from gpudbmetalcodegen_b200 import workloads as W
+from gpudbmetalcodegen_b200._lib import GpudbError, DEVERR_HASH_OVERFLOW
+from oracle import oracle_py as O
+
+pytestmark = pytest.mark.gpu
+REL = 1e-12
+
+Q1_TUNES = ["", "scan=direct", "bs=256;tile=1024;stages=2", "bs=1024;tile=2048;stages=3", "bs=128;tile=512;stages=8",
+            "keyed=2", "keyed=3"]
+
+
+def assert_q1_equal(res, expect):
+    got = res.as_dicts()
+    assert [(r["flag_a"], r["flag_b"]) for r in got] == [(r["flag_a"], r["flag_b"]) for r in expect]
+    for g, e in zip(got, expect):
+        for k in O.Q1_AGGS:
+            assert g[k] == e[k], (k, g[k], e[k])
+        for k in ("avg_qty", "avg_price", "avg_disc"):
+            assert abs(g[k] - e[k]) <= REL * abs(e[k]), (k, g[k], e[k])
+
+
+@pytest.fixture(scope="module")
+def fact_small():
+    return W.gen_fact(300_000, seed=11)
+
+
+@pytest.mark.parametrize("tune", Q1_TUNES)
+def test_q1_parity(ctx, fact_small, tune):
+    ctx.upload_table("fact", fact_small)
+    res, t = ctx.run("template=q1", tune)
+    assert t.device_error == 0
+    assert_q1_equal(res, O.q1(fact_small))
+
+
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=1024;tile=4096;stages=2"])
+def test_q6_parity(ctx, fact_small, tune):
+    ctx.upload_table("fact", fact_small)
+    res, _ = ctx.run("template=q6", tune)
+    assert res.rows == [(O.q6(fact_small),)]
+    res, _ = ctx.run("template=q6;ship_ge=0;ship_lt=3000;disc_lo=0;disc_hi=10;qty_lt=51", tune)
+    assert res.rows == [(O.q6(fact_small, 0, 3000, 0, 10, 51),)]
+
+
+@pytest.mark.parametrize("n", [0, 1, 15, 1023, 1025, 4097, 70_001])
+def test_q1_ragged_and_empty_tables(ctx, n):
+    f = W.gen_fact(n, seed=5)
+    ctx.upload_table("fact", f)
+    res, _ = ctx.run("template=q1")
+    expect = O.q1(f)
+    if n == 0:
+        assert res.rows == [] and expect == []
+    else:
+        assert_q1_equal(res, expect)
+
+
+def test_q1_filter_rejects_everything(ctx, fact_small):
+    ctx.upload_table("fact", fact_small)
+    res, _ = ctx.run("template=q1;ship_le=-1")
+    assert res.rows == []
+
+
+def test_q1_misaligned_columns_fall_back_to_direct_loads(ctx):
+    torch = pytest.importorskip("torch")
+    f = W.gen_fact(50_001, seed=9)
+    keep = {}
+    for name, arr in f.items():
+        t = torch.from_numpy(arr).cuda()
+        keep[name] = t
+        # rows 1..n: the u8 columns start 1 byte past a 16-byte boundary
+        ctx.register_column("fact", name, t.data_ptr() + arr.itemsize, arr.shape[0] - 1, arr.itemsize)
+    torch.cuda.synchronize()
+    sub = {k: v[1:] for k, v in f.items()}
+    res, _ = ctx.run("template=q1")
+    assert_q1_equal(res, O.q1(sub))
+    del keep
+
+
+def test_q1_full_size(ctx):
+    f = W.gen_fact(W.FACT_ROWS)
+    ctx.upload_table("fact", f)
+    for tune in ("", "scan=direct"):
+        res, _ = ctx.run("template=q1", tune)
+        assert_q1_equal(res, O.q1(f))
+    res, _ = ctx.run("template=q6")
+    assert res.rows == [(O.q6(f),)]
+
+
+# ---------------------------------------------------------------------------
+# join + group + top-k
+# ---------------------------------------------------------------------------
+def load_join(ctx, nd, npr, seed=3):
+    d = W.gen_dim(nd, seed=seed)
+    p = W.gen_probe(npr, dim_rows=nd, seed=seed)
+    ctx.upload_table("dim", d)
+    ctx.upload_table("probe", p)
+    return d, p
+
+
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0"])
+def test_join_topk_parity(ctx, tune):
+    d, p = load_join(ctx, 200_000, 800_000)
+    top, groups, distinct = O.join_topk(d, p, k=10)
+    res, t = ctx.run("template=join_topk", tune)
+    assert t.device_error == 0
+    assert res.rows == top
+    assert ctx.get_symbol("jt_groups") == distinct
+    res, _ = ctx.run("template=join_topk;k=32")
+    assert res.rows == O.join_topk(d, p, k=32)[0]
+
+
+def test_join_topk_ties_break_by_key(ctx):
+    # every probe row carries the same revenue: ranking is decided by key
+    d = W.gen_dim(5000, seed=4)
+    p = W.gen_probe(20_000, dim_rows=5000, seed=4)
+    p["p_price"][:] = 100_000
+    p["p_discount"][:] = 0
+    p["p_fk"][:] = (np.arange(p["p_fk"].shape[0]) % 5000 + 1).astype(np.int32)
+    ctx.upload_table("dim", d)
+    ctx.upload_table("probe", p)
+    res, _ = ctx.run("template=join_topk;k=10;ship_gt=0;od_lt=3000")
+    assert res.rows == O.join_topk(d, p, k=10, ship_gt=0, od_lt=3000)[0]
+
+
+def test_join_topk_learned_size_overflow_is_reported(ctx):
+    load_join(ctx, 200_000, 800_000)
+    with pytest.raises(GpudbError) as e:
+        ctx.run("template=join_topk;groups=4")
+    assert e.value.status == -7
+    assert e.value.timing.device_error & DEVERR_HASH_OVERFLOW
+
+
+def test_max_key_pass(ctx):
+    d, _ = load_join(ctx, 123_457, 1000)
+    assert ctx.register_max_key("b_key") == O.max_i32(d["b_key"]) == 123_457
+
+
+def test_join_topk_full_size(ctx):
+    d, p = load_join(ctx, W.DIM_ROWS, W.PROBE_ROWS, seed=W.SEED)
+    top, groups, distinct = O.join_topk(d, p, k=10)
+    res, _ = ctx.run("template=join_topk")
+    assert res.rows == top
+    assert ctx.get_symbol("jt_groups") == distinct
+
+
+# ---------------------------------------------------------------------------
+# skewed group-by and hash join
+# ---------------------------------------------------------------------------
+GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0"]
+
+
+@pytest.fixture(scope="module")
+def zipf_small():
+    nkeys = 1 << 16
+    return W.gen_zbuild(nkeys, seed=2), W.gen_zprobe(1_000_000, nkeys=nkeys, s=1.1, seed=2), nkeys
+
+
+@pytest.mark.parametrize("tune", GB_TUNES)
+def test_groupby_parity(ctx, zipf_small, tune):
+    _, zp, nkeys = zipf_small
+    ctx.upload_table("zprobe", zp)
+    ctx.register_symbol("zgroups", nkeys)
+    res, t = ctx.run("template=groupby", tune)
+    assert t.device_error == 0
+    k, c, s = O.groupby(zp["z_key"], zp["z_value"], cap=nkeys)
+    assert np.array_equal(np.array(res.column("key")), k)
+    assert np.array_equal(np.array(res.column("count")), c)
+    assert np.array_equal(np.array(res.column("sum")), s)
+
+
+@pytest.mark.parametrize("tune", ["", "layout=bucket8", "smem=11", "warp=0"])
+def test_hashjoin_parity(ctx, zipf_small, tune):
+    zb, zp, _ = zipf_small
+    ctx.upload_table("zbuild", zb)
+    ctx.upload_table("zprobe", zp)
+    res, _ = ctx.run("template=hashjoin", tune)
+    k, c, s = O.hashjoin(zb, zp["z_key"], cap=zb["zb_key"].shape[0])
+    assert np.array_equal(np.array(res.column("key")), k)
+    assert np.array_equal(np.array(res.column("count")), c)
+    assert np.array_equal(np.array(res.column("sum")), s)
+
+
+# ---------------------------------------------------------------------------
+# mixed-workload templates
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def mix_small():
+    return W.gen_mix(400_000, nranks=1 << 20, dim_rows=50_000, seed=8), W.gen_mixdim(50_000, seed=8)
+
+
+@pytest.mark.parametrize("thr", [100, 5000, 9900])
+def test_mix_templates_parity(ctx, mix_small, thr):
+    m, md = mix_small
+    ctx.upload_table("mix", m)
+    ctx.upload_table("mixdim", md)
+    res, _ = ctx.run(f"template=mix_agg;thr={thr}")
+    assert res.rows == [O.mix_agg(m, thr)]
+    res, _ = ctx.run(f"template=mix_join;thr={thr};attr_lt=400")
+    assert res.rows == [O.mix_join(md, m, 400, thr)]
+    for key_col, card in (("m_rank_u", 1000), ("m_rank_z", 50_000)):
+        ctx.register_symbol("mix_groups", card)
+        res, _ = ctx.run(f"template=mix_groupby;thr={thr};card={card};key={key_col}")
+        k, c, s = O.mix_groupby(m, key_col, thr, card)
+        assert np.array_equal(np.array(res.column("key")), k)
+        assert np.array_equal(np.array(res.column("sum")), s)
+        res, _ = ctx.run(f"template=mix_topk;thr={thr};card={card};key={key_col};k=7")
+        assert res.rows == O.topk(k, s, 7)
