@@ -173,6 +173,7 @@ def load_traffic():
 
 
 def main():
+    global BUILD_ROWS, PROBE_ROWS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -184,7 +185,6 @@ def main():
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS, help="smaller cases for profiling only")
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS, help="smaller cases for profiling only")
     args = ap.parse_args()
-    global BUILD_ROWS, PROBE_ROWS
     BUILD_ROWS, PROBE_ROWS = args.build_rows, args.probe_rows
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_info()

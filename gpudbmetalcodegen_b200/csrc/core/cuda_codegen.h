@@ -80,6 +80,7 @@ public:
     // Carve `bytes` (128-byte aligned) out of the phase's dynamic shared
     // memory; returns the byte offset from `gpudb_smem`.
     int allocDynamicSmem(int bytes);
+    int dynamicSmemBytes() const { return current_ < 0 ? 0 : phases_[current_].dynamicSmemBytes; }
     void addConstantDataParam(const std::string& name, const std::string& type, size_t bytes);
     void addBitmapReadParam(const std::string& name, const std::string& sizeExpr);
     void addBitmapWriteParam(const std::string& name, const std::string& sizeExpr);

@@ -75,7 +75,7 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     // ---- TMA bulk staged tile loop ------------------------------------
     const int bs = cg.currentThreadgroupSize();
     const int tile = cfg_.tileRows;
-    const int stages = cfg_.stages;
+    int stages = cfg_.stages;
     if (tile <= 0 || tile % 16 != 0 || tile % bs != 0)
         throw std::runtime_error("CudaGridStrideScan: tileRows must be a positive multiple of 16 and of the block size");
     if (stages < 1 || stages > 8) throw std::runtime_error("CudaGridStrideScan: stages must be in [1,8]");
@@ -88,6 +88,14 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
         txBytes += (long long)tile * w;
     }
     if (txBytes >= (1 << 20)) throw std::runtime_error("CudaGridStrideScan: tile too large for one mbarrier transaction");
+    // Ring depth is clamped to what fits one CTA's shared memory (227 KB on
+    // sm_100) next to the operators' own shared tables and reductions.
+    constexpr long long kSmemBudget = 200 * 1024;
+    const long long avail = kSmemBudget - 128 - cg.dynamicSmemBytes();
+    if (stageBytes > avail)
+        throw std::runtime_error("CudaGridStrideScan: one " + S(tile) + "-row tile (" + S(stageBytes) +
+                                 " B) does not fit in shared memory; use fewer tile rows");
+    if ((long long)stages * stageBytes > avail) stages = (int)(avail / stageBytes);
     const int barOff = cg.allocDynamicSmem(128);
     const int ringOff = cg.allocDynamicSmem((int)(stageBytes * stages));
     cg.setPhaseTileRows(tile);
