@@ -78,6 +78,8 @@ _SIGNATURES = [
     ("gpudb_release_buffers", C.c_int, [C.c_void_p]),
     ("gpudb_host_alloc", C.c_void_p, [C.c_uint64]),
     ("gpudb_host_free", None, [C.c_void_p]),
+    ("gpudb_distinct_count_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_int64,
+                                               C.c_void_p, C.c_void_p]),
     # gpudb_engine.h
     ("gpudb_query_prepare", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     ("gpudb_query_free", None, [C.c_void_p]),

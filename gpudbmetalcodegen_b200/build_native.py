@@ -42,7 +42,9 @@ HOST_SOURCES = [
     "capi/gpudb_capi.cpp",
     "datagen/datagen.cpp",
 ]
-CUDA_SOURCES: list[str] = []
+CUDA_SOURCES: list[str] = [
+    "kernels/noalloc_distinct.cu",
+]
 
 LIB_NAME = "libgpudb.so"
 

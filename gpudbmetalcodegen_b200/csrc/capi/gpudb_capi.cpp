@@ -87,6 +87,11 @@ void fillTiming(const gpudb::ExecutionResult& r, gpudb_timing* t) {
 
 }  // namespace
 
+namespace gpudb {
+// Error text of context-free entry points, read back by gpudb_last_error(NULL).
+void setThreadError(const std::string& message) { tlCreateError = message; }
+}  // namespace gpudb
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
