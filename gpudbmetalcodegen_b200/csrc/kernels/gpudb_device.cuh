@@ -192,6 +192,11 @@ __device__ __forceinline__ void gpudb_mbar_expect_tx(unsigned long long* bar, un
                  : "memory");
 }
 
+// Plain arrival (one count) on `bar`, e.g. a consumer warp releasing a stage.
+__device__ __forceinline__ void gpudb_mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(gpudb_smem_addr(bar)) : "memory");
+}
+
 // Copy `bytes` (multiple of 16; both addresses 16-byte aligned) from
 // global to this CTA's shared memory; completion is signalled on `bar`.
 __device__ __forceinline__ void gpudb_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
@@ -257,10 +262,11 @@ __device__ __forceinline__ unsigned long long gpudb_hash_slot(unsigned long long
 }
 
 // Linear probing, 64-bit keys. Returns the slot holding `key` (inserted
-// if absent) or -1 when `max_probe` slots were all taken.
+// if absent) or -1 when `max_probe` slots were all taken. *fresh (when
+// given) is set when this call claimed the slot, i.e. created the group.
 __device__ __forceinline__ long long gpudb_ht_insert64(unsigned long long* keys, int log2cap,
                                                        unsigned long long key, unsigned max_probe,
-                                                       unsigned* err) {
+                                                       unsigned* err, bool* fresh = nullptr) {
     if (key == GPUDB_EMPTY64) {
         gpudb_set_error(err, GPUDB_ERR_SENTINEL_KEY);
         return -1;
@@ -272,7 +278,11 @@ __device__ __forceinline__ long long gpudb_ht_insert64(unsigned long long* keys,
         if (cur == key) return (long long)s;
         if (cur == GPUDB_EMPTY64) {
             const unsigned long long prev = atomicCAS(keys + s, GPUDB_EMPTY64, key);
-            if (prev == GPUDB_EMPTY64 || prev == key) return (long long)s;
+            if (prev == GPUDB_EMPTY64) {
+                if (fresh) *fresh = true;
+                return (long long)s;
+            }
+            if (prev == key) return (long long)s;
         }
         s = (s + 1ull) & mask;
     }
@@ -295,7 +305,7 @@ __device__ __forceinline__ long long gpudb_ht_find64(const unsigned long long* _
 
 // 32-bit keys (dense integer join / group keys).
 __device__ __forceinline__ long long gpudb_ht_insert32(unsigned* keys, int log2cap, unsigned key,
-                                                       unsigned max_probe, unsigned* err) {
+                                                       unsigned max_probe, unsigned* err, bool* fresh = nullptr) {
     if (key == GPUDB_EMPTY32) {
         gpudb_set_error(err, GPUDB_ERR_SENTINEL_KEY);
         return -1;
@@ -307,7 +317,11 @@ __device__ __forceinline__ long long gpudb_ht_insert32(unsigned* keys, int log2c
         if (cur == key) return (long long)s;
         if (cur == GPUDB_EMPTY32) {
             const unsigned prev = atomicCAS(keys + s, GPUDB_EMPTY32, key);
-            if (prev == GPUDB_EMPTY32 || prev == key) return (long long)s;
+            if (prev == GPUDB_EMPTY32) {
+                if (fresh) *fresh = true;
+                return (long long)s;
+            }
+            if (prev == key) return (long long)s;
         }
         s = (s + 1ull) & mask;
     }
@@ -333,7 +347,7 @@ __device__ __forceinline__ long long gpudb_ht_find32(const unsigned* __restrict_
 // Slot index = bucket * 8 + way. log2cap counts slots (>= 3).
 __device__ __forceinline__ long long gpudb_htb_insert64(unsigned long long* keys, int log2cap,
                                                         unsigned long long key, unsigned max_buckets,
-                                                        unsigned* err) {
+                                                        unsigned* err, bool* fresh = nullptr) {
     if (key == GPUDB_EMPTY64) {
         gpudb_set_error(err, GPUDB_ERR_SENTINEL_KEY);
         return -1;
@@ -358,7 +372,11 @@ __device__ __forceinline__ long long gpudb_htb_insert64(unsigned long long* keys
         for (int w = 0; w < 8; ++w) {
             if (k[w] != GPUDB_EMPTY64) continue;
             const unsigned long long prev = atomicCAS(base + w, GPUDB_EMPTY64, key);
-            if (prev == GPUDB_EMPTY64 || prev == key) return (long long)(b * 8ull + w);
+            if (prev == GPUDB_EMPTY64) {
+                if (fresh) *fresh = true;
+                return (long long)(b * 8ull + w);
+            }
+            if (prev == key) return (long long)(b * 8ull + w);
             k[w] = prev;  // lost the race: slot now holds another key, keep scanning
         }
         b = (b + 1ull) & bmask;

@@ -76,8 +76,8 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     const int bs = cg.currentThreadgroupSize();
     const int tile = cfg_.tileRows;
     int stages = cfg_.stages;
-    if (tile <= 0 || tile % 16 != 0 || tile % bs != 0)
-        throw std::runtime_error("CudaGridStrideScan: tileRows must be a positive multiple of 16 and of the block size");
+    if (tile <= 0 || tile % 16 != 0)
+        throw std::runtime_error("CudaGridStrideScan: tileRows must be a positive multiple of 16");
     if (stages < 1 || stages > 8) throw std::runtime_error("CudaGridStrideScan: stages must be in [1,8]");
     std::vector<long long> off;
     long long stageBytes = 0, txBytes = 0;
@@ -96,77 +96,84 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
         throw std::runtime_error("CudaGridStrideScan: one " + S(tile) + "-row tile (" + S(stageBytes) +
                                  " B) does not fit in shared memory; use fewer tile rows");
     if ((long long)stages * stageBytes > avail) stages = (int)(avail / stageBytes);
+    if (bs < 64) throw std::runtime_error("CudaGridStrideScan: the TMA scan needs at least two warps per block");
     const int barOff = cg.allocDynamicSmem(128);
     const int ringOff = cg.allocDynamicSmem((int)(stageBytes * stages));
     cg.setPhaseTileRows(tile);
 
-    const std::string SB = S(stageBytes);
-    cg.addComment("TMA-bulk staged scan of " + tableName_ + ": " + S(tile) + "-row tiles, " + S(stages) +
-                  "-stage cp.async.bulk ring, " + S(txBytes) + " B per tile");
+    const std::string SB = S(stageBytes), ST = S(stages), TL = S(tile);
+    cg.addComment("TMA-bulk staged scan of " + tableName_ + ": " + TL + "-row tiles, " + ST +
+                  "-stage cp.async.bulk ring, " + S(txBytes) + " B per tile; warp 0 produces, the other warps consume");
     cg.addBlock("", [&]() {
-        cg.addLine("unsigned long long* _sb_bar = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(barOff) +
+        cg.addLine("unsigned long long* _sb_full = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(barOff) +
                    ");");
+        cg.addLine("unsigned long long* _sb_empty = _sb_full + " + ST + ";");
         cg.addLine("unsigned char* _sb_ring = gpudb_smem + " + S(ringOff) + ";");
         cg.addLine("const long long _sb_n = " + n + ";");
         std::string alignExpr;
         for (size_t k = 0; k < columns_.size(); k++)
             alignExpr += (k ? " | " : "") + std::string("(unsigned long long)") + columns_[k].paramName;
         cg.addLine("const bool _sb_aligned = ((" + alignExpr + ") & 15ull) == 0ull;");
-        cg.addLine("const long long _sb_ntiles = _sb_aligned ? (_sb_n / " + S(tile) + "ll) : 0ll;");
+        cg.addLine("const long long _sb_ntiles = _sb_aligned ? (_sb_n / " + TL + "ll) : 0ll;");
         cg.addIf("threadIdx.x == 0", [&]() {
-            cg.addLine("for (int _s = 0; _s < " + S(stages) + "; ++_s) gpudb_mbar_init(_sb_bar + _s, 1u);");
+            cg.addBlock("for (int _s = 0; _s < " + ST + "; ++_s)", [&]() {
+                cg.addLine("gpudb_mbar_init(_sb_full + _s, 1u);");
+                cg.addLine("gpudb_mbar_init(_sb_empty + _s, (blockDim.x >> 5) - 1u);");
+            });
             cg.addLine("gpudb_mbar_init_fence();");
         });
         cg.addLine("__syncthreads();");
-        cg.addLine("const unsigned long long _sb_pol = gpudb_policy_evict_first();");
-        cg.addBlock("auto _sb_issue = [&](long long _t, int _s)", [&]() {
-            cg.addLine("unsigned char* _st = _sb_ring + (long long)_s * " + SB + "ll;");
-            cg.addLine("gpudb_mbar_expect_tx(_sb_bar + _s, " + S(txBytes) + "u);");
-            for (size_t k = 0; k < columns_.size(); k++) {
-                const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
-                cg.addLine("gpudb_bulk_g2s_stream(_st + " + S(off[k]) + ", " + columns_[k].paramName + " + _t * " +
-                           S(tile) + "ll, " + S(tile * w) + "u, _sb_bar + _s, _sb_pol);");
-            }
-        }, ";");
-        cg.addIf("threadIdx.x == 0", [&]() {
-            cg.addBlock("for (int _s = 0; _s < " + S(stages) + "; ++_s)", [&]() {
-                cg.addLine("const long long _t = (long long)blockIdx.x + (long long)_s * gridDim.x;");
-                cg.addLine("if (_t < _sb_ntiles) _sb_issue(_t, _s);");
-            });
-        });
-        cg.addLine("unsigned _sb_par = 0u;");
-        cg.addLine("int _sb_s = 0;");
         cg.addLine("bool _sb_ok = true;");
-        cg.addBlock("for (long long _sb_t = blockIdx.x; _sb_t < _sb_ntiles; _sb_t += gridDim.x)", [&]() {
-            cg.addLine("const bool _sb_got = gpudb_mbar_wait(_sb_bar + _sb_s, (_sb_par >> _sb_s) & 1u, gpudb_err);");
-            cg.addLine("_sb_par ^= (1u << _sb_s);");
-            cg.addIf("_sb_got", [&]() {
-                cg.addLine("const long long _sb_base = _sb_t * " + S(tile) + "ll;");
-                cg.addLine("const unsigned char* _sb_st = _sb_ring + (long long)_sb_s * " + SB + "ll;");
+        cg.addBlock("if ((threadIdx.x >> 5) == 0)", [&]() {
+            cg.addComment("producer: one lane streams tiles into the ring, refilling a stage once every consumer warp released it");
+            cg.addBlock("if (threadIdx.x == 0)", [&]() {
+                cg.addLine("const unsigned long long _sb_pol = gpudb_policy_evict_first();");
+                cg.addLine("long long _sb_j = 0;");
+                cg.addBlock("for (long long _sb_t = blockIdx.x; _sb_t < _sb_ntiles; _sb_t += gridDim.x, ++_sb_j)", [&]() {
+                    cg.addLine("const int _s = (int)(_sb_j % " + ST + ");");
+                    cg.addBlock("if (_sb_j >= " + ST + ")", [&]() {
+                        cg.addLine("if (!gpudb_mbar_wait(_sb_empty + _s, (unsigned)(((_sb_j / " + ST +
+                                   ") - 1) & 1), gpudb_err)) { _sb_ok = false; break; }");
+                        cg.addLine("gpudb_fence_proxy_async();");
+                    });
+                    cg.addLine("unsigned char* _st = _sb_ring + (long long)_s * " + SB + "ll;");
+                    cg.addLine("gpudb_mbar_expect_tx(_sb_full + _s, " + S(txBytes) + "u);");
+                    for (size_t k = 0; k < columns_.size(); k++) {
+                        const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
+                        cg.addLine("gpudb_bulk_g2s_stream(_st + " + S(off[k]) + ", " + columns_[k].paramName + " + _sb_t * " +
+                                   TL + "ll, " + S(tile * w) + "u, _sb_full + _s, _sb_pol);");
+                    }
+                });
+            });
+        }, " else {");
+        cg.increaseIndent();
+        cg.addComment("consumers: wait for a full stage, process its rows from shared memory, release it");
+        cg.addLine("long long _sb_j = 0;");
+        cg.addBlock("for (long long _sb_t = blockIdx.x; _sb_t < _sb_ntiles; _sb_t += gridDim.x, ++_sb_j)", [&]() {
+            cg.addLine("const int _s = (int)(_sb_j % " + ST + ");");
+            cg.addLine("if (!__all_sync(0xffffffffu, gpudb_mbar_wait(_sb_full + _s, (unsigned)((_sb_j / " + ST +
+                       ") & 1), gpudb_err))) { _sb_ok = false; break; }");
+            cg.addBlock("", [&]() {
+                cg.addLine("const long long _sb_base = _sb_t * " + TL + "ll;");
+                cg.addLine("const unsigned char* _sb_st = _sb_ring + (long long)_s * " + SB + "ll;");
                 for (size_t k = 0; k < columns_.size(); k++)
                     cg.addLine("const " + columns_[k].cudaType + "* " + columns_[k].paramName + " = reinterpret_cast<const " +
                                columns_[k].cudaType + "*>(_sb_st + " + S(off[k]) + ");");
-                cg.addBlock("for (int " + i + " = threadIdx.x; " + i + " < " + S(tile) + "; " + i + " += " + S(bs) + ")",
+                cg.addBlock("for (int " + i + " = (int)threadIdx.x - 32; " + i + " < " + TL + "; " + i +
+                                " += (int)blockDim.x - 32)",
                             [&]() {
                                 cg.addLine("const long long _row = _sb_base + " + i + "; (void)_row;");
                                 consume();
                             });
             });
-            cg.addIf("!__syncthreads_and(_sb_got)", [&]() {
-                cg.addLine("_sb_ok = false;");
-                cg.addLine("break;");
-            });
-            cg.addIf("threadIdx.x == 0", [&]() {
-                cg.addLine("const long long _nt = _sb_t + (long long)" + S(stages) + " * gridDim.x;");
-                cg.addIf("_nt < _sb_ntiles", [&]() {
-                    cg.addLine("gpudb_fence_proxy_async();");
-                    cg.addLine("_sb_issue(_nt, _sb_s);");
-                });
-            });
-            cg.addLine("_sb_s = (_sb_s + 1 == " + S(stages) + ") ? 0 : _sb_s + 1;");
+            cg.addLine("__syncwarp();");
+            cg.addLine("if ((threadIdx.x & 31u) == 0u) gpudb_mbar_arrive(_sb_empty + _s);");
         });
+        cg.decreaseIndent();
+        cg.addLine("}");
+        cg.addLine("_sb_ok = !__syncthreads_or(!_sb_ok);");
         cg.addComment("rows of the partial last tile (all rows if a column is not 16-byte aligned)");
-        cg.addBlock("if (_sb_ok) for (long long " + i + " = _sb_ntiles * " + S(tile) + "ll + tid; " + i + " < _sb_n; " + i +
+        cg.addBlock("if (_sb_ok) for (long long " + i + " = _sb_ntiles * " + TL + "ll + tid; " + i + " < _sb_n; " + i +
                         " += tpg)",
                     [&]() {
                         cg.addLine("const long long _row = " + i + "; (void)_row;");
@@ -195,6 +202,25 @@ void CudaBufferScan::produce(CudaCodegen& cg, ConsumerFn consume) {
 }
 
 std::string CudaBufferScan::describe() const { return "BufferScan(" + countName_ + " = " + countExpr_ + ")"; }
+
+CudaSlotListScan::CudaSlotListScan(const std::string& listBuffer, const std::string& countBuffer,
+                                   const std::string& idxVar)
+    : list_(listBuffer), count_(countBuffer), idxVar_(idxVar) {}
+
+void CudaSlotListScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.addReadBufferParam(list_, "unsigned");
+    cg.addReadBufferParam(count_, "unsigned long long");
+    cg.addBufferLengthParam("len_" + list_, list_);
+    const std::string& i = idxVar_;
+    cg.addLine("const long long _sl_n = (long long)min(__ldcg(" + count_ + "), (unsigned long long)len_" + list_ + ");");
+    cg.addBlock("for (long long _sl = tid; _sl < _sl_n; _sl += tpg)", [&]() {
+        cg.addLine("const long long " + i + " = (long long)__ldcg(" + list_ + " + _sl);");
+        cg.addLine("const long long _row = " + i + "; (void)_row;");
+        consume();
+    });
+}
+
+std::string CudaSlotListScan::describe() const { return "SlotListScan(" + list_ + "[0.." + count_ + "))"; }
 
 // ===================================================================
 // Selection / ComputeExpr
@@ -231,7 +257,10 @@ CudaBitmapBuild::CudaBitmapBuild(std::unique_ptr<CudaOperator> child, const std:
 void CudaBitmapBuild::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addBitmapWriteParam(bitmapName_, sizeExpr_);
     cg.addBufferLengthParam("len_" + bitmapName_, bitmapName_);
-    if (!counter_.empty()) cg.addAtomicBufferParam(counter_, "unsigned long long", "1");
+    if (!counter_.empty()) {
+        cg.addAtomicBufferParam(counter_, "unsigned long long", "1");
+        cg.addLine("unsigned long long _bm_fresh = 0ull;  // keys this thread was first to set");
+    }
     child_->produce(cg, [&]() {
         cg.addLine("const long long _bk = (long long)(" + keyExpr_ + ");");
         cg.addBlock("if ((unsigned long long)(_bk >> 5) >= (unsigned long long)len_" + bitmapName_ + ")", [&]() {
@@ -242,13 +271,17 @@ void CudaBitmapBuild::produce(CudaCodegen& cg, ConsumerFn consume) {
             cg.addLine("gpudb_bitmap_set(" + bitmapName_ + ", _bk);");
         } else {
             cg.addLine("const unsigned _bbit = 1u << (unsigned)(_bk & 31);");
-            cg.addLine("if ((atomicOr(" + bitmapName_ + " + (_bk >> 5), _bbit) & _bbit) == 0u) atomicAdd(" + counter_ +
-                       ", 1ull);");
+            cg.addLine("if ((atomicOr(" + bitmapName_ + " + (_bk >> 5), _bbit) & _bbit) == 0u) ++_bm_fresh;");
         }
         consume();
         cg.decreaseIndent();
         cg.addLine("}");
     });
+    if (!counter_.empty()) {
+        cg.addComment("distinct count: warp sum, one atomic per warp");
+        cg.addLine("_bm_fresh = gpudb_warp_sum_u64(_bm_fresh);");
+        cg.addLine("if ((threadIdx.x & 31u) == 0u && _bm_fresh) atomicAdd(" + counter_ + ", _bm_fresh);");
+    }
 }
 
 std::string CudaBitmapBuild::describe() const { return "BitmapBuild(" + bitmapName_ + ", key=" + keyExpr_ + ")"; }
@@ -813,12 +846,20 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
         });
         cg.addLine("__syncthreads();");
     }
+    const std::string list = table_ + "_slotlist", nlist = table_ + "_nslots";
+    if (slotList_) {
+        cg.addBufferParam(list, "unsigned", cap, false);
+        cg.addAtomicBufferParam(nlist, "unsigned long long", "1");
+    }
     auto globalUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
+        if (slotList_) cg.addLine("bool _gnew = false;");
         cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + table_ + "_log2cap, " + ko.cast + keyVar + ", " +
-                   S(probeArg(layout_, maxProbe_)) + "u, gpudb_err);");
+                   S(probeArg(layout_, maxProbe_)) + "u, gpudb_err" + (slotList_ ? ", &_gnew" : "") + ");");
         cg.addBlock("if (_gslot >= 0)", [&]() {
             for (int j = 0; j < na; j++)
                 cg.addLine("atomicAdd(" + table_ + "_" + aggs_[j].name + " + _gslot, (unsigned long long)" + vals[j] + ");");
+            if (slotList_)
+                cg.addLine("if (_gnew) " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;  // group created");
         });
     };
     child_->produce(cg, [&]() {

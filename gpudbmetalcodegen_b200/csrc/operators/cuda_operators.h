@@ -93,6 +93,19 @@ private:
     std::string countName_, countExpr_, idxVar_;
 };
 
+// Leaf: visits the slot indices listed in `listBuffer` (u32), as many as
+// the device counter `countBuffer` (u64) holds when the kernel runs — the
+// used slots of a hash table built with a slot list. `idxVar` is the slot.
+class CudaSlotListScan : public CudaOperator {
+public:
+    CudaSlotListScan(const std::string& listBuffer, const std::string& countBuffer, const std::string& idxVar = "i");
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string list_, count_, idxVar_;
+};
+
 // Selection: if (predicate) consume(). Reference: metal_operators.cpp:63-69.
 class CudaSelection : public CudaUnaryOperator {
 public:
@@ -371,6 +384,9 @@ public:
     void addAggregate(const std::string& name, const std::string& valueExpr);  // "1" = count
     void setWarpAggregate(bool on) { warpAgg_ = on; }
     void setSharedPreAgg(int log2Slots) { smemLog2_ = log2Slots; }
+    // Record every slot when its group is created in <table>_slotlist
+    // (count in <table>_nslots): later phases visit only used slots.
+    void setSlotList(bool on) { slotList_ = on; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
@@ -384,6 +400,7 @@ private:
     std::vector<Agg> aggs_;
     bool warpAgg_ = true;
     int smemLog2_ = 0;
+    bool slotList_ = false;
 };
 
 // Top-k (value desc, key asc) of the consumed (key, value) pairs.

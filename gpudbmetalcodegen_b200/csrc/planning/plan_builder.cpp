@@ -262,12 +262,13 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
                                                     tune.maxProbe);
         gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
         gb->setWarpAggregate(tune.warpAggregate);
+        gb->setSlotList(true);
         appendPhase(plan, "JT_probe_group", std::move(gb), tune);
     }
     {
-        auto bscan = std::make_unique<CudaBufferScan>("n_jg_slots", hashSlotsExpr(cap));
-        auto f = std::make_unique<CudaSelection>(std::move(bscan), "jg_keys[i] != GPUDB_EMPTY32");
-        auto tk = std::make_unique<CudaTopK>(std::move(f), "jt_top", "(long long)(int)jg_keys[i]",
+        // only the slots whose groups were created (the probe's slot list)
+        auto lscan = std::make_unique<CudaSlotListScan>("jg_slotlist", "jg_nslots");
+        auto tk = std::make_unique<CudaTopK>(std::move(lscan), "jt_top", "(long long)(int)jg_keys[i]",
                                              "(long long)jg_revenue[i]", (int)k);
         auto& ph = appendPhase(plan, "JT_topk", std::move(tk), tune);
         ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});
@@ -430,11 +431,11 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
     gb->addAggregate("sum", "m_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
     gb->setSharedPreAgg(tune.smemPreAggLog2);
+    gb->setSlotList(tmpl == "mix_topk");
     appendPhase(plan, "MIXG_group", std::move(gb), tune);
     if (tmpl == "mix_topk") {
-        auto bscan = std::make_unique<CudaBufferScan>("n_mg_slots", hashSlotsExpr(cap));
-        auto sel = std::make_unique<CudaSelection>(std::move(bscan), "mg_keys[i] != GPUDB_EMPTY64");
-        auto tk = std::make_unique<CudaTopK>(std::move(sel), "mt_top", "(long long)mg_keys[i]", "(long long)mg_sum[i]",
+        auto lscan = std::make_unique<CudaSlotListScan>("mg_slotlist", "mg_nslots");
+        auto tk = std::make_unique<CudaTopK>(std::move(lscan), "mt_top", "(long long)mg_keys[i]", "(long long)mg_sum[i]",
                                              (int)k);
         auto& ph = appendPhase(plan, "MIXG_topk", std::move(tk), tune);
         ph.extraBuffers.push_back({"mg_keys", "unsigned long long", true, false});
