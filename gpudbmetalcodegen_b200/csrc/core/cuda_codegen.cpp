@@ -104,8 +104,9 @@ void CudaCodegen::pushBinding(const char* op, CudaParamBinding b, bool dedup) {
 }
 
 void CudaCodegen::addColumnParam(const std::string& paramName, const std::string& elemType,
-                                 const std::string& tableName) {
+                                 const std::string& tableName, bool late) {
     CudaParamBinding b;
+    b.late = late;
     b.name = paramName;
     b.cudaTypeDecl = "const " + elemType + "* __restrict__";
     b.kind = CudaParamKind::TableData;

@@ -65,7 +65,7 @@ public:
 
     // ---- parameters ----------------------------------------------------
     void addColumnParam(const std::string& paramName, const std::string& elemType,
-                        const std::string& tableName);
+                        const std::string& tableName, bool late = false);
     void addTableSizeParam(const std::string& table);
     void addBufferParam(const std::string& name, const std::string& elemType,
                         const std::string& sizeExpr, bool zeroInit = true, int fillByte = 0);

@@ -64,6 +64,7 @@ struct CudaParamBinding {
     bool zeroInit = false;     // memset before every run (fillByte)
     int fillByte = 0;          // 0x00 or 0xFF (sentinel -1 / empty hash key)
     bool readOnly = false;
+    bool late = false;         // TableData read only for surviving rows (never staged)
     size_t hostCopyBytes = 0;  // ConstantData
     int argIndex = -1;         // position in the kernel's argument list
 

@@ -48,22 +48,24 @@ CudaGridStrideScan::CudaGridStrideScan(const std::string& table, const std::stri
                                        const std::string& idxVar)
     : tableName_(table), rowVar_(rowVar), idxVar_(idxVar) {}
 
-void CudaGridStrideScan::addColumn(const std::string& paramName, const std::string& cudaType) {
+void CudaGridStrideScan::addColumn(const std::string& paramName, const std::string& cudaType, bool late) {
     for (const auto& c : columns_)
         if (c.paramName == paramName) return;
-    columns_.push_back({paramName, cudaType});
+    columns_.push_back({paramName, cudaType, late});
 }
 
 void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.setPhaseScannedTable(tableName_);
     if (columns_.empty())
         throw std::runtime_error("CudaGridStrideScan(" + tableName_ + "): no columns registered; call addColumn()");
-    for (const auto& c : columns_) cg.addColumnParam(c.paramName, c.cudaType, tableName_);
+    for (const auto& c : columns_) cg.addColumnParam(c.paramName, c.cudaType, tableName_, c.late);
     cg.addTableSizeParam(tableName_);
+    bool anyStaged = false;
+    for (const auto& c : columns_) anyStaged |= !c.late;
     const std::string n = tableSizeName(tableName_);
     const std::string& i = idxVar_;
 
-    if (cfg_.mode == ScanConfig::Direct) {
+    if (cfg_.mode == ScanConfig::Direct || !anyStaged) {
         cg.addComment("grid-stride scan of " + tableName_ + " (direct coalesced loads)");
         cg.addBlock("for (long long " + i + " = tid; " + i + " < " + n + "; " + i + " += tpg)", [&]() {
             cg.addLine("const long long _row = " + i + "; (void)_row;");
@@ -84,6 +86,7 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     for (const auto& c : columns_) {
         const long long w = (long long)cudaTypeBytes(c.cudaType);
         off.push_back(stageBytes);
+        if (c.late) continue;
         stageBytes += ((long long)tile * w + 127) / 128 * 128;
         txBytes += (long long)tile * w;
     }
@@ -111,8 +114,15 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
         cg.addLine("unsigned char* _sb_ring = gpudb_smem + " + S(ringOff) + ";");
         cg.addLine("const long long _sb_n = " + n + ";");
         std::string alignExpr;
-        for (size_t k = 0; k < columns_.size(); k++)
-            alignExpr += (k ? " | " : "") + std::string("(unsigned long long)") + columns_[k].paramName;
+        for (size_t k = 0; k < columns_.size(); k++) {
+            if (columns_[k].late) {
+                // outer name for the consumers' tile-relative view of a late column
+                cg.addLine("const " + columns_[k].cudaType + "* const _lt_" + columns_[k].paramName + " = " +
+                           columns_[k].paramName + ";");
+                continue;
+            }
+            alignExpr += (alignExpr.empty() ? "" : " | ") + std::string("(unsigned long long)") + columns_[k].paramName;
+        }
         cg.addLine("const bool _sb_aligned = ((" + alignExpr + ") & 15ull) == 0ull;");
         cg.addLine("const long long _sb_ntiles = _sb_aligned ? (_sb_n / " + TL + "ll) : 0ll;");
         cg.addIf("threadIdx.x == 0", [&]() {
@@ -139,6 +149,7 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                     cg.addLine("unsigned char* _st = _sb_ring + (long long)_s * " + SB + "ll;");
                     cg.addLine("gpudb_mbar_expect_tx(_sb_full + _s, " + S(txBytes) + "u);");
                     for (size_t k = 0; k < columns_.size(); k++) {
+                        if (columns_[k].late) continue;
                         const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
                         cg.addLine("gpudb_bulk_g2s_stream(_st + " + S(off[k]) + ", " + columns_[k].paramName + " + _sb_t * " +
                                    TL + "ll, " + S(tile * w) + "u, _sb_full + _s, _sb_pol);");
@@ -156,9 +167,14 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
             cg.addBlock("", [&]() {
                 cg.addLine("const long long _sb_base = _sb_t * " + TL + "ll;");
                 cg.addLine("const unsigned char* _sb_st = _sb_ring + (long long)_s * " + SB + "ll;");
-                for (size_t k = 0; k < columns_.size(); k++)
-                    cg.addLine("const " + columns_[k].cudaType + "* " + columns_[k].paramName + " = reinterpret_cast<const " +
-                               columns_[k].cudaType + "*>(_sb_st + " + S(off[k]) + ");");
+                for (size_t k = 0; k < columns_.size(); k++) {
+                    const auto& c = columns_[k];
+                    if (c.late)
+                        cg.addLine("const " + c.cudaType + "* " + c.paramName + " = _lt_" + c.paramName + " + _sb_base;");
+                    else
+                        cg.addLine("const " + c.cudaType + "* " + c.paramName + " = reinterpret_cast<const " + c.cudaType +
+                                   "*>(_sb_st + " + S(off[k]) + ");");
+                }
                 cg.addBlock("for (int " + i + " = (int)threadIdx.x - 32; " + i + " < " + TL + "; " + i +
                                 " += (int)blockDim.x - 32)",
                             [&]() {
@@ -946,40 +962,43 @@ void CudaTopK::produce(CudaCodegen& cg, ConsumerFn consume) {
                    "));");
         consume();
     });
-    cg.addComment("warp merge -> block merge -> last-block merge of the per-block lists");
+    cg.addComment("block merge (warp shuffle merge, then warp 0 over the warps' lists), per-block list to global,"
+                  " then the last block merges all per-block lists the same way");
     cg.addLine("long long _tw_v[" + K + "], _tw_k[" + K + "];");
-    cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
     cg.addLine("__shared__ long long _ts_v[32 * " + K + "], _ts_k[32 * " + K + "];");
     cg.addLine("__shared__ bool _t_last;");
-    cg.addBlock("if ((threadIdx.x & 31u) == 0u)", [&]() {
-        cg.addLine("#pragma unroll");
-        cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _ts_v[(threadIdx.x >> 5) * " + K + " + _q] = _tw_v[_q]; "
-                   "_ts_k[(threadIdx.x >> 5) * " + K + " + _q] = _tw_k[_q]; }");
+    // every thread's (_tk_v, _tk_k) list -> warp 0 holds the block's best K in (_tw_v, _tw_k)
+    auto blockMerge = [&]() {
+        cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
+        cg.addBlock("if ((threadIdx.x & 31u) == 0u)", [&]() {
+            cg.addLine("#pragma unroll");
+            cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _ts_v[(threadIdx.x >> 5) * " + K + " + _q] = _tw_v[_q]; "
+                       "_ts_k[(threadIdx.x >> 5) * " + K + " + _q] = _tw_k[_q]; }");
+        });
+        cg.addLine("__syncthreads();");
+        cg.addBlock("if (threadIdx.x < 32u)", [&]() {
+            cg.addLine("#pragma unroll");
+            cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _tk_v[_q] = GPUDB_TOPK_NONE_VAL; _tk_k[_q] = GPUDB_TOPK_NONE_KEY; }");
+            cg.addLine("for (int _e = (int)threadIdx.x; _e < (int)(blockDim.x >> 5) * " + K + "; _e += 32) gpudb_topk_push<" +
+                       K + ">(_tk_v, _tk_k, _ts_v[_e], _ts_k[_e]);");
+            cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
+        });
+    };
+    blockMerge();
+    cg.addBlock("if (threadIdx.x == 0u)", [&]() {
+        cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { " + out_ + "_pvals[blockIdx.x * " + K + " + _q] = _tw_v[_q]; " +
+                   out_ + "_pkeys[blockIdx.x * " + K + " + _q] = _tw_k[_q]; }");
+        cg.addLine("__threadfence();");
+        cg.addLine("_t_last = (atomicAdd(" + out_ + "_ticket, 1u) == gridDim.x - 1u);");
     });
     cg.addLine("__syncthreads();");
-    // merges n entries of (vals, keys) held in memory into the first warp's list
-    auto warpMerge = [&](const std::string& vsrc, const std::string& ksrc, const std::string& n, bool coherent) {
+    cg.addBlock("if (_t_last)", [&]() {
+        cg.addLine("__threadfence();");
         cg.addLine("#pragma unroll");
         cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _tk_v[_q] = GPUDB_TOPK_NONE_VAL; _tk_k[_q] = GPUDB_TOPK_NONE_KEY; }");
-        const std::string ld_v = coherent ? "__ldcg(" + vsrc + " + _e)" : vsrc + "[_e]";
-        const std::string ld_k = coherent ? "__ldcg(" + ksrc + " + _e)" : ksrc + "[_e]";
-        cg.addLine("for (int _e = (int)threadIdx.x; _e < " + n + "; _e += 32) gpudb_topk_push<" + K + ">(_tk_v, _tk_k, " + ld_v +
-                   ", " + ld_k + ");");
-        cg.addLine("gpudb_topk_warp_merge<" + K + ">(_tk_v, _tk_k, _tw_v, _tw_k);");
-    };
-    cg.addBlock("if (threadIdx.x < 32u)", [&]() {
-        warpMerge("_ts_v", "_ts_k", "(int)(blockDim.x >> 5) * " + K, false);
-        cg.addBlock("if (threadIdx.x == 0u)", [&]() {
-            cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { " + out_ + "_pvals[blockIdx.x * " + K + " + _q] = _tw_v[_q]; " +
-                       out_ + "_pkeys[blockIdx.x * " + K + " + _q] = _tw_k[_q]; }");
-            cg.addLine("__threadfence();");
-            cg.addLine("_t_last = (atomicAdd(" + out_ + "_ticket, 1u) == gridDim.x - 1u);");
-        });
-    });
-    cg.addLine("__syncthreads();");
-    cg.addBlock("if (_t_last && threadIdx.x < 32u)", [&]() {
-        cg.addLine("__threadfence();");
-        warpMerge(out_ + "_pvals", out_ + "_pkeys", "(int)gridDim.x * " + K, true);
+        cg.addLine("for (int _e = (int)threadIdx.x; _e < (int)gridDim.x * " + K + "; _e += (int)blockDim.x) gpudb_topk_push<" +
+                   K + ">(_tk_v, _tk_k, __ldcg(" + out_ + "_pvals + _e), __ldcg(" + out_ + "_pkeys + _e));");
+        blockMerge();
         cg.addBlock("if (threadIdx.x == 0u)", [&]() {
             cg.addLine("unsigned long long _cnt = 0ull;");
             cg.addBlock("for (int _q = 0; _q < " + K + "; ++_q)", [&]() {

@@ -65,10 +65,13 @@ public:
     struct ColumnDesc {
         std::string paramName;
         std::string cudaType;
+        bool late = false;  // read at consumption through its global pointer, never staged
     };
     CudaGridStrideScan(const std::string& table, const std::string& rowVar = "row",
                        const std::string& idxVar = "i");
-    void addColumn(const std::string& paramName, const std::string& cudaType);
+    // `late` columns are only touched by rows that survive earlier
+    // selections (late materialisation): the TMA ring does not stage them.
+    void addColumn(const std::string& paramName, const std::string& cudaType, bool late = false);
     void setConfig(const ScanConfig& c) { cfg_ = c; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;

@@ -96,7 +96,8 @@ std::string TuneConfig::toString() const {
     o << "bs=" << blockSize << ";scan=" << (scan.mode == ScanConfig::TmaBulk ? "tma" : "direct")
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
-      << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe;
+      << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
+      << ";late=" << (lateMaterialize ? 1 : 0);
     return o.str();
 }
 
@@ -118,6 +119,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "warp") t.warpAggregate = std::stoi(v) != 0;
         else if (k == "keyed") t.keyedStrategy = std::stoi(v);
         else if (k == "probe") t.maxProbe = std::stoi(v);
+        else if (k == "late") t.lateMaterialize = std::stoi(v) != 0;
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -157,12 +159,15 @@ struct Spec {
 
 std::string L(long long v) { return std::to_string(v) + "ll"; }
 
+// `late` names columns read only by rows that survive a selective operator
+// (semi-join / hash probe); with late materialisation they are not staged.
 std::unique_ptr<CudaGridStrideScan> makeScan(CudaQueryPlan& plan, const std::string& table,
                                              const std::vector<std::string>& cols, const TuneConfig& tune,
-                                             bool allowTma = true) {
+                                             bool allowTma = true, const std::vector<std::string>& late = {}) {
     const TableDef& td = catalogTable(table);
     auto scan = std::make_unique<CudaGridStrideScan>(table, "row", "i");
     for (const auto& c : cols) scan->addColumn(c, td.col(c).cudaType);
+    for (const auto& c : late) scan->addColumn(c, td.col(c).cudaType, tune.lateMaterialize);
     ScanConfig sc = tune.scan;
     if (!allowTma) sc.mode = ScanConfig::Direct;
     scan->setConfig(sc);
@@ -255,7 +260,7 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
     }
     const std::string cap = "2 * max(jt_groups, 1)";
     {
-        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day", "p_price", "p_discount"}, tune);
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune, true, {"p_price", "p_discount"});
         auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
         auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
         auto gb = std::make_unique<CudaHashGroupBy>(std::move(pr), "jg", "p_fk[i]", "int", cap, HashLayout::Linear,
@@ -409,7 +414,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
             auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "mj_bitmap", "md_key[i]", "max_md_key / 32 + 1");
             appendPhase(plan, "MIXJ_build", std::move(bm), tune);
         }
-        auto scan = makeScan(plan, "mix", {"m_fk", "m_filter", "m_value"}, tune);
+        auto scan = makeScan(plan, "mix", {"m_fk", "m_filter"}, tune, true, {"m_value"});
         auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
         auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "mj_bitmap", "m_fk[i]");
         auto r = std::make_unique<CudaTGReduce>(std::move(pr), "d_mixj");

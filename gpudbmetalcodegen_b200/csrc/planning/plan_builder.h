@@ -101,6 +101,7 @@ struct TuneConfig {
     bool warpAggregate = true;  // match_any pre-aggregation in hash / atomic aggregation
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
     int maxProbe = 128;
+    bool lateMaterialize = true;  // columns read only by surviving rows are not staged
     std::string toString() const;
     static TuneConfig parse(const std::string& s);  // "bs=512;scan=tma;tile=1024;stages=4;..."
 };

@@ -103,7 +103,7 @@ def load_join(ctx, nd, npr, seed=3):
     return d, p
 
 
-@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0"])
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0", "late=0", "bs=1024;tile=2048;stages=3"])
 def test_join_topk_parity(ctx, tune):
     d, p = load_join(ctx, 200_000, 800_000)
     top, groups, distinct = O.join_topk(d, p, k=10)
