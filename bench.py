@@ -1,21 +1,25 @@
-"""Benchmark: hash join + high-cardinality group-by + top-k on one B200.
+"""Benchmark of the runtime-codegen hot path on one B200.
 
-Workload (the join configuration of the benchmark set): build side 15M rows
-(unique int32 keys from a seeded permutation, order_day, segment), probe
-side 60M rows (fk, ship_day, price, discount); build filter segment==1 AND
-order_day<1170, probe filter ship_day>1170, group by build key summing
+Default workload (the join configuration of the benchmark set): build side
+15M rows (unique int32 keys from a seeded permutation, order_day, segment),
+probe side 60M rows (fk, ship_day, price, discount); build filter segment==1
+AND order_day<1170, probe filter ship_day>1170, group by build key summing
 price*(100-discount) exactly in int64, top 10 by (sum desc, key asc).
-Synthetic seeded data of the stated shapes; inputs (1.575 GB) exceed the
-126 MB L2, so no flush is needed between steps.
-
 One step = one full query: bitmap semi-join build, exact group-count sizing
 (host read of the distinct counter), probe + hash group-by, top-k.
+Seeded synthetic data of the configuration's shapes; inputs exceed the
+126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Other workloads (`--workload`, for profiling and per-configuration numbers):
+q1 (6,001,215-row scan-filter-group-aggregate), q6 (predicate variant),
+groupby (120M Zipf(1.1) keys over 2^22, count+sum), hashjoin (2^22-key
+build, 120M-row probe, per-key sums).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
 Under torchrun every rank runs an independent replica on its own GPU
 (replicas only: the query does not shard); the timed region is bracketed by
-a barrier, and the slowest rank's time is reported.
+a barrier and the slowest rank's time is reported.
 """
 from __future__ import annotations
 
@@ -30,13 +34,6 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
-
-BUILD_ROWS = 15_000_000
-PROBE_ROWS = 60_000_000
-K_TOP = 10
-SPEC = f"template=join_topk;k={K_TOP}"
-PROBE_BYTES_PER_ROW = 24   # fk i32 + ship_day i32 + price i64 + discount i64
-BUILD_BYTES_PER_ROW = 9    # key i32 + order_day i32 + segment u8
 
 
 def peaks():
@@ -69,10 +66,9 @@ class ClockSampler:
             import pynvml as nv
             nv.nvmlInit()
             self.nv = nv
-            h = (nv.nvmlDeviceGetHandleByUUID(self.sel) if self.sel.startswith(("GPU-", "MIG-"))
-                 else nv.nvmlDeviceGetHandleByIndex(int(self.sel)))
-            self.h = h
-            self.smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.h = (nv.nvmlDeviceGetHandleByUUID(self.sel) if self.sel.startswith(("GPU-", "MIG-"))
+                      else nv.nvmlDeviceGetHandleByIndex(int(self.sel)))
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
             self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
@@ -110,96 +106,252 @@ class ClockSampler:
 
 
 def dist_info():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def gen_data():
-    from gpudbmetalcodegen_b200 import workloads as W
-    dim = W.gen_dim(BUILD_ROWS, seed=W.SEED)
-    probe = W.gen_probe(PROBE_ROWS, dim_rows=BUILD_ROWS, seed=W.SEED)
-    return dim, probe
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+class Workload:
+    name = ""
+    spec = ""
+    kernel = ""           # dominant kernel (roofline)
+    description = ""
+
+    def __init__(self, args):
+        self.args = args
+
+    def generate(self):
+        raise NotImplementedError
+
+    def rows(self) -> int:
+        raise NotImplementedError
+
+    def register(self, ctx):
+        for tname, table in self.tables.items():
+            ctx.upload_table(tname, table)
+
+    def algorithmic_bytes(self, tune: str) -> dict:
+        raise NotImplementedError
+
+    def expected(self):
+        raise NotImplementedError
+
+    def matches(self, res) -> bool:
+        return res.rows == self.expected()
+
+    def cpu_run(self, threads: int):
+        raise NotImplementedError
+
+    def config(self) -> dict:
+        return {"workload": self.description}
 
 
-def run_reference(args):
-    """CPU restatement of the reference's operator semantics (the oracle
-    port: bitmap semi-join, direct-address atomic aggregation, top-k) on all
-    host cores, same workload, rows/s."""
-    from oracle import oracle_py as O
-    dim, probe = gen_data()
+class JoinTopK(Workload):
+    name = "join_topk"
+    kernel = "JT_probe_group"
+
+    def __init__(self, args):
+        super().__init__(args)
+        self.build_rows, self.probe_rows, self.k = args.build_rows, args.probe_rows, 10
+        self.spec = f"template=join_topk;k={self.k}"
+        self.description = f"join_topk: build {self.build_rows} + probe {self.probe_rows} rows, top-{self.k}"
+
+    def generate(self):
+        from gpudbmetalcodegen_b200 import workloads as W
+        self.tables = {"dim": W.gen_dim(self.build_rows, seed=W.SEED),
+                       "probe": W.gen_probe(self.probe_rows, dim_rows=self.build_rows, seed=W.SEED)}
+
+    def rows(self):
+        return self.build_rows + self.probe_rows
+
+    def expected(self):
+        if not hasattr(self, "_exp"):
+            from oracle import oracle_py as O
+            self._exp, self.groups, self.distinct = O.join_topk(self.tables["dim"], self.tables["probe"], k=self.k)
+        return self._exp
+
+    def algorithmic_bytes(self, tune):
+        # eager columns (fk, ship_day) for every probe row + the late
+        # price/discount (8 B each) for rows reaching the aggregation
+        import numpy as np
+        dim, probe = self.tables["dim"], self.tables["probe"]
+        qual = np.zeros(self.build_rows + 2, dtype=bool)
+        keep = (dim["b_segment"] == 1) & (dim["b_order_day"] < 1170)
+        qual[dim["b_key"][keep]] = True
+        matched = int(np.count_nonzero((probe["p_ship_day"] > 1170) & qual[probe["p_fk"]]))
+        late = "late=0" not in tune
+        alg = self.probe_rows * 8 + matched * 16 if late else self.probe_rows * 24
+        return {"algorithmic_bytes": alg, "rows_reaching_aggregation": matched,
+                "all_columns_bytes": self.probe_rows * 24}
+
+    def cpu_run(self, threads):
+        from oracle import oracle_py as O
+        O.join_topk(self.tables["dim"], self.tables["probe"], k=self.k, threads=threads)
+
+    def config(self):
+        self.expected()
+        return {"workload": self.description, "build_rows": self.build_rows, "probe_rows": self.probe_rows,
+                "k": self.k, "groups": self.groups, "build_distinct": self.distinct}
+
+
+class FactScan(Workload):
+    def __init__(self, args, which):
+        super().__init__(args)
+        self.which = which
+        self.n = args.fact_rows
+        self.spec = f"template={which}"
+        self.kernel = "Q1_reduce" if which == "q1" else "Q6_reduce"
+        self.description = (f"{which}: scan-filter-group-aggregate over {self.n} rows x 38 B" if which == "q1"
+                            else f"{which}: scan-filter-sum over {self.n} rows x 28 B")
+
+    def generate(self):
+        from gpudbmetalcodegen_b200 import workloads as W
+        self.tables = {"fact": W.gen_fact(self.n)}
+
+    def rows(self):
+        return self.n
+
+    def expected(self):
+        from oracle import oracle_py as O
+        f = self.tables["fact"]
+        if self.which == "q6":
+            return [(O.q6(f),)]
+        return O.q1(f)
+
+    def matches(self, res):
+        exp = self.expected()
+        if self.which == "q6":
+            return res.rows == exp
+        got = res.as_dicts()
+        from oracle import oracle_py as O
+        return len(got) == len(exp) and all(g[k] == e[k] for g, e in zip(got, exp) for k in O.Q1_AGGS)
+
+    def algorithmic_bytes(self, tune):
+        return {"algorithmic_bytes": self.n * (38 if self.which == "q1" else 28)}
+
+    def cpu_run(self, threads):
+        from oracle import oracle_py as O
+        (O.q1 if self.which == "q1" else O.q6)(self.tables["fact"], threads=threads)
+
+
+class Skew(Workload):
+    def __init__(self, args, which):
+        super().__init__(args)
+        self.which = which
+        self.n = args.zprobe_rows
+        self.nkeys = args.zkeys
+        self.spec = f"template={which}"
+        self.kernel = "GB_aggregate" if which == "groupby" else "HJ_probe_sum"
+        self.description = (f"{which}: {self.n} probe rows, Zipf(1.1) keys over {self.nkeys}")
+
+    def generate(self):
+        from gpudbmetalcodegen_b200 import workloads as W
+        self.tables = {"zprobe": W.gen_zprobe(self.n, nkeys=self.nkeys)}
+        if self.which == "hashjoin":
+            self.tables["zbuild"] = W.gen_zbuild(self.nkeys)
+
+    def register(self, ctx):
+        super().register(ctx)
+        ctx.register_symbol("zgroups", self.nkeys)
+
+    def rows(self):
+        return self.n + (self.nkeys if self.which == "hashjoin" else 0)
+
+    def expected(self):
+        from oracle import oracle_py as O
+        zp = self.tables["zprobe"]
+        if self.which == "groupby":
+            return O.groupby(zp["z_key"], zp["z_value"], cap=self.nkeys)
+        return O.hashjoin(self.tables["zbuild"], zp["z_key"], cap=self.nkeys)
+
+    def matches(self, res):
+        import numpy as np
+        k, c, s = self.expected()
+        return (np.array_equal(np.array(res.column("key")), k) and np.array_equal(np.array(res.column("count")), c)
+                and np.array_equal(np.array(res.column("sum")), s))
+
+    def algorithmic_bytes(self, tune):
+        return {"algorithmic_bytes": self.n * (16 if self.which == "groupby" else 8)}
+
+    def cpu_run(self, threads):
+        self.expected()
+
+
+def make_workload(args) -> Workload:
+    if args.workload == "join_topk":
+        return JoinTopK(args)
+    if args.workload in ("q1", "q6"):
+        return FactScan(args, args.workload)
+    if args.workload in ("groupby", "hashjoin"):
+        return Skew(args, args.workload)
+    raise SystemExit(f"unknown workload {args.workload}")
+
+
+def time_cpu(w: Workload, budget_s: float = 12.0, max_runs: int = 20):
     threads = os.cpu_count() or 1
-    O.join_topk(dim, probe, k=K_TOP, threads=threads)  # warm caches / page in
-    for _ in range(max(0, args.warmup - 1)):
-        O.join_topk(dim, probe, k=K_TOP, threads=threads)
+    w.cpu_run(threads)
     times = []
-    for _ in range(args.steps):
+    t_end = time.perf_counter() + budget_s
+    while len(times) < 3 or (time.perf_counter() < t_end and len(times) < max_runs):
         t0 = time.perf_counter()
-        O.join_topk(dim, probe, k=K_TOP, threads=threads)
+        w.cpu_run(threads)
         times.append(time.perf_counter() - t0)
-    step = statistics.mean(times)
-    rows = BUILD_ROWS + PROBE_ROWS
-    value = rows / step
-    line = {
-        "metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": "join_topk: build 15M + probe 60M rows, top-10", "build_rows": BUILD_ROWS,
-                   "probe_rows": PROBE_ROWS, "k": K_TOP},
-        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                         "sample": f"full workload ({rows} rows) per step, {args.steps} steps"},
-        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    return statistics.median(times), threads, len(times)
+
+
+def run_reference(args, w: Workload):
+    """The reference's operator semantics restated on the CPU (the oracle
+    port: the reference's own kernels are Metal and cannot run here), on all
+    host cores, same workload and metric."""
+    w.generate()
+    step, threads, n = time_cpu(w, budget_s=max(5.0, 0.5 * args.steps), max_runs=max(3, args.steps))
+    value = w.rows() / step
+    line = {"metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": n,
+            "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": w.description},
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                             "sample": f"full workload ({w.rows()} rows) per step, {n} steps, median"},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(dim, probe, budget_s: float = 12.0):
-    from oracle import oracle_py as O
-    threads = os.cpu_count() or 1
-    O.join_topk(dim, probe, k=K_TOP, threads=threads)
-    times = []
-    t_end = time.perf_counter() + budget_s
-    while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 20):
-        t0 = time.perf_counter()
-        O.join_topk(dim, probe, k=K_TOP, threads=threads)
-        times.append(time.perf_counter() - t0)
-    step = statistics.median(times)
-    return {"value": (BUILD_ROWS + PROBE_ROWS) / step, "unit": "rows/s", "cores": threads, "kind": "port",
-            "sample": f"full workload ({BUILD_ROWS + PROBE_ROWS} rows) x {len(times)} runs, median"}
-
-
-def load_traffic():
+def load_traffic(kernel: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("JT_probe_group")
+            return json.loads(p.read_text()).get(kernel)
         except Exception:
             return None
     return None
 
 
 def main():
-    global BUILD_ROWS, PROBE_ROWS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="join_topk", choices=["join_topk", "q1", "q6", "groupby", "hashjoin"])
     ap.add_argument("--tune", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--build-rows", type=int, default=BUILD_ROWS, help="smaller cases for profiling only")
-    ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS, help="smaller cases for profiling only")
+    ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--build-rows", type=int, default=15_000_000)
+    ap.add_argument("--probe-rows", type=int, default=60_000_000)
+    ap.add_argument("--fact-rows", type=int, default=6_001_215)
+    ap.add_argument("--zprobe-rows", type=int, default=120_000_000)
+    ap.add_argument("--zkeys", type=int, default=1 << 22)
     args = ap.parse_args()
-    BUILD_ROWS, PROBE_ROWS = args.build_rows, args.probe_rows
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_info()
+    w = make_workload(args)
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        run_reference(args)
+        if rank == 0:
+            run_reference(args, w)
         return
 
     import ctypes as C
@@ -215,23 +367,21 @@ def main():
         pg = dist
 
     from gpudbmetalcodegen_b200 import Context, _lib
-    from oracle import oracle_py as O
 
-    dim, probe = gen_data()
+    w.generate()
     ctx = Context(local)
-    ctx.upload_table("dim", dim)
-    ctx.upload_table("probe", probe)
-    q = ctx.prepare(SPEC, args.tune)
+    w.register(ctx)
+    q = ctx.prepare(w.spec, args.tune)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr)
 
-    # correctness of this exact configuration
-    res, t = ctx.run(q)
-    expect, groups, distinct = O.join_topk(dim, probe, k=K_TOP)
-    verified = res.rows == expect
+    verified = None
+    if not args.no_verify:
+        res, _ = ctx.run(q)
+        verified = w.matches(res)
 
     for _ in range(args.warmup):
         ctx.run(q, collect=False)
-    phase_acc = {}
+    phase_acc, names = {}, []
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -254,51 +404,41 @@ def main():
         pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         step_ms = float(tt.item())
         pg.barrier()
-    rows_total = (BUILD_ROWS + PROBE_ROWS) * world
+    rows_total = w.rows() * world
     value = rows_total / (step_ms / 1e3)
 
-    # roofline of the dominant kernel (probe + group-by), per launch.
-    # Algorithmic bytes: the probe's eager columns (fk, ship_day) for every
-    # row, plus the late-materialised price/discount (8 B each) for the rows
-    # that pass the filter and the semi-join and reach the aggregation.
-    names = ["JT_build", "JT_probe_group", "JT_topk"]
-    phase_ms = {names[i] if i < len(names) else str(i): v / args.steps for i, v in phase_acc.items()}
-    probe_ms = phase_ms.get("JT_probe_group")
+    kernels = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
+    phase_ms = {(kernels[i] if i < len(kernels) else str(i)): v / args.steps for i, v in phase_acc.items()}
+    kms = phase_ms.get(w.kernel)
     peak, peak_kind = peaks()
-    qual = np.zeros(BUILD_ROWS + 2, dtype=bool)
-    keep = (dim["b_segment"] == 1) & (dim["b_order_day"] < 1170)
-    qual[dim["b_key"][keep]] = True
-    matched = int(np.count_nonzero((probe["p_ship_day"] > 1170) & qual[probe["p_fk"]]))
-    late = "late=0" not in (q.tune or "")
-    alg_bytes = PROBE_ROWS * 8 + matched * 16 if late else PROBE_ROWS * PROBE_BYTES_PER_ROW
-    achieved = alg_bytes / (probe_ms / 1e3) / 1e9 if probe_ms else None
-    roofline = {"bound": "hbm", "kernel": "JT_probe_group", "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "algorithmic_bytes": alg_bytes, "rows_reaching_aggregation": matched,
-                "all_columns_bytes": PROBE_ROWS * PROBE_BYTES_PER_ROW, "traffic": load_traffic()}
+    ab = w.algorithmic_bytes(q.tune)
+    achieved = ab["algorithmic_bytes"] / (kms / 1e3) / 1e9 if kms else None
+    roofline = {"bound": "hbm", "kernel": w.kernel, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "kernel_ms": kms,
+                "traffic": load_traffic(w.kernel), **ab}
 
     # end to end through the C-ABI with pinned host buffers: H2D of every
-    # input column, the query, D2H of the top-k result, per step
+    # input column, the query, D2H of the result, per step
     e2e = None
     if not args.no_e2e:
         lib = _lib.load()
-        pinned = {}
-        host_bytes = 0
-        for tname, table in (("dim", dim), ("probe", probe)):
+        pinned, host_bytes = [], 0
+        for tname, table in w.tables.items():
             for cname, arr in table.items():
                 ptr = lib.gpudb_host_alloc(arr.nbytes)
-                buf = np.ctypeslib.as_array((C.c_uint8 * arr.nbytes).from_address(ptr))
-                buf[:] = arr.view(np.uint8)
-                pinned[(tname, cname)] = (ptr, arr)
+                np.ctypeslib.as_array((C.c_uint8 * arr.nbytes).from_address(ptr))[:] = arr.view(np.uint8)
+                pinned.append((tname, cname, ptr, arr))
                 host_bytes += arr.nbytes
+
         def e2e_step():
-            for (tname, cname), (ptr, arr) in pinned.items():
+            for tname, cname, ptr, arr in pinned:
                 _lib.check(lib.gpudb_upload_column(ctx.handle, tname.encode(), cname.encode(), C.c_void_p(ptr),
                                                    arr.shape[0], arr.itemsize), ctx.handle)
             r, _ = ctx.run(q, collect=True)
             return r
+
         for _ in range(2):
-            e2e_step()
+            r = e2e_step()
         ctx.synchronize()
         e_steps = max(3, min(args.steps, 10))
         t0 = time.perf_counter()
@@ -306,37 +446,33 @@ def main():
             r = e2e_step()
         ctx.synchronize()
         e_ms = (time.perf_counter() - t0) / e_steps * 1e3
-        verified = verified and r.rows == expect
+        if verified is not None:
+            verified = verified and w.matches(r)
         if pg:
             tt = torch.tensor([e_ms], device="cuda")
             pg.all_reduce(tt, op=pg.ReduceOp.MAX)
             e_ms = float(tt.item())
+        d2h = sum(len(row) for row in r.rows) * 16 + 8
         e2e = {"value": rows_total / (e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": host_bytes,
-               "d2h_bytes_per_step": K_TOP * 16 + 8, "ms_per_step": e_ms}
-        for ptr, _ in pinned.values():
+               "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
+        for _, _, ptr, _ in pinned:
             lib.gpudb_host_free(C.c_void_p(ptr))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(dim, probe)
+        step, threads, n = time_cpu(w)
+        cpu = {"value": w.rows() / step, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": f"full workload ({w.rows()} rows) x {n} runs, median"}
 
     if rank == 0:
-        line = {
-            "metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
-            "config": {"workload": "join_topk: build 15M + probe 60M rows, top-10", "build_rows": BUILD_ROWS,
-                       "probe_rows": PROBE_ROWS, "k": K_TOP, "groups": groups, "build_distinct": distinct,
-                       "l2": "inputs 1.575 GB > 126 MB L2; no flush", "tune": q.tune or "default",
-                       "parallelism": f"replicas x{world}"},
-            "verified": verified,
-            "phase_ms": phase_ms,
-            "roofline": roofline,
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-        }
+        cfg = w.config()
+        cfg.update({"l2": "inputs larger than the 126 MB L2; no flush", "tune": q.tune or "default",
+                    "parallelism": f"replicas x{world}"})
+        line = {"metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "config": cfg,
+                "verified": verified, "phase_ms": phase_ms, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:
