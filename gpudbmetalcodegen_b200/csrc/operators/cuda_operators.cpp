@@ -76,7 +76,15 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
 
     // ---- TMA bulk staged tile loop ------------------------------------
     const int bs = cg.currentThreadgroupSize();
-    const int tile = cfg_.tileRows;
+    int tile = cfg_.tileRows;
+    if (tile <= 0) {
+        // auto: about 24 KB of staged columns per stage, 1024..8192 rows
+        long long rowBytes = 0;
+        for (const auto& c : columns_)
+            if (!c.late) rowBytes += (long long)cudaTypeBytes(c.cudaType);
+        tile = 1024;
+        while (tile < 8192 && (long long)tile * 2 * rowBytes <= 24 * 1024) tile *= 2;
+    }
     int stages = cfg_.stages;
     if (tile <= 0 || tile % 16 != 0)
         throw std::runtime_error("CudaGridStrideScan: tileRows must be a positive multiple of 16");
@@ -485,7 +493,7 @@ CudaKeyedAgg::Strategy CudaKeyedAgg::chosenStrategy() const {
         return strategy_;
     }
     if (!allAdds) return Strategy::Global;
-    if (numBuckets_ * (int)aggregates_.size() <= 64 && numBuckets_ <= 16) return Strategy::Registers;
+    if (numBuckets_ * (int)aggregates_.size() <= 64 && numBuckets_ <= 16) return Strategy::RegistersSwitch;
     if ((long long)numBuckets_ * valuesPerBucket_ <= 16384) return Strategy::Shared;
     return Strategy::Global;
 }
@@ -503,7 +511,7 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
             cg.addLine("const long long _kv" + S(j) + " = (long long)(" + aggregates_[j].valueExpr + ");");
     };
 
-    if (st == Strategy::Registers) {
+    if (st == Strategy::Registers || st == Strategy::RegistersSwitch) {
         cg.addComment("keyed aggregation: per-thread register accumulators (" + S(nb) + " buckets x " + S(na) +
                       " aggregates), predicated on the bucket id");
         for (int j = 0; j < na; j++) {
@@ -513,11 +521,24 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
         }
         child_->produce(cg, [&]() {
             emitValues();
-            cg.addLine("#pragma unroll");
-            cg.addBlock("for (int _b = 0; _b < " + S(nb) + "; ++_b)", [&]() {
-                cg.addLine("const bool _hit = (_bucket == _b);");
-                for (int j = 0; j < na; j++) cg.addLine("_ka" + S(j) + "[_b] += _hit ? _kv" + S(j) + " : 0ll;");
-            });
+            if (st == Strategy::RegistersSwitch) {
+                // one path per bucket: a row pays only its own bucket's adds;
+                // a warp executes the paths of the buckets its rows hit
+                cg.addBlock("switch (_bucket)", [&]() {
+                    for (int b = 0; b < nb; b++) {
+                        std::string body = "case " + S(b) + ":";
+                        for (int j = 0; j < na; j++) body += " _ka" + S(j) + "[" + S(b) + "] += _kv" + S(j) + ";";
+                        cg.addLine(body + " break;");
+                    }
+                    cg.addLine("default: gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); break;");
+                });
+            } else {
+                cg.addLine("#pragma unroll");
+                cg.addBlock("for (int _b = 0; _b < " + S(nb) + "; ++_b)", [&]() {
+                    cg.addLine("const bool _hit = (_bucket == _b);");
+                    for (int j = 0; j < na; j++) cg.addLine("_ka" + S(j) + "[_b] += _hit ? _kv" + S(j) + " : 0ll;");
+                });
+            }
             consume();
         });
         const int nacc = nb * na;
@@ -594,7 +615,7 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
 }
 
 std::string CudaKeyedAgg::describe() const {
-    static const char* names[] = {"auto", "registers", "shared", "global"};
+    static const char* names[] = {"auto", "registers", "shared", "global", "registers-switch"};
     return "KeyedAgg(" + outputArrayName_ + ", " + S(numBuckets_) + " buckets, " + S((long long)aggregates_.size()) +
            " aggs, " + names[(int)chosenStrategy()] + ") <- " + describeChain();
 }

@@ -46,8 +46,8 @@ public:
 struct ScanConfig {
     enum Mode { Direct, TmaBulk };
     Mode mode = TmaBulk;
-    int tileRows = 1024;   // rows per TMA tile (multiple of 16 and of the block size)
-    int stages = 4;        // TMA ring depth
+    int tileRows = 0;      // rows per TMA tile (multiple of 16); 0 = about 24 KB of staged columns
+    int stages = 4;        // TMA ring depth (clamped to the shared-memory budget)
 };
 
 // ------------------------------------------------------------------
@@ -245,7 +245,9 @@ public:
         bool isWide = false;
         int scaleDown = 0;
     };
-    enum class Strategy { Auto, Registers, Shared, Global };
+    // Registers: predicated update of every bucket's accumulators per row;
+    // RegistersSwitch: a switch on the bucket, each row updates only its own.
+    enum class Strategy { Auto, Registers, Shared, Global, RegistersSwitch };
     CudaKeyedAgg(std::unique_ptr<CudaOperator> child, const std::string& outputArrayName,
                  const std::string& bucketExpr, int numBuckets, int valuesPerBucket,
                  const std::string& sizeExpr = "");

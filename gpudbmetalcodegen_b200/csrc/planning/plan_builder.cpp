@@ -97,7 +97,7 @@ std::string TuneConfig::toString() const {
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
-      << ";late=" << (lateMaterialize ? 1 : 0);
+      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM;
     return o.str();
 }
 
@@ -120,11 +120,12 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "keyed") t.keyedStrategy = std::stoi(v);
         else if (k == "probe") t.maxProbe = std::stoi(v);
         else if (k == "late") t.lateMaterialize = std::stoi(v) != 0;
+        else if (k == "occ") t.minBlocksPerSM = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
         throw std::runtime_error("tune: bs must be a multiple of 32 in [32,1024]");
-    if (t.scan.tileRows % t.blockSize) t.scan.tileRows = ((t.scan.tileRows + t.blockSize - 1) / t.blockSize) * t.blockSize;
+    if (t.scan.tileRows < 0 || t.scan.tileRows % 16) throw std::runtime_error("tune: tile must be a multiple of 16 (0 = auto)");
     return t;
 }
 
@@ -183,6 +184,7 @@ CudaQueryPlan::Phase& appendPhase(CudaQueryPlan& plan, const std::string& name, 
     ph.name = name;
     ph.root = std::move(root);
     ph.threadgroupSize = tune.blockSize;
+    ph.minBlocksPerSM = std::max(1, std::min(tune.minBlocksPerSM, 2048 / tune.blockSize));
     plan.phases.push_back(std::move(ph));
     return plan.phases.back();
 }

@@ -97,7 +97,8 @@ struct TuneConfig {
     int blockSize = 512;
     ScanConfig scan;
     HashLayout hashLayout = HashLayout::Linear;
-    int smemPreAggLog2 = 0;     // hash group-by shared-memory table (0 = off)
+    int smemPreAggLog2 = 10;    // hash group-by shared-memory table (0 = off)
+    int minBlocksPerSM = 1;     // __launch_bounds__ occupancy hint (caps registers)
     bool warpAggregate = true;  // match_any pre-aggregation in hash / atomic aggregation
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
     int maxProbe = 128;

@@ -39,7 +39,7 @@ def test_q1_structure_matches_reference_plan():
     src, plan = q.source, q.plan
     # reference Q1: one phase, KeyedAgg(6 buckets) <- Selection <- Scan(lineitem)
     assert plan.count("phase ") == 1 and "Q1_reduce" in plan
-    assert "KeyedAgg(d_q1_aggs, 6 buckets, 6 aggs, registers)" in plan
+    assert "KeyedAgg(d_q1_aggs, 6 buckets, 6 aggs, registers-switch)" in plan
     assert "f_ship_day[i] <= 2436" in src
     # reference bucket expression (metal_plan_builder.cpp:335)
     assert "(f_flag_a[i] == 'A' ? 0 : (f_flag_a[i] == 'N' ? 2 : 4)) + (f_flag_b[i] == 'F' ? 0 : 1)" in src

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 REL = 1e-12
 
 Q1_TUNES = ["", "scan=direct", "bs=256;tile=1024;stages=2", "bs=1024;tile=2048;stages=3", "bs=128;tile=512;stages=8",
-            "keyed=2", "keyed=3"]
+            "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3"]
 
 
 def assert_q1_equal(res, expect):
