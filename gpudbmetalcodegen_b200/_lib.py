@@ -115,6 +115,33 @@ _SIGNATURES = [
     ("gpudb_gen_mix", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
      + [C.c_void_p] * 5 + [C.c_int]),
     ("gpudb_gen_mixdim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    # gpudb_batch.h
+    ("gpudb_sizer_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("gpudb_sizer_free", None, [C.c_void_p]),
+    ("gpudb_sizer_param_count", C.c_int, []),
+    ("gpudb_sizer_get_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gpudb_sizer_set_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gpudb_sizer_grads", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.POINTER(C.c_float)]),
+    ("gpudb_sizer_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                    C.c_uint64, C.POINTER(C.c_float)]),
+    ("gpudb_sizer_predict", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    ("gpudb_batch_create", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("gpudb_batch_free", None, [C.c_void_p]),
+    ("gpudb_batch_set_queries", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_batch_set_groups", C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
+    ("gpudb_batch_set_tuning", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("gpudb_batch_execute", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p]),
+    ("gpudb_batch_exact_stats", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    ("gpudb_batch_features", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    ("gpudb_batch_result_scalar", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
+                                            C.POINTER(C.c_int64)]),
+    ("gpudb_batch_result_groups", C.c_int, [C.c_void_p, C.c_int, C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
+                                            C.c_void_p, C.c_void_p]),
+    ("gpudb_batch_result_topk", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    ("gpudb_batch_collect", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                                      C.POINTER(C.c_double)]),
+    ("gpudb_batch_last_launches", C.c_longlong, [C.c_void_p]),
 ]
 
 EXPORTED = [s[0] for s in _SIGNATURES]

@@ -1,0 +1,595 @@
+"""Batched mixed queries, the learned sizer and the plain per-query path.
+
+Python face of include/gpudb_batch.h. The reference runs one query per
+invocation and sizes every table by an exact max-key pass
+(codegen/execution/max_key_symbols.cpp:188-235); here many queries of the
+four mixed templates run as one set of persistent work-queue kernels, and
+their hash tables are sized by an MLP trained on the engine's own logged
+executions, with the exact per-query path as fallback when a table
+overflows. Every path returns the same canonical results:
+
+    agg / join : ("scalar", count, sum)
+    groupby    : ("groups", keys, counts, sums)  numpy int64, sorted by key
+    topk       : ("topk", ((key, sum), ...))     best first
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field, replace
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+TEMPLATES = ("agg", "join", "groupby", "topk")
+TPL = {name: i for i, name in enumerate(TEMPLATES)}
+DEVERR_HASH_OVERFLOW = 0x1
+SIZER_FEATURES = 16
+SIZER_OUTPUTS = 2
+CARD_SCALE = 24.0  # sizer output 0 = log2(groups + 1) / CARD_SCALE
+
+
+class BatchQueryStruct(C.Structure):
+    """gpudb_batch_query (include/gpudb_batch.h)."""
+    _fields_ = [("tmpl", C.c_int), ("thr", C.c_int32), ("card", C.c_int64), ("k", C.c_int32),
+                ("attr_lt", C.c_int32), ("rows", C.c_uint64), ("key", C.c_void_p), ("filter", C.c_void_p),
+                ("value", C.c_void_p), ("fk", C.c_void_p), ("dim_key", C.c_void_p), ("dim_attr", C.c_void_p),
+                ("dim_rows", C.c_uint64), ("dim_max_key", C.c_int64), ("groups", C.c_uint64),
+                ("key_min", C.c_int64), ("key_max", C.c_int64), ("filter_min", C.c_int32),
+                ("filter_max", C.c_int32)]
+
+
+@dataclass(frozen=True)
+class MixQuery:
+    """One query of the mixed workload over a slice of a resident mix table."""
+    tmpl: str                # agg | join | groupby | topk
+    table: int               # index of the resident mix table
+    row0: int
+    rows: int
+    thr: int                 # m_filter < thr
+    key: str = "m_rank_u"    # group key column: m_rank_u (uniform) or m_rank_z (Zipf)
+    card: int = 1            # group key = key % card
+    k: int = 10              # top-k
+    attr_lt: int = 500       # join: mixdim rows with md_attr < attr_lt
+
+    @property
+    def grouped(self) -> bool:
+        return self.tmpl in ("groupby", "topk")
+
+
+# ---------------------------------------------------------------------------
+# canonical results
+# ---------------------------------------------------------------------------
+def canonical_groups(keys, counts, sums):
+    keys = np.asarray(keys, dtype=np.int64)
+    order = np.argsort(keys, kind="stable")
+    return ("groups", keys[order], np.asarray(counts, dtype=np.int64)[order],
+            np.asarray(sums, dtype=np.int64)[order])
+
+
+def same_result(a, b) -> bool:
+    if a[0] != b[0]:
+        return False
+    if a[0] == "groups":
+        return all(np.array_equal(x, y) for x, y in zip(a[1:], b[1:]))
+    return tuple(a[1:]) == tuple(b[1:])
+
+
+def describe_difference(a, b) -> str:
+    if a[0] != b[0]:
+        return f"kind {a[0]} vs {b[0]}"
+    if a[0] == "groups":
+        if a[1].shape != b[1].shape:
+            return f"{a[1].shape[0]} vs {b[1].shape[0]} groups"
+        for name, x, y in zip(("keys", "counts", "sums"), a[1:], b[1:]):
+            bad = np.nonzero(x != y)[0]
+            if bad.size:
+                return f"{name} differ at {bad.size} rows, first row {bad[0]}: {x[bad[0]]} vs {y[bad[0]]}"
+        return "equal"
+    return f"{a[1:]} vs {b[1:]}"
+
+
+# ---------------------------------------------------------------------------
+# resident tables
+# ---------------------------------------------------------------------------
+class MixTables:
+    """Resident mixed-workload tables: several mix tables (one Zipf exponent
+    each for m_rank_z; m_rank_u is uniform) and one mixdim table, as
+    contiguous CUDA tensors, with per-column min / max (zone-map statistics
+    computed once at load)."""
+
+    def __init__(self, rows: int, zipf_s: Sequence[float] = (0.8, 0.95, 1.1, 1.3), nranks: int = 1 << 22,
+                 dim_rows: int = 1_000_000, seed: int = 20240501, device: str = "cuda", host: bool = False):
+        import torch
+        from . import workloads as W
+
+        self.rows, self.zipf_s, self.nranks, self.dim_rows, self.seed = rows, tuple(zipf_s), nranks, dim_rows, seed
+        self.tables: List[Dict[str, "torch.Tensor"]] = []
+        self.host: List[Dict[str, np.ndarray]] = []
+        self.stats: List[Dict[str, Tuple[int, int]]] = []
+        for t, s in enumerate(self.zipf_s):
+            m = W.gen_mix(rows, nranks=nranks, s=s, dim_rows=dim_rows, seed=seed + 7919 * t)
+            self.stats.append({c: (int(a.min()), int(a.max())) if a.size else (0, 0) for c, a in m.items()})
+            self.tables.append({c: torch.from_numpy(a).to(device) for c, a in m.items()})
+            if host:
+                self.host.append(m)
+        md = W.gen_mixdim(dim_rows, seed=seed)
+        self.dim = {c: torch.from_numpy(a).to(device) for c, a in md.items()}
+        self.dim_host = md if host else None
+        self.dim_max_key = int(md["md_key"].max()) if dim_rows else 0
+        if device.startswith("cuda"):
+            torch.cuda.synchronize()
+
+    def ptr(self, table: int, col: str, row0: int = 0) -> int:
+        t = self.tables[table][col]
+        return t.data_ptr() + row0 * t.element_size()
+
+    def slice_host(self, q: MixQuery) -> Dict[str, np.ndarray]:
+        m = self.host[q.table]
+        return {c: a[q.row0:q.row0 + q.rows] for c, a in m.items()}
+
+    def query_struct(self, q: MixQuery, groups: int = 1) -> BatchQueryStruct:
+        st = self.stats[q.table]
+        kmin, kmax = st[q.key]
+        s = BatchQueryStruct(tmpl=TPL[q.tmpl], thr=q.thr, card=max(1, q.card), k=q.k, attr_lt=q.attr_lt,
+                             rows=q.rows, key=self.ptr(q.table, q.key, q.row0),
+                             filter=self.ptr(q.table, "m_filter", q.row0),
+                             value=self.ptr(q.table, "m_value", q.row0),
+                             fk=self.ptr(q.table, "m_fk", q.row0),
+                             dim_key=self.dim["md_key"].data_ptr(), dim_attr=self.dim["md_attr"].data_ptr(),
+                             dim_rows=self.dim_rows, dim_max_key=self.dim_max_key, groups=groups,
+                             key_min=kmin, key_max=kmax, filter_min=st["m_filter"][0],
+                             filter_max=st["m_filter"][1])
+        return s
+
+    def bytes(self) -> int:
+        return sum(t.numel() * t.element_size() for tab in self.tables for t in tab.values()) + \
+            sum(t.numel() * t.element_size() for t in self.dim.values())
+
+
+def query_bytes(q: MixQuery, dim_rows: int) -> int:
+    """Algorithmic bytes of one query: every referenced column read once
+    (the value column of the filtered templates counted in full)."""
+    if q.tmpl == "agg":
+        return 12 * q.rows
+    if q.tmpl == "join":
+        return 16 * q.rows + 8 * dim_rows
+    return 16 * q.rows
+
+
+# ---------------------------------------------------------------------------
+# the C batch object
+# ---------------------------------------------------------------------------
+class Batch:
+    """A set of mixed queries on resident device columns (gpudb_batch)."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        check(self._lib.gpudb_batch_create(None, C.byref(h)))
+        self.handle = h
+        self.n = 0
+        self._pinned, self._pinned_bytes = None, 0
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.gpudb_batch_free(self.handle)
+            self.handle = None
+        self._free_pinned()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_queries(self, structs: Sequence[BatchQueryStruct]) -> None:
+        arr = (BatchQueryStruct * max(1, len(structs)))(*structs)
+        self._structs = arr
+        check(self._lib.gpudb_batch_set_queries(self.handle, arr, len(structs)))
+        self.n = len(structs)
+
+    def set_groups(self, i: int, groups: int) -> None:
+        check(self._lib.gpudb_batch_set_groups(self.handle, i, int(groups)))
+
+    def set_tuning(self, block: int = 512, tile_rows: int = 16384, warp_aggregate: bool = True,
+                   max_probe: int = 128) -> None:
+        check(self._lib.gpudb_batch_set_tuning(self.handle, block, tile_rows, int(warp_aggregate), max_probe))
+
+    def execute(self, use_graph: bool = True) -> Tuple[float, np.ndarray]:
+        ms = C.c_double()
+        err = np.zeros(max(1, self.n), dtype=np.uint32)
+        check(self._lib.gpudb_batch_execute(self.handle, int(use_graph), C.byref(ms), err.ctypes.data))
+        return ms.value, err[:self.n]
+
+    def exact_stats(self) -> Tuple[np.ndarray, np.ndarray, float]:
+        p = np.zeros(max(1, self.n), dtype=np.uint64)
+        d = np.zeros(max(1, self.n), dtype=np.uint64)
+        ms = C.c_double()
+        check(self._lib.gpudb_batch_exact_stats(self.handle, p.ctypes.data, d.ctypes.data, C.byref(ms)))
+        return p[:self.n], d[:self.n], ms.value
+
+    def features(self) -> Tuple[np.ndarray, float]:
+        f = np.zeros((max(1, self.n), SIZER_FEATURES), dtype=np.float32)
+        ms = C.c_double()
+        check(self._lib.gpudb_batch_features(self.handle, f.ctypes.data, C.byref(ms)))
+        return f[:self.n], ms.value
+
+    def collect(self) -> Tuple[np.ndarray, np.ndarray, float]:
+        """(rows per query, packed int64 rows [total, 3], device+copy ms).
+        The packed rows live in a pinned buffer that the next collect reuses."""
+        rows = np.zeros(max(1, self.n), dtype=np.uint64)
+        need = C.c_uint64()
+        ms = C.c_double()
+        check(self._lib.gpudb_batch_collect(self.handle, rows.ctypes.data, None, 0, C.byref(need), None))
+        nbytes = max(24, need.value)
+        if nbytes > self._pinned_bytes:
+            self._free_pinned()
+            cap = int(nbytes * 1.25) + 4096
+            ptr = self._lib.gpudb_host_alloc(cap)
+            if not ptr:
+                raise MemoryError(f"pinned host buffer of {cap} bytes")
+            self._pinned, self._pinned_bytes = ptr, cap
+        check(self._lib.gpudb_batch_collect(self.handle, None, self._pinned, self._pinned_bytes,
+                                            C.byref(need), C.byref(ms)))
+        view = np.ctypeslib.as_array((C.c_int64 * (self._pinned_bytes // 8)).from_address(self._pinned))
+        return rows[:self.n], view[:need.value // 8].reshape(-1, 3), ms.value
+
+    def _free_pinned(self) -> None:
+        if self._pinned:
+            self._lib.gpudb_host_free(self._pinned)
+        self._pinned, self._pinned_bytes = None, 0
+
+    def result_scalar(self, i: int) -> Tuple[int, int]:
+        c, lo, hi = C.c_int64(), C.c_uint64(), C.c_int64()
+        check(self._lib.gpudb_batch_result_scalar(self.handle, i, C.byref(c), C.byref(lo), C.byref(hi)))
+        return c.value, (hi.value << 64) | lo.value
+
+    def result_groups(self, i: int):
+        n = C.c_uint64()
+        check(self._lib.gpudb_batch_result_groups(self.handle, i, 0, C.byref(n), None, None, None))
+        k, c, s = (np.zeros(max(1, n.value), dtype=np.int64) for _ in range(3))
+        check(self._lib.gpudb_batch_result_groups(self.handle, i, n.value, C.byref(n), k.ctypes.data,
+                                                  c.ctypes.data, s.ctypes.data))
+        return k[:n.value], c[:n.value], s[:n.value]
+
+    def result_topk(self, i: int):
+        k = np.zeros(16, dtype=np.int64)
+        v = np.zeros(16, dtype=np.int64)
+        n = C.c_int()
+        check(self._lib.gpudb_batch_result_topk(self.handle, i, k.ctypes.data, v.ctypes.data, C.byref(n)))
+        return tuple((int(k[j]), int(v[j])) for j in range(n.value))
+
+    def last_launches(self) -> int:
+        return int(self._lib.gpudb_batch_last_launches(self.handle))
+
+
+def unpack_results(queries: Sequence[MixQuery], rows: np.ndarray, packed: np.ndarray) -> List[tuple]:
+    """Canonical results from gpudb_batch_collect's packed rows."""
+    out = []
+    off = 0
+    for q, r in zip(queries, rows):
+        r = int(r)
+        blk = packed[off:off + r]
+        off += r
+        if q.tmpl in ("agg", "join"):
+            lo = int(blk[0, 1]) & ((1 << 64) - 1)
+            out.append(("scalar", int(blk[0, 0]), (int(blk[0, 2]) << 64) | lo))
+        elif q.tmpl == "groupby":
+            out.append(canonical_groups(blk[:, 0], blk[:, 1], blk[:, 2]))
+        else:
+            out.append(("topk", tuple((int(a), int(b)) for a, b in blk[:, :2])))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# learned sizer
+# ---------------------------------------------------------------------------
+class Sizer:
+    """16 -> 64 -> 64 -> 64 -> 2 MLP (BF16 weights, FP32 accumulate), trained
+    and evaluated on the GPU by the library's own kernels."""
+
+    def __init__(self, seed: int = 0, device: int = 0):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        check(self._lib.gpudb_sizer_create(device, seed, C.byref(h)))
+        self.handle = h
+        self.nparams = int(self._lib.gpudb_sizer_param_count())
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.gpudb_sizer_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparams, dtype=np.float32)
+        check(self._lib.gpudb_sizer_get_params(self.handle, p.ctypes.data))
+        return p
+
+    @params.setter
+    def params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.shape == (self.nparams,)
+        check(self._lib.gpudb_sizer_set_params(self.handle, p.ctypes.data))
+
+    def grads(self, X: np.ndarray, Y: np.ndarray) -> Tuple[np.ndarray, float]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_float()
+        check(self._lib.gpudb_sizer_grads(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], g.ctypes.data,
+                                          C.byref(loss)))
+        return g, loss.value
+
+    def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 20, batch: int = 256, lr: float = 2e-3,
+              seed: int = 0) -> float:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        loss = C.c_float()
+        check(self._lib.gpudb_sizer_train(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], epochs, batch,
+                                          lr, seed, C.byref(loss)))
+        return loss.value
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], SIZER_OUTPUTS), dtype=np.float32)
+        if X.shape[0]:
+            check(self._lib.gpudb_sizer_predict(self.handle, X.ctypes.data, X.shape[0], Y.ctypes.data))
+        return Y
+
+    def save(self, path) -> None:
+        np.save(path, self.params)
+
+    def load(self, path) -> None:
+        self.params = np.load(path)
+
+
+def labels(queries: Sequence[MixQuery], passing: np.ndarray, distinct: np.ndarray) -> np.ndarray:
+    """Sizer targets: (log2(groups + 1) / 24, selectivity)."""
+    y = np.zeros((len(queries), SIZER_OUTPUTS), dtype=np.float32)
+    for i, q in enumerate(queries):
+        y[i, 0] = math.log2(float(distinct[i]) + 1.0) / CARD_SCALE if q.grouped else 0.0
+        y[i, 1] = float(passing[i]) / q.rows if q.rows else 0.0
+    return y
+
+
+def groups_from_prediction(q: MixQuery, y0: float, margin: float) -> int:
+    """Hash-table sizing from a predicted log2 cardinality, clamped to the
+    exact upper bounds (card values of key % card, and the slice rows)."""
+    g = (2.0 ** (float(y0) * CARD_SCALE) - 1.0) * margin
+    bound = max(1, min(q.card, q.rows))
+    return int(min(bound, max(1, math.ceil(g))))
+
+
+def sample_estimate(features: np.ndarray) -> np.ndarray:
+    """The closed-form sizing estimate the network competes with: the
+    uniform-key estimate of feature 14, as log2(groups + 1) / 24."""
+    return features[:, 14] * (24.0 / CARD_SCALE)
+
+
+class ExecutionLog:
+    """Features and exact outcomes of executed queries: the sizer's training set."""
+
+    def __init__(self):
+        self.X: List[np.ndarray] = []
+        self.Y: List[np.ndarray] = []
+
+    def add(self, X: np.ndarray, Y: np.ndarray) -> None:
+        self.X.append(np.asarray(X, dtype=np.float32))
+        self.Y.append(np.asarray(Y, dtype=np.float32))
+
+    def __len__(self) -> int:
+        return sum(x.shape[0] for x in self.X)
+
+    def arrays(self) -> Tuple[np.ndarray, np.ndarray]:
+        if not self.X:
+            return np.zeros((0, SIZER_FEATURES), np.float32), np.zeros((0, SIZER_OUTPUTS), np.float32)
+        return np.concatenate(self.X), np.concatenate(self.Y)
+
+    def save(self, path) -> None:
+        X, Y = self.arrays()
+        np.savez_compressed(path, X=X, Y=Y)
+
+    @classmethod
+    def load(cls, path) -> "ExecutionLog":
+        z = np.load(path)
+        log = cls()
+        log.add(z["X"], z["Y"])
+        return log
+
+
+def log_executions(tables: MixTables, queries: Sequence[MixQuery], log: ExecutionLog,
+                   batch_size: int = 1024) -> float:
+    """Run the exact statistics pass and the feature sample over `queries`
+    (in batches) and append (features, exact outcome) to `log`. Returns the
+    device milliseconds spent."""
+    ms = 0.0
+    b = Batch()
+    try:
+        for i in range(0, len(queries), batch_size):
+            part = list(queries[i:i + batch_size])
+            b.set_queries([tables.query_struct(q) for q in part])
+            X, t0 = b.features()
+            p, d, t1 = b.exact_stats()
+            log.add(X, labels(part, p, d))
+            ms += t0 + t1
+    finally:
+        b.close()
+    return ms
+
+
+# ---------------------------------------------------------------------------
+# the two execution paths
+# ---------------------------------------------------------------------------
+class PlainRunner:
+    """One query at a time through the engine's generated kernels
+    (gpudb_query_run of the mix_* templates), with the exact count pass
+    (`distinct` template) sizing every hash table: the plain method, and the
+    fallback / judge of the batched path."""
+
+    SPEC = {"agg": "mix_agg", "join": "mix_join", "groupby": "mix_groupby", "topk": "mix_topk"}
+
+    def __init__(self, ctx, tables: MixTables, tune: str = ""):
+        self.ctx, self.tables, self.tune = ctx, tables, tune
+        for c, t in tables.dim.items():
+            ctx.register_column("mixdim", c, t.data_ptr(), t.numel(), t.element_size())
+        self.count_passes = 0
+
+    def _register_slice(self, q: MixQuery) -> None:
+        cols = ["m_filter", "m_value"] + (["m_fk"] if q.tmpl == "join" else []) + ([q.key] if q.grouped else [])
+        for c in cols:
+            t = self.tables.tables[q.table][c]
+            self.ctx.register_column("mix", c, t.data_ptr() + q.row0 * t.element_size(), q.rows, t.element_size())
+
+    def exact_groups(self, q: MixQuery) -> int:
+        self._register_slice(q)
+        res, _ = self.ctx.run(f"template=distinct;key={q.key};thr={q.thr};card={q.card}", self.tune)
+        self.count_passes += 1
+        return int(res.rows[0][0])
+
+    def run(self, q: MixQuery) -> tuple:
+        self._register_slice(q)
+        spec = f"template={self.SPEC[q.tmpl]};thr={q.thr}"
+        if q.tmpl == "join":
+            spec += f";attr_lt={q.attr_lt}"
+        if q.grouped:
+            groups = self.exact_groups(q)
+            self.ctx.register_symbol("mix_groups", max(1, groups))
+            spec += f";key={q.key};card={q.card}"
+            if q.tmpl == "topk":
+                spec += f";k={q.k}"
+        res, _ = self.ctx.run(spec, self.tune)
+        if q.tmpl in ("agg", "join"):
+            c, s = res.rows[0]
+            return ("scalar", int(c), int(s))
+        if q.tmpl == "groupby":
+            return canonical_groups(res.column("key"), res.column("count"), res.column("sum"))
+        return ("topk", tuple((int(k), int(v)) for k, v in res.rows))
+
+
+@dataclass
+class BatchReport:
+    sizing: str
+    queries: int
+    features_ms: float = 0.0
+    predict_ms: float = 0.0
+    stats_ms: float = 0.0
+    execute_ms: float = 0.0
+    collect_ms: float = 0.0
+    overflowed: List[int] = field(default_factory=list)
+    fallback_s: float = 0.0
+    wall_s: float = 0.0
+    table_slots: int = 0
+    launches: int = 0
+
+
+class BatchRunner:
+    """The batched form: all queries of a batch through the persistent
+    work-queue kernels, hash tables sized by `sizing`:
+      "learned" — the sizer's predicted cardinality (no count pass);
+      "exact"   — the batched exact count pass;
+      "bound"   — the exact upper bound min(card, rows) (no pass, largest tables).
+    Queries whose table overflowed re-run through the plain exact path."""
+
+    def __init__(self, tables: MixTables, sizing: str = "learned", sizer: Optional[Sizer] = None,
+                 plain: Optional[PlainRunner] = None, margin: float = 1.5, use_graph: bool = True,
+                 tuning: Optional[dict] = None):
+        if sizing == "learned" and sizer is None:
+            raise ValueError("learned sizing needs a trained Sizer")
+        self.tables, self.sizing, self.sizer, self.plain = tables, sizing, sizer, plain
+        self.margin, self.use_graph = margin, use_graph
+        self.batch = Batch()
+        if tuning:
+            self.batch.set_tuning(**tuning)
+        self._key = None
+        self._groups = None
+
+    def close(self) -> None:
+        self.batch.close()
+
+    def size(self, queries: Sequence[MixQuery], report: BatchReport) -> List[int]:
+        b = self.batch
+        if self.sizing == "learned":
+            X, report.features_ms = b.features()
+            t = time.perf_counter()
+            Y = self.sizer.predict(X)
+            report.predict_ms = 1e3 * (time.perf_counter() - t)
+            return [groups_from_prediction(q, Y[i, 0], self.margin) if q.grouped else 1
+                    for i, q in enumerate(queries)]
+        if self.sizing == "exact":
+            _, d, report.stats_ms = b.exact_stats()
+            return [max(1, int(d[i])) if q.grouped else 1 for i, q in enumerate(queries)]
+        if self.sizing == "bound":
+            return [max(1, min(q.card, q.rows)) if q.grouped else 1 for q in queries]
+        raise ValueError(f"unknown sizing '{self.sizing}'")
+
+    def run(self, queries: Sequence[MixQuery]) -> Tuple[List[tuple], BatchReport]:
+        t0 = time.perf_counter()
+        report = BatchReport(self.sizing, len(queries))
+        key = tuple(queries)
+        b = self.batch
+        if key != self._key:
+            b.set_queries([self.tables.query_struct(q) for q in queries])
+            self._key, self._groups = key, None
+        groups = self.size(queries, report)
+        if groups != self._groups:
+            for i, g in enumerate(groups):
+                b.set_groups(i, g)
+            self._groups = groups
+        report.table_slots = sum(1 << max(4, math.ceil(math.log2(2 * g))) for g, q in zip(groups, queries)
+                                 if q.grouped)
+        report.execute_ms, err = b.execute(self.use_graph)
+        report.launches = b.last_launches()
+        rows, packed, report.collect_ms = b.collect()
+        results = unpack_results(queries, rows, packed)
+        err = [int(e) for e in err]
+        bad = [i for i, e in enumerate(err) if e & DEVERR_HASH_OVERFLOW]
+        other = [i for i, e in enumerate(err) if e & ~DEVERR_HASH_OVERFLOW]
+        if other:
+            raise RuntimeError(f"device errors {[(i, int(err[i])) for i in other[:8]]}")
+        if bad:
+            if self.plain is None:
+                raise RuntimeError(f"{len(bad)} hash tables overflowed and no exact fallback is configured")
+            tf = time.perf_counter()
+            for i in bad:
+                results[i] = self.plain.run(queries[i])
+            report.fallback_s = time.perf_counter() - tf
+        report.overflowed = bad
+        report.wall_s = time.perf_counter() - t0
+        return results, report
+
+
+def train_sizer(log: ExecutionLog, seed: int = 0, epochs: int = 30, batch: int = 512, lr: float = 2e-3,
+                holdout: float = 0.1) -> Tuple[Sizer, dict]:
+    """Train a sizer on an execution log; report held-out errors of the
+    network and of the closed-form sample estimate."""
+    X, Y = log.arrays()
+    rng = np.random.default_rng(seed)
+    idx = rng.permutation(X.shape[0])
+    nh = max(1, int(holdout * X.shape[0]))
+    te, tr = idx[:nh], idx[nh:]
+    s = Sizer(seed=seed)
+    t = time.perf_counter()
+    loss = s.train(X[tr], Y[tr], epochs=epochs, batch=batch, lr=lr, seed=seed)
+    train_s = time.perf_counter() - t
+    P = s.predict(X[te])
+    grouped = X[te, 2] + X[te, 3] > 0
+    err_net = np.abs(P[grouped, 0] - Y[te][grouped, 0]) * CARD_SCALE
+    err_est = np.abs(sample_estimate(X[te][grouped]) - Y[te][grouped, 0]) * CARD_SCALE
+    return s, {"train_loss": loss, "train_s": train_s, "train_rows": int(tr.size), "holdout_rows": int(te.size),
+               "log2_err_net_mean": float(err_net.mean()) if err_net.size else 0.0,
+               "log2_err_net_p99": float(np.quantile(err_net, 0.99)) if err_net.size else 0.0,
+               "log2_err_estimate_mean": float(err_est.mean()) if err_est.size else 0.0,
+               "log2_err_estimate_p99": float(np.quantile(err_est, 0.99)) if err_est.size else 0.0,
+               "sel_err_net_mean": float(np.abs(P[:, 1] - Y[te][:, 1]).mean())}

@@ -44,6 +44,8 @@ HOST_SOURCES = [
 ]
 CUDA_SOURCES: list[str] = [
     "kernels/noalloc_distinct.cu",
+    "kernels/sizer_mlp.cu",
+    "kernels/batch_kernels.cu",
 ]
 
 LIB_NAME = "libgpudb.so"

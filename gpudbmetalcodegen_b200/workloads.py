@@ -99,3 +99,45 @@ def gen_mixdim(n: int = 1_000_000, seed: int = SEED, threads: int = 0) -> Dict[s
 
 def table_bytes(t: Dict[str, np.ndarray]) -> int:
     return sum(a.nbytes for a in t.values())
+
+
+# ---------------------------------------------------------------------------
+# mixed-query workload: 256 queries over slices of resident mix tables
+# ---------------------------------------------------------------------------
+MIX_TABLE_ROWS = 120_000_000
+MIX_ZIPF_S = (0.8, 0.95, 1.1, 1.3)   # one resident mix table per exponent
+MIX_NRANKS = 1 << 22
+MIX_DIM_ROWS = 1_000_000
+MIX_QUERIES = 256
+
+
+def gen_mixed_queries(n: int = MIX_QUERIES, seed: int = SEED, table_rows: int = MIX_TABLE_ROWS,
+                      n_tables: int = len(MIX_ZIPF_S), min_rows: int = 1_000_000, max_rows: int = 120_000_000,
+                      min_card: int = 4, max_card: int = 1 << 22, k: int = 10, templates=None):
+    """Seeded mixed queries: template uniform over agg / join / groupby / topk
+    (or over `templates`); slice rows log-uniform in [min_rows, max_rows]
+    (capped by the table) at a uniform offset of a uniformly chosen table;
+    group key uniform (m_rank_u) or Zipf (m_rank_z, the table's exponent)
+    with equal odds; cardinality log-uniform in [min_card, max_card]; filter
+    selectivity uniform in 1%..99% (m_filter is uniform on 0..9999, so the
+    threshold is 100 x the percentage); join keeps md_attr < U[1, 999]."""
+    from .batch import MixQuery, TEMPLATES
+
+    templates = tuple(templates or TEMPLATES)
+    rng = np.random.default_rng(seed)
+    hi = min(max_rows, table_rows)
+    lo = min(min_rows, hi)
+    out = []
+    for _ in range(n):
+        tmpl = templates[int(rng.integers(len(templates)))]
+        rows = int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+        rows = max(1, min(rows, table_rows))
+        row0 = int(rng.integers(0, table_rows - rows + 1))
+        table = int(rng.integers(n_tables))
+        key = "m_rank_z" if rng.random() < 0.5 else "m_rank_u"
+        card = int(round(float(np.exp(rng.uniform(np.log(min_card), np.log(max_card))))))
+        thr = int(round(rng.uniform(0.01, 0.99) * 10000))
+        attr_lt = int(rng.integers(1, 1000))
+        out.append(MixQuery(tmpl=tmpl, table=table, row0=row0, rows=rows, thr=thr, key=key, card=card, k=k,
+                            attr_lt=attr_lt))
+    return out

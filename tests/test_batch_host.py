@@ -1,0 +1,123 @@
+"""Host-side logic of the batched / learned-sizing layer (no GPU): the C
+struct layout seen from Python, the mixed-query generator, result packing,
+the sizing policy, the execution log, and the MLP oracle itself (its
+gradients against central finite differences)."""
+import ctypes as C
+import subprocess
+import textwrap
+
+import numpy as np
+import pytest
+
+from gpudbmetalcodegen_b200 import batch as B
+from gpudbmetalcodegen_b200 import workloads as W
+from oracle import mlp_oracle as M
+
+from conftest import ROOT
+
+
+def test_query_struct_layout_matches_header(tmp_path):
+    fields = [f for f, _ in B.BatchQueryStruct._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text(textwrap.dedent("""
+        #include <stddef.h>
+        #include <stdio.h>
+        #include "gpudb_batch.h"
+        int main(void) {
+            printf("%zu\\n", sizeof(gpudb_batch_query));
+        """) + "".join(f'    printf("%zu\\n", offsetof(gpudb_batch_query, {f}));\n' for f in fields) + "}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == C.sizeof(B.BatchQueryStruct)
+    assert out[1:] == [getattr(B.BatchQueryStruct, f).offset for f in fields]
+
+
+def test_mixed_query_generator():
+    qs = W.gen_mixed_queries(256, seed=5)
+    assert qs == W.gen_mixed_queries(256, seed=5)
+    assert qs != W.gen_mixed_queries(256, seed=6)
+    assert {q.tmpl for q in qs} == set(B.TEMPLATES)
+    rows = np.array([q.rows for q in qs])
+    assert rows.min() >= 1_000_000 and rows.max() <= 120_000_000
+    # log-uniform over [1M, 120M]: median near sqrt(1M * 120M) ~ 11M
+    assert 5e6 < np.median(rows) < 25e6
+    for q in qs:
+        assert 0 <= q.row0 and q.row0 + q.rows <= W.MIX_TABLE_ROWS
+        assert 100 <= q.thr <= 9900
+        assert 4 <= q.card <= 1 << 22
+        assert q.key in ("m_rank_u", "m_rank_z")
+        assert 0 <= q.table < len(W.MIX_ZIPF_S)
+    small = W.gen_mixed_queries(50, seed=1, table_rows=10_000, min_rows=100, max_rows=5_000)
+    assert all(100 <= q.rows <= 5_000 and q.row0 + q.rows <= 10_000 for q in small)
+
+
+def test_unpack_results():
+    qs = [B.MixQuery("agg", 0, 0, 10, 5), B.MixQuery("groupby", 0, 0, 10, 5, card=9),
+          B.MixQuery("topk", 0, 0, 10, 5, card=9, k=2), B.MixQuery("join", 0, 0, 10, 5)]
+    big = (1 << 70) + 12345  # a sum beyond int64: lo / hi words
+    packed = np.array([[7, big & ((1 << 64) - 1), big >> 64],
+                       [5, 1, 10], [2, 3, 30],
+                       [2, 30, 0], [5, 10, 0],
+                       [0, 0, 0]], dtype=np.uint64).astype(np.int64)
+    res = B.unpack_results(qs, np.array([1, 2, 2, 1], dtype=np.uint64), packed)
+    assert res[0] == ("scalar", 7, big)
+    assert res[1][0] == "groups" and list(res[1][1]) == [2, 5] and list(res[1][3]) == [30, 10]
+    assert res[2] == ("topk", ((2, 30), (5, 10)))
+    assert res[3] == ("scalar", 0, 0)
+    assert B.same_result(res[1], B.canonical_groups([5, 2], [1, 3], [10, 30]))
+    assert not B.same_result(res[1], B.canonical_groups([5, 2], [1, 3], [10, 31]))
+
+
+def test_sizing_policy():
+    q = B.MixQuery("groupby", 0, 0, rows=1000, thr=5000, card=100_000)
+    y = lambda g: np.log2(g + 1) / B.CARD_SCALE
+    assert B.groups_from_prediction(q, y(300), 1.5) == pytest.approx(450, abs=2)
+    assert B.groups_from_prediction(q, y(1e6), 1.5) == 1000          # clamped to the slice rows
+    q2 = B.MixQuery("groupby", 0, 0, rows=10**8, thr=5000, card=64)
+    assert B.groups_from_prediction(q2, y(1e6), 1.5) == 64           # clamped to card
+    assert B.groups_from_prediction(q2, -1.0, 1.5) == 1
+
+
+def test_labels_and_log(tmp_path):
+    qs = [B.MixQuery("groupby", 0, 0, 1000, 5000, card=64), B.MixQuery("agg", 0, 0, 1000, 5000)]
+    y = B.labels(qs, np.array([500, 250]), np.array([63, 0]))
+    assert y[0, 0] == pytest.approx(6 / B.CARD_SCALE) and y[0, 1] == pytest.approx(0.5)
+    assert y[1, 0] == 0 and y[1, 1] == pytest.approx(0.25)
+    log = B.ExecutionLog()
+    log.add(np.ones((2, 16)), y)
+    log.add(np.zeros((3, 16)), np.zeros((3, 2)))
+    assert len(log) == 5
+    log.save(tmp_path / "log.npz")
+    X, Y = B.ExecutionLog.load(tmp_path / "log.npz").arrays()
+    assert X.shape == (5, 16) and np.array_equal(Y[:2], y)
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1 + 2 ** -8, 1 + 3 * 2 ** -8, -2.5, 1 + 2 ** -7, 3.0e38], dtype=np.float32)
+    r = M.bf16_round(x)
+    assert list(r[:5]) == [1.0, 1.0, 1 + 2 ** -6, -2.5, 1 + 2 ** -7]  # ties to even
+    assert np.isfinite(r[5])
+
+
+def test_mlp_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(3)
+    p = rng.normal(0, 0.3, M.NPARAMS)
+    X = rng.uniform(-1, 1, (7, 16))
+    Y = rng.uniform(-1, 1, (7, 2))
+    _, g = M.loss_and_grads(p, X, Y, quantize=False)
+    idx = rng.choice(M.NPARAMS, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        e = np.zeros(M.NPARAMS)
+        e[i] = h
+        lp, _ = M.loss_and_grads(p + e, X, Y, quantize=False)
+        lm, _ = M.loss_and_grads(p - e, X, Y, quantize=False)
+        assert abs((lp - lm) / (2 * h) - g[i]) <= 1e-5 * max(1.0, abs(g[i])), i
+
+
+def test_adam_oracle_first_step_is_signed_lr():
+    w = np.zeros(5)
+    g = np.array([1.0, -2.0, 0.5, -1e-3, 3.0])
+    w1, m, v = M.adam_step(w, np.zeros(5), np.zeros(5), g, 1, lr=0.01)
+    assert np.allclose(w1, -0.01 * np.sign(g), atol=1e-7)
