@@ -318,6 +318,202 @@ def run_reference(args, w: Workload):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# mixed-query batches with the learned sizer
+# ---------------------------------------------------------------------------
+def mixed_oracle_seconds(args, queries, budget_s: float):
+    """The oracle (the reference's operator semantics restated on the CPU,
+    all host cores) over the first queries of the batch until `budget_s`
+    has passed; slices are regenerated on the host from the same seeds."""
+    from gpudbmetalcodegen_b200 import workloads as W
+    from oracle import oracle_py as O
+    threads = os.cpu_count() or 1
+    md = W.gen_mixdim(args.mix_dim_rows, seed=W.SEED)
+    done, spent = 0, 0.0
+    for q in queries:
+        m = W.gen_mix(q.rows, nranks=W.MIX_NRANKS, s=W.MIX_ZIPF_S[q.table], dim_rows=args.mix_dim_rows,
+                      seed=W.SEED + 7919 * q.table, row0=q.row0)
+        t0 = time.perf_counter()
+        if q.tmpl == "agg":
+            O.mix_agg(m, q.thr, threads=threads)
+        elif q.tmpl == "join":
+            O.mix_join(md, m, q.attr_lt, q.thr, threads=threads)
+        else:
+            k, c, sm = O.mix_groupby(m, q.key, q.thr, q.card, threads=threads)
+            if q.tmpl == "topk":
+                O.topk(k, sm, q.k)
+        spent += time.perf_counter() - t0
+        done += 1
+        if spent >= budget_s:
+            break
+    return done, spent, threads
+
+
+def run_mixed(args):
+    """Config: 256 seeded mixed queries over slices (1M-120M rows) of four
+    resident 120M-row mix tables. One step = the whole batch through the
+    batched, learned-sizing path (4096-row sample features, MLP prediction,
+    persistent work-queue kernels in a CUDA graph, one packed result copy,
+    exact re-run of any overflowed table). Beside it: the plain
+    one-query-at-a-time path (exact count pass + generated kernels per
+    query) and the batched path with the exact count pass."""
+    import torch
+    from gpudbmetalcodegen_b200 import Context, batch as B, workloads as W
+
+    world, rank, local = dist_info()
+    if args.impl == "reference":
+        if rank == 0:
+            qs = W.gen_mixed_queries(args.mix_queries, seed=W.SEED, table_rows=args.mix_rows)
+            done, spent, threads = mixed_oracle_seconds(args, qs, budget_s=max(10.0, 2.0 * args.steps))
+            v = done / spent
+            print(json.dumps({
+                "metric": "mixed_queries_per_s", "value": v, "unit": "queries/s", "n_gpus": args.gpus,
+                "steps": 1, "warmup": 0, "ms_per_step": 1e3 * spent / done * args.mix_queries,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": f"mixed: {args.mix_queries} queries over slices of 120M-row tables"},
+                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": f"first {done} of the {args.mix_queries} queries"},
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+                flush=True)
+        return
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    t0 = time.perf_counter()
+    tables = B.MixTables(rows=args.mix_rows, zipf_s=W.MIX_ZIPF_S, nranks=W.MIX_NRANKS,
+                         dim_rows=args.mix_dim_rows, seed=W.SEED)
+    gen_s = time.perf_counter() - t0
+    queries = W.gen_mixed_queries(args.mix_queries, seed=W.SEED, table_rows=args.mix_rows)
+    total_rows = sum(q.rows for q in queries)
+    alg_bytes = sum(B.query_bytes(q, args.mix_dim_rows) for q in queries)
+
+    # the sizer: trained on engine-logged executions of other queries
+    t0 = time.perf_counter()
+    log = B.ExecutionLog()
+    train_q = W.gen_mixed_queries(args.train_executions, seed=W.SEED + 1, table_rows=args.mix_rows)
+    log_ms = B.log_executions(tables, train_q, log, batch_size=1024)
+    log_s = time.perf_counter() - t0
+    sizer, sinfo = B.train_sizer(log, seed=1, epochs=args.sizer_epochs, batch=512, lr=3e-3)
+    sinfo.update({"executions": len(log), "log_device_ms": log_ms, "log_s": log_s})
+
+    ctx = Context(local)
+    plain = B.PlainRunner(ctx, tables)
+    # plain one-query-at-a-time path (first pass compiles / warms)
+    plain_res = [plain.run(q) for q in queries]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.plain_passes):
+        plain_res = [plain.run(q) for q in queries]
+    torch.cuda.synchronize()
+    plain_s = (time.perf_counter() - t0) / args.plain_passes
+
+    exact = B.BatchRunner(tables, sizing="exact", plain=plain)
+    for _ in range(2):
+        exact.run(queries)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        exact_res, exact_rep = exact.run(queries)
+    exact_s = (time.perf_counter() - t0) / 3
+    exact.close()
+
+    learned = B.BatchRunner(tables, sizing="learned", sizer=sizer, plain=plain)
+    for _ in range(args.warmup):
+        res, rep = learned.run(queries)
+    stream = torch.cuda.current_stream()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps = []
+    launches = 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        w0 = time.perf_counter()
+        for i in range(args.steps):
+            res, rep = learned.run(queries, copy=(i == args.steps - 1))
+            reps.append(rep)
+            launches += rep.launches + 2  # + the sample kernel and the predictor
+        ev1.record(stream)
+        ev1.synchronize()
+        wall_ms = (time.perf_counter() - w0) * 1e3 / args.steps
+    step_ms = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        tt = torch.tensor([step_ms, wall_ms], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        step_ms, wall_ms = float(tt[0].item()), float(tt[1].item())
+        pg.barrier()
+    verified = all(B.same_result(a, b) for a, b in zip(res, plain_res)) and \
+        all(B.same_result(a, b) for a, b in zip(exact_res, plain_res))
+
+    # per-kernel device times (one execute without a graph) for the roofline
+    learned.batch.execute(use_graph=False)
+    stages = learned.batch.stage_ms()
+    grouped_bytes = sum(B.query_bytes(q, 0) for q in queries if q.grouped)
+    scalar_bytes = sum(B.query_bytes(q, 0) for q in queries if not q.grouped)
+    peak, peak_kind = peaks()
+    dom = max(("group", "agg_probe"), key=lambda k: stages[k])
+    dom_bytes = grouped_bytes if dom == "group" else scalar_bytes
+    achieved = dom_bytes / (stages[dom] / 1e3) / 1e9 if stages[dom] else None
+    roofline = {"bound": "hbm", "kernel": "kGroup" if dom == "group" else "kAgg", "achieved": achieved,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "kernel_ms": stages[dom], "algorithmic_bytes": dom_bytes, "stage_ms": stages,
+                "batch_hbm_frac": alg_bytes / (sum(stages.values()) / 1e3) / 1e9 / peak,
+                "traffic": load_traffic("kGroup" if dom == "group" else "kAgg")}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        done, spent, threads = mixed_oracle_seconds(args, queries, budget_s=15.0)
+        cpu = {"value": done / spent, "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"first {done} of the {len(queries)} queries, slices regenerated on the host"}
+
+    n_q = len(queries) * world
+    value = n_q / (step_ms / 1e3)
+    if rank == 0:
+        desc_bytes = len(queries) * 128
+        line = {"metric": "mixed_queries_per_s", "value": value, "unit": "queries/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+                "config": {"workload": f"mixed: {len(queries)} queries (agg / join / groupby / topk) over slices "
+                                       f"of {len(W.MIX_ZIPF_S)} resident {args.mix_rows}-row tables, learned sizing",
+                           "queries": len(queries), "rows_scanned_per_step": total_rows,
+                           "algorithmic_bytes_per_step": alg_bytes, "table_gen_s": gen_s,
+                           "l2": "inputs larger than the 126 MB L2; no flush",
+                           "parallelism": f"replicas x{world}"},
+                "verified": verified,
+                "plain_per_query": {"queries_per_s": len(queries) / plain_s, "ms_per_batch": plain_s * 1e3,
+                                    "count_passes": plain.count_passes},
+                "batched_exact": {"queries_per_s": len(queries) / exact_s, "ms_per_batch": exact_s * 1e3,
+                                  "stats_ms": exact_rep.stats_ms},
+                "batched_learned": {"queries_per_s": len(queries) / (wall_ms / 1e3), "ms_per_batch": wall_ms,
+                                    "execute_ms": statistics.median(r.execute_ms for r in reps),
+                                    "features_ms": statistics.median(r.features_ms for r in reps),
+                                    "collect_ms": statistics.median(r.collect_ms for r in reps),
+                                    "overflowed": len(reps[-1].overflowed),
+                                    "table_slots": reps[-1].table_slots},
+                "speedup_vs_plain": (len(queries) / (wall_ms / 1e3)) / (len(queries) / plain_s),
+                "rows_per_s": total_rows * world / (step_ms / 1e3),
+                "sizer": sinfo, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": n_q / (wall_ms / 1e3), "unit": "queries/s", "h2d_bytes_per_step": desc_bytes,
+                        "d2h_bytes_per_step": reps[-1].result_bytes,
+                        "note": "wall clock through BatchRunner.run; tables resident in HBM by the workload's "
+                                "definition, per-step inputs are the query descriptors"},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    learned.close()
+    sizer.close()
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+
+
 def load_traffic(kernel: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -334,7 +530,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="join_topk", choices=["join_topk", "q1", "q6", "groupby", "hashjoin"])
+    ap.add_argument("--workload", default="join_topk",
+                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed"])
     ap.add_argument("--tune", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -344,8 +541,16 @@ def main():
     ap.add_argument("--fact-rows", type=int, default=6_001_215)
     ap.add_argument("--zprobe-rows", type=int, default=120_000_000)
     ap.add_argument("--zkeys", type=int, default=1 << 22)
+    ap.add_argument("--mix-rows", type=int, default=120_000_000)
+    ap.add_argument("--mix-dim-rows", type=int, default=1_000_000)
+    ap.add_argument("--mix-queries", type=int, default=256)
+    ap.add_argument("--train-executions", type=int, default=200_000)
+    ap.add_argument("--sizer-epochs", type=int, default=30)
+    ap.add_argument("--plain-passes", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload == "mixed":
+        return run_mixed(args)
     world, rank, local = dist_info()
     w = make_workload(args)
 

@@ -115,6 +115,9 @@ _SIGNATURES = [
     ("gpudb_gen_mix", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
      + [C.c_void_p] * 5 + [C.c_int]),
     ("gpudb_gen_mixdim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_mix_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
+     + [C.c_void_p] * 6),
+    ("gpudb_gen_mixdim_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     # gpudb_batch.h
     ("gpudb_sizer_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     ("gpudb_sizer_free", None, [C.c_void_p]),
@@ -142,6 +145,7 @@ _SIGNATURES = [
     ("gpudb_batch_collect", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_double)]),
     ("gpudb_batch_last_launches", C.c_longlong, [C.c_void_p]),
+    ("gpudb_batch_stage_ms", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
 
 EXPORTED = [s[0] for s in _SIGNATURES]

@@ -11,6 +11,10 @@ overflows. Every path returns the same canonical results:
     agg / join : ("scalar", count, sum)
     groupby    : ("groups", keys, counts, sums)  numpy int64, sorted by key
     topk       : ("topk", ((key, sum), ...))     best first
+
+The batched path hands group-by results over unsorted, as
+("groups_raw", rows[n, 3]) in table order (a GROUP BY has no row order);
+`canonical` sorts them when a comparison needs it.
 """
 from __future__ import annotations
 
@@ -71,7 +75,15 @@ def canonical_groups(keys, counts, sums):
             np.asarray(sums, dtype=np.int64)[order])
 
 
+def canonical(r):
+    if r[0] == "groups_raw":
+        blk = r[1]
+        return canonical_groups(blk[:, 0], blk[:, 1], blk[:, 2])
+    return r
+
+
 def same_result(a, b) -> bool:
+    a, b = canonical(a), canonical(b)
     if a[0] != b[0]:
         return False
     if a[0] == "groups":
@@ -80,6 +92,7 @@ def same_result(a, b) -> bool:
 
 
 def describe_difference(a, b) -> str:
+    a, b = canonical(a), canonical(b)
     if a[0] != b[0]:
         return f"kind {a[0]} vs {b[0]}"
     if a[0] == "groups":
@@ -104,25 +117,39 @@ class MixTables:
 
     def __init__(self, rows: int, zipf_s: Sequence[float] = (0.8, 0.95, 1.1, 1.3), nranks: int = 1 << 22,
                  dim_rows: int = 1_000_000, seed: int = 20240501, device: str = "cuda", host: bool = False):
+        """Generates the tables in HBM with the device generators (values
+        identical to the host generators of the same seeds); `host` also
+        keeps numpy copies (for the CPU oracle)."""
         import torch
         from . import workloads as W
 
         self.rows, self.zipf_s, self.nranks, self.dim_rows, self.seed = rows, tuple(zipf_s), nranks, dim_rows, seed
+        lib = _lib.load()
+        stream = torch.cuda.current_stream().cuda_stream
+        tdt = {np.int32: torch.int32, np.int64: torch.int64}
         self.tables: List[Dict[str, "torch.Tensor"]] = []
         self.host: List[Dict[str, np.ndarray]] = []
         self.stats: List[Dict[str, Tuple[int, int]]] = []
         for t, s in enumerate(self.zipf_s):
-            m = W.gen_mix(rows, nranks=nranks, s=s, dim_rows=dim_rows, seed=seed + 7919 * t)
-            self.stats.append({c: (int(a.min()), int(a.max())) if a.size else (0, 0) for c, a in m.items()})
-            self.tables.append({c: torch.from_numpy(a).to(device) for c, a in m.items()})
+            cols = {c: torch.empty(rows, dtype=tdt[dt], device=device) for c, dt in W.MIX_COLUMNS.items()}
+            st = lib.gpudb_gen_mix_device(self.table_seed(t), nranks, s, dim_rows, 0, rows,
+                                          *(cols[c].data_ptr() for c in W.MIX_COLUMNS), stream)
+            if st != 0:
+                raise RuntimeError(f"device generator failed: {_lib.last_error(None)}")
+            self.stats.append({c: (int(v.min()), int(v.max())) if rows else (0, 0) for c, v in cols.items()})
+            self.tables.append(cols)
             if host:
-                self.host.append(m)
-        md = W.gen_mixdim(dim_rows, seed=seed)
-        self.dim = {c: torch.from_numpy(a).to(device) for c, a in md.items()}
-        self.dim_host = md if host else None
-        self.dim_max_key = int(md["md_key"].max()) if dim_rows else 0
-        if device.startswith("cuda"):
-            torch.cuda.synchronize()
+                self.host.append({c: v.cpu().numpy() for c, v in cols.items()})
+        self.dim = {c: torch.empty(dim_rows, dtype=tdt[dt], device=device) for c, dt in W.MIXDIM_COLUMNS.items()}
+        if lib.gpudb_gen_mixdim_device(seed, 0, dim_rows, self.dim["md_key"].data_ptr(),
+                                       self.dim["md_attr"].data_ptr(), stream) != 0:
+            raise RuntimeError(f"device generator failed: {_lib.last_error(None)}")
+        self.dim_host = {c: v.cpu().numpy() for c, v in self.dim.items()} if host else None
+        self.dim_max_key = dim_rows  # keys are 1..dim_rows
+        torch.cuda.synchronize()
+
+    def table_seed(self, t: int) -> int:
+        return self.seed + 7919 * t
 
     def ptr(self, table: int, col: str, row0: int = 0) -> int:
         t = self.tables[table][col]
@@ -267,9 +294,21 @@ class Batch:
     def last_launches(self) -> int:
         return int(self._lib.gpudb_batch_last_launches(self.handle))
 
+    STAGES = ("fill", "join_build", "agg_probe", "group", "topk_chunks", "topk_merge")
 
-def unpack_results(queries: Sequence[MixQuery], rows: np.ndarray, packed: np.ndarray) -> List[tuple]:
-    """Canonical results from gpudb_batch_collect's packed rows."""
+    def stage_ms(self) -> Dict[str, float]:
+        """Per-step device ms of the last execute(use_graph=False)."""
+        ms = np.zeros(len(self.STAGES), dtype=np.float64)
+        check(self._lib.gpudb_batch_stage_ms(self.handle, ms.ctypes.data))
+        return dict(zip(self.STAGES, ms.tolist()))
+
+
+def unpack_results(queries: Sequence[MixQuery], rows: np.ndarray, packed: np.ndarray,
+                   copy: bool = True) -> List[tuple]:
+    """Results from gpudb_batch_collect's packed rows (group-by rows as
+    "groups_raw" blocks; views into `packed` unless `copy`)."""
+    if copy:
+        packed = packed.copy()
     out = []
     off = 0
     for q, r in zip(queries, rows):
@@ -280,7 +319,7 @@ def unpack_results(queries: Sequence[MixQuery], rows: np.ndarray, packed: np.nda
             lo = int(blk[0, 1]) & ((1 << 64) - 1)
             out.append(("scalar", int(blk[0, 0]), (int(blk[0, 2]) << 64) | lo))
         elif q.tmpl == "groupby":
-            out.append(canonical_groups(blk[:, 0], blk[:, 1], blk[:, 2]))
+            out.append(("groups_raw", blk))
         else:
             out.append(("topk", tuple((int(a), int(b)) for a, b in blk[:, :2])))
     return out
@@ -492,6 +531,7 @@ class BatchReport:
     wall_s: float = 0.0
     table_slots: int = 0
     launches: int = 0
+    result_bytes: int = 0
 
 
 class BatchRunner:
@@ -534,7 +574,10 @@ class BatchRunner:
             return [max(1, min(q.card, q.rows)) if q.grouped else 1 for q in queries]
         raise ValueError(f"unknown sizing '{self.sizing}'")
 
-    def run(self, queries: Sequence[MixQuery]) -> Tuple[List[tuple], BatchReport]:
+    def run(self, queries: Sequence[MixQuery], copy: bool = True) -> Tuple[List[tuple], BatchReport]:
+        """Results of group-by queries are "groups_raw" blocks; with
+        copy=False they are views of a pinned buffer that the next run on
+        this runner overwrites."""
         t0 = time.perf_counter()
         report = BatchReport(self.sizing, len(queries))
         key = tuple(queries)
@@ -552,7 +595,8 @@ class BatchRunner:
         report.execute_ms, err = b.execute(self.use_graph)
         report.launches = b.last_launches()
         rows, packed, report.collect_ms = b.collect()
-        results = unpack_results(queries, rows, packed)
+        report.result_bytes = int(packed.nbytes)
+        results = unpack_results(queries, rows, packed, copy=copy)
         err = [int(e) for e in err]
         bad = [i for i, e in enumerate(err) if e & DEVERR_HASH_OVERFLOW]
         other = [i for i, e in enumerate(err) if e & ~DEVERR_HASH_OVERFLOW]

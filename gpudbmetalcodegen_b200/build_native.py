@@ -46,6 +46,7 @@ CUDA_SOURCES: list[str] = [
     "kernels/noalloc_distinct.cu",
     "kernels/sizer_mlp.cu",
     "kernels/batch_kernels.cu",
+    "kernels/datagen_device.cu",
 ]
 
 LIB_NAME = "libgpudb.so"

@@ -8,24 +8,11 @@
 #include <vector>
 
 #include "../../../include/gpudb_datagen.h"
+#include "datagen_core.h"
 
 namespace {
 
-// splitmix64 finalizer: a bijection on 64-bit words.
-inline uint64_t mix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
-// Independent stream per (seed, column id); value per row.
-inline uint64_t rnd(uint64_t seed, uint64_t stream, uint64_t row) {
-    return mix64(mix64(seed * 0x9E3779B97F4A7C15ull + stream * 0xD1B54A32D192ED03ull) + row);
-}
-
-inline int64_t uni(uint64_t r, int64_t lo, int64_t hi) { return lo + (int64_t)(r % (uint64_t)(hi - lo + 1)); }
-
-inline double unit(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+using namespace gpudb_gen;
 
 template <typename F>
 void parallelFor(uint64_t n, int threads, F&& f) {
@@ -41,14 +28,6 @@ void parallelFor(uint64_t n, int threads, F&& f) {
     }
     for (auto& th : ts) th.join();
 }
-
-// Stream ids (one per generated column).
-enum : uint64_t {
-    S_SHIP = 1, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG_A, S_RECV,
-    S_PERM, S_ODAY, S_SEG, S_FK, S_SHIPD, S_PPRICE, S_PDISC,
-    S_ZKEY, S_ZPAY, S_ZRANK, S_ZVAL,
-    S_MRU, S_MRZ, S_MF, S_MV, S_MFK, S_MDA
-};
 
 // Seeded bijection on [0, n): 4-round Feistel on the smallest even-width
 // bit domain >= n, cycle-walking values that fall outside [0, n).
@@ -108,15 +87,7 @@ std::shared_ptr<ZipfTable> zipf(uint64_t n, double s) {
     return t;
 }
 
-inline uint64_t zipfRank(const ZipfTable& t, double u) {
-    uint64_t lo = 0, hi = t.cdf.size() - 1;
-    while (lo < hi) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (t.cdf[mid] > u) hi = mid;
-        else lo = mid + 1;
-    }
-    return lo;
-}
+inline uint64_t zipfRank(const ZipfTable& t, double u) { return gpudb_gen::zipfRank(t.cdf.data(), t.cdf.size(), u); }
 
 inline int64_t zkey(uint64_t seed, uint64_t rank) {
     uint64_t k = mix64(rank ^ mix64(seed + 0x5851F42D4C957F2Dull));
@@ -125,6 +96,12 @@ inline int64_t zkey(uint64_t seed, uint64_t rank) {
 }
 
 }  // namespace
+
+namespace gpudb {
+// Zipf(s) CDF over [0, n) (cached for the process), shared with the device
+// generators so both search the same table.
+const std::vector<double>& zipfCdf(uint64_t n, double s) { return zipf(n, s)->cdf; }
+}  // namespace gpudb
 
 extern "C" {
 
@@ -219,12 +196,12 @@ int gpudb_gen_mix(uint64_t seed, uint64_t nranks, double s, uint64_t dim_rows, u
     auto t = zipf(nranks, s);
     parallelFor(n, threads, [&](uint64_t b, uint64_t e) {
         for (uint64_t i = b; i < e; i++) {
-            const uint64_t r = row0 + i;
-            rank_u[i] = (int32_t)uni(rnd(seed, S_MRU, r), 0, (int64_t)nranks - 1);
-            rank_z[i] = (int32_t)zipfRank(*t, unit(rnd(seed, S_MRZ, r)));
-            filter[i] = (int32_t)uni(rnd(seed, S_MF, r), 0, 9999);
-            value[i] = uni(rnd(seed, S_MV, r), 1, 1000000);
-            fk[i] = (int32_t)uni(rnd(seed, S_MFK, r), 1, (int64_t)dim_rows);
+            const MixRow m = mixRow(seed, nranks, dim_rows, t->cdf.data(), row0 + i);
+            rank_u[i] = m.rank_u;
+            rank_z[i] = m.rank_z;
+            filter[i] = m.filter;
+            value[i] = m.value;
+            fk[i] = m.fk;
         }
     });
     return 0;
@@ -236,7 +213,7 @@ int gpudb_gen_mixdim(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int
         for (uint64_t i = b; i < e; i++) {
             const uint64_t r = row0 + i;
             key[i] = (int32_t)(r + 1);
-            attr[i] = (int32_t)uni(rnd(seed, S_MDA, r), 0, 999);
+            attr[i] = mixdimAttr(seed, r);
         }
     });
     return 0;

@@ -8,10 +8,14 @@
 // a handful of launches (build, agg, group, top-k, top-k merge), replayable
 // as a CUDA graph.
 //
-// Hash tables are arrays of 32-byte slots {key ^ 2^63, count, sum, -}: one L2
-// sector per probe, and the all-zero pattern is the empty slot (the encoded
-// key 0 would be INT64_MIN, which `int32 % card` never produces), so a single
-// memset initialises the whole arena.
+// Hash tables are arrays of 16-byte slots {key + card (u32), count (u32),
+// sum (u64)}: two slots per L2 sector, and the all-zero pattern is the empty
+// slot (`int32 % card` lies in (-card, card), so key + card is never 0), so a
+// single memset initialises the whole arena. Each CTA first aggregates into
+// a shared-memory table of kSmemSlots entries (bounded probing; a row whose
+// key finds no room goes to the global table directly) and flushes it at
+// the end of every work item: few-group queries then cost a handful of
+// global atomics per tile, and hot keys of skewed ones stay on chip.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,15 +38,25 @@ namespace {
 constexpr int kTopK = 16;             // largest k a top-k query may ask for
 constexpr long long kTkChunk = 4096;  // slot-list entries per top-k work item
 constexpr int kUnroll = 4;            // independent rows in flight per thread
-constexpr unsigned long long kKeyBias = 0x8000000000000000ull;
+constexpr int kSmemSlots = 2048;      // per-CTA shared-memory aggregation table
+constexpr int kSmemProbe = 4;         // probes into it before spilling to global
 
-struct __align__(32) Slot {
-    unsigned long long key, count, sum, pad;
+struct __align__(16) Slot {
+    unsigned key;    // key + card, 0 = empty
+    unsigned count;  // rows of the group (slices are < 2^32 rows)
+    unsigned long long sum;
 };
+
+__host__ __device__ __forceinline__ unsigned encKey(long long key, long long card) {
+    return (unsigned)(key + card);
+}
+__host__ __device__ __forceinline__ long long decKey(unsigned enc, long long card) { return (long long)enc - card; }
 
 struct QDesc {
     int tmpl, thr, k, attr_lt;
     long long card, rows;
+    unsigned cardMagic;  // key % card by multiply-high for keys >= 0
+    int cardSh1, cardSh2;
     const int* key;
     const int* filter;
     const long long* value;
@@ -67,6 +81,30 @@ struct QDesc {
     unsigned* st_bitmap;
     long long st_words;
 };
+
+// Group key = key % card. Non-negative keys use division by the invariant
+// card via a multiply-high (Granlund & Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, Fig. 4.1): with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), t = mulhi(m, n).
+void cardDivisor(long long card, unsigned* magic, int* sh1, int* sh2) {
+    const unsigned long long d = (unsigned long long)card;
+    int l = 0;
+    while ((1ull << l) < d) l++;
+    *magic = (unsigned)(((1ull << 32) * ((1ull << l) - d)) / d + 1ull);
+    *sh1 = l < 1 ? l : 1;
+    *sh2 = l - 1 > 0 ? l - 1 : 0;
+}
+
+__device__ __forceinline__ long long keyMod(int k, const QDesc& q) {
+    if (k >= 0) {
+        const unsigned n = (unsigned)k;
+        const unsigned t = __umulhi(n, q.cardMagic);
+        const unsigned quo = (t + ((n - t) >> q.cardSh1)) >> q.cardSh2;
+        return (long long)(n - quo * (unsigned)q.card);
+    }
+    return (long long)k % q.card;
+}
 
 // A work list: queries (indices into the descriptor array) and the prefix
 // sum of their work items.
@@ -115,17 +153,16 @@ __device__ __forceinline__ void blockAdd2(long long c, long long s, unsigned lon
     }
 }
 
-__device__ __forceinline__ long long slotFor(Slot* ht, int log2cap, long long key, unsigned maxProbe, unsigned* err,
+__device__ __forceinline__ long long slotFor(Slot* ht, int log2cap, unsigned enc, unsigned maxProbe, unsigned* err,
                                              bool* fresh) {
-    const unsigned long long enc = (unsigned long long)key ^ kKeyBias;
     const unsigned long long mask = (1ull << log2cap) - 1ull;
-    unsigned long long s = gpudb_hash_slot((unsigned long long)key, log2cap);
+    unsigned long long s = gpudb_hash_slot((unsigned long long)enc, log2cap);
     for (unsigned p = 0; p < maxProbe; ++p) {
-        const unsigned long long cur = *((volatile unsigned long long*)&ht[s].key);
+        const unsigned cur = *((volatile unsigned*)&ht[s].key);
         if (cur == enc) return (long long)s;
-        if (cur == 0ull) {
-            const unsigned long long prev = atomicCAS(&ht[s].key, 0ull, enc);
-            if (prev == 0ull) {
+        if (cur == 0u) {
+            const unsigned prev = atomicCAS(&ht[s].key, 0u, enc);
+            if (prev == 0u) {
                 *fresh = true;
                 return (long long)s;
             }
@@ -135,6 +172,23 @@ __device__ __forceinline__ long long slotFor(Slot* ht, int log2cap, long long ke
     }
     gpudb_set_error(err, GPUDB_ERR_HASH_OVERFLOW);
     return -1;
+}
+
+// Add (count, sum) to a group of the query's global table; a group created
+// here is appended to the slot list (one atomic per warp for the positions).
+__device__ __forceinline__ void globalAdd(const QDesc& q, bool live, unsigned enc, unsigned long long c,
+                                          unsigned long long v) {
+    bool fresh = false;
+    long long slot = -1;
+    if (live) {
+        slot = slotFor(q.ht, q.log2cap, enc, (unsigned)q.maxProbe, q.err, &fresh);
+        if (slot >= 0) {
+            atomicAdd(&q.ht[slot].count, (unsigned)c);
+            atomicAdd(&q.ht[slot].sum, v);
+        }
+    }
+    const unsigned long long pos = gpudb_warp_reserve(q.nslots, fresh);
+    if (fresh) q.slots[pos] = (unsigned)slot;
 }
 
 // ---- JOIN build: bitmap of dim keys with attr < attr_lt -------------------
@@ -211,9 +265,18 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
 }
 
 // ---- GROUPBY / TOPK: filter -> key % card -> hash table (count, sum) -------
-__global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile, unsigned long long* counter,
-                       int warpAgg) {
+__global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
+                                               unsigned long long* counter, int warpAgg) {
     __shared__ long long s_item;
+    __shared__ unsigned sKey[kSmemSlots];
+    __shared__ unsigned sCnt[kSmemSlots];
+    __shared__ unsigned long long sSum[kSmemSlots];
+    for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
+        sKey[i] = 0u;
+        sCnt[i] = 0u;
+        sSum[i] = 0ull;
+    }
+    volatile unsigned* vKey = sKey;
     const long long total = __ldg(wl.prefix + wl.nq);
     for (long long w; (w = pullWork(counter, total, &s_item)) >= 0;) {
         const int qi = findQuery(wl, w);
@@ -223,9 +286,6 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const long long* __restrict__ value = q.value;
         const int thr = q.thr;
         const long long card = q.card;
-        Slot* ht = q.ht;
-        const int log2cap = q.log2cap;
-        const unsigned maxProbe = (unsigned)q.maxProbe;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
         for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
@@ -242,22 +302,41 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
                 if (f[u] >= thr) continue;
-                const long long key = (long long)kr[u] % card;
-                long long c = 1, val = v[u];
+                const unsigned enc = encKey(keyMod(kr[u], q), card);
+                unsigned long long c = 1, val = (unsigned long long)v[u];
                 if (warpAgg) {
                     const unsigned am = __activemask();
-                    const unsigned peers = __match_any_sync(am, (unsigned long long)key);
+                    const unsigned peers = __match_any_sync(am, enc);
                     c = gpudb_peer_sum(am, peers, c);
                     val = gpudb_peer_sum(am, peers, val);
                     if ((int)(threadIdx.x & 31u) != __ffs(peers) - 1) continue;
                 }
-                bool fresh = false;
-                const long long slot = slotFor(ht, log2cap, key, maxProbe, q.err, &fresh);
-                if (slot < 0) continue;  // overflow bit set for this query
-                atomicAdd(&ht[slot].count, (unsigned long long)c);
-                atomicAdd(&ht[slot].sum, (unsigned long long)val);
-                if (fresh) q.slots[atomicAdd(q.nslots, 1ull)] = (unsigned)slot;
+                // shared-memory table first
+                unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc, 11);
+                bool done = false;
+#pragma unroll 1
+                for (int p = 0; p < kSmemProbe; ++p) {
+                    unsigned cur = vKey[h];
+                    if (cur == 0u) cur = atomicCAS(&sKey[h], 0u, enc) == 0u ? enc : vKey[h];
+                    if (cur == enc) {
+                        atomicAdd(&sCnt[h], (unsigned)c);
+                        atomicAdd(&sSum[h], val);
+                        done = true;
+                        break;
+                    }
+                    h = (h + 1u) & (kSmemSlots - 1);
+                }
+                if (!done) globalAdd(q, true, enc, c, val);
             }
+        }
+        __syncthreads();
+        // flush the shared table into the query's global table
+        for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
+            const unsigned k = sKey[i];
+            globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
+            sKey[i] = 0u;
+            sCnt[i] = 0u;
+            sSum[i] = 0ull;
         }
     }
 }
@@ -306,7 +385,7 @@ __global__ void __launch_bounds__(256) kTopKChunks(const QDesc* __restrict__ qs,
         }
         for (long long j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
             const Slot& s = q.ht[q.slots[j]];
-            gpudb_topk_push<kTopK>(vv, kk, (long long)s.sum, (long long)(s.key ^ kKeyBias));
+            gpudb_topk_push<kTopK>(vv, kk, (long long)s.sum, decKey(s.key, q.card));
         }
         long long ov[kTopK], ok[kTopK];
         blockTopK(vv, kk, sv, sk, ov, ok);
@@ -356,8 +435,7 @@ __global__ void __launch_bounds__(1024) kStats(const QDesc* __restrict__ qs, Wor
         const int* __restrict__ filter = q.filter;
         const int* __restrict__ keyc = q.key;
         const int thr = q.thr;
-        const long long card = q.card;
-        unsigned* bm = q.st_bitmap;
+                unsigned* bm = q.st_bitmap;
         const long long words = q.st_words;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const bool grouped = q.tmpl == GPUDB_TPL_GROUPBY || q.tmpl == GPUDB_TPL_TOPK;
@@ -374,7 +452,7 @@ __global__ void __launch_bounds__(1024) kStats(const QDesc* __restrict__ qs, Wor
                 if (f[u] >= thr) continue;
                 ++pass;
                 if (!grouped) continue;
-                const long long k = (long long)kr[u] % card;
+                const long long k = keyMod(kr[u], q);
                 const long long wd = k >> 5;
                 const unsigned bit = 1u << (unsigned)(k & 31);
                 if (k < 0 || wd >= words) {
@@ -412,7 +490,7 @@ __global__ void kSampleStats(const QDesc* __restrict__ qs, unsigned long long* o
         if (q.filter[r] >= q.thr) continue;
         atomicAdd(&s_pass, 1ull);
         if (!grouped) continue;
-        const unsigned long long k = (unsigned long long)((long long)q.key[r] % q.card);
+        const unsigned long long k = (unsigned long long)keyMod(q.key[r], q);
         unsigned h = (unsigned)gpudb_hash_slot(k, 13);
         for (int p = 0; p < kSampleSlots; ++p) {
             const unsigned long long cur = setKeys[h];
@@ -498,7 +576,7 @@ __global__ void kCollect(const QDesc* __restrict__ qs, WorkList wl, long long ch
             const long long j1 = min(n, (c + 1) * chunk);
             for (long long j = c * chunk + threadIdx.x; j < j1; j += blockDim.x) {
                 const Slot& s = q.ht[q.slots[j]];
-                dst[3 * j] = (long long)(s.key ^ kKeyBias);
+                dst[3 * j] = decKey(s.key, q.card);
                 dst[3 * j + 1] = (long long)s.count;
                 dst[3 * j + 2] = (long long)s.sum;
             }
@@ -574,6 +652,9 @@ struct gpudb_batch {
     bool dirty = true;
     long long lastLaunches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evStage[GPUDB_BATCH_STAGES + 1] = {};
+    double stageMs[GPUDB_BATCH_STAGES] = {};
+    bool stagesValid = false;
 };
 
 namespace {
@@ -628,6 +709,7 @@ int plan(gpudb_batch* b) {
         d.k = q.k;
         d.attr_lt = q.attr_lt;
         d.card = q.card > 0 ? q.card : 1;
+        cardDivisor(d.card, &d.cardMagic, &d.cardSh1, &d.cardSh2);
         d.rows = (long long)q.rows;
         d.key = q.key;
         d.filter = q.filter;
@@ -733,32 +815,43 @@ int gridFor(gpudb_batch* b, const void* fn, int block) {
     return std::max(1, occ) * b->numSMs;
 }
 
-// Enqueue the memset + kernels of one execution on b->stream.
-int enqueue(gpudb_batch* b) {
+// Enqueue the memset + kernels of one execution on b->stream; with `stages`
+// an event follows every step (not inside a graph capture).
+int enqueue(gpudb_batch* b, bool stages) {
     const int n = (int)b->queries.size();
     long long launches = 0;
+    auto mark = [&](int i) { if (stages) cudaEventRecord(b->evStage[i], b->stream); };
+    mark(0);
     B_CHECK(cudaMemsetAsync(b->arena.p, 0, b->zeroBytes, b->stream), GPUDB_E_CUDA);
+    mark(1);
     if (b->wlBuild.nq) {
         kJoinBuild<<<gridFor(b, (const void*)kJoinBuild, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlBuild,
                                                                                               b->tile, b->counters + 0);
         launches++;
     }
+    mark(2);
     if (b->wlAgg.nq) {
         kAgg<<<gridFor(b, (const void*)kAgg, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlAgg, b->tile,
                                                                                   b->counters + 1);
         launches++;
     }
+    mark(3);
     if (b->wlGroup.nq) {
         kGroup<<<gridFor(b, (const void*)kGroup, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlGroup, b->tile,
                                                                                       b->counters + 2, b->warpAgg);
         launches++;
     }
+    mark(4);
     if (b->nTopk) {
         kTopKChunks<<<gridFor(b, (const void*)kTopKChunks, 256), 256, 0, b->stream>>>(b->dDesc, b->wlTopk,
                                                                                       b->counters + 3);
+        mark(5);
         kTopKMerge<<<b->nTopk, 256, 0, b->stream>>>(b->dDesc, b->dTopk);
         launches += 2;
+    } else {
+        mark(5);
     }
+    mark(6);
     B_CHECK(cudaGetLastError(), GPUDB_E_LAUNCH);
     // per-query error words -> pinned host copy
     for (int i = 0; i < n; i++)
@@ -790,6 +883,7 @@ int gpudb_batch_create(gpudb_ctx* ctx, gpudb_batch** out) {
     B_CHECK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), GPUDB_E_CUDA);
     B_CHECK(cudaEventCreate(&b->ev0), GPUDB_E_CUDA);
     B_CHECK(cudaEventCreate(&b->ev1), GPUDB_E_CUDA);
+    for (auto& e : b->evStage) B_CHECK(cudaEventCreate(&e), GPUDB_E_CUDA);
     B_CHECK(cudaFuncSetAttribute(kSampleStats, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kSampleSlots * sizeof(unsigned long long))),
             GPUDB_E_LAUNCH);
@@ -806,6 +900,8 @@ void gpudb_batch_free(gpudb_batch* b) {
     if (b->errHost) cudaFreeHost(b->errHost);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    for (auto& e : b->evStage)
+        if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -819,8 +915,8 @@ int gpudb_batch_set_queries(gpudb_batch* b, const gpudb_batch_query* q, int n) {
             gpudb::setThreadError(who + " is malformed");
             return GPUDB_E_INVALID;
         }
-        if (grouped(x.tmpl) && ((x.rows && !x.key) || x.card < 1 || x.card > (1ll << 31))) {
-            gpudb::setThreadError(who + " needs a key column and 1 <= card <= 2^31");
+        if (grouped(x.tmpl) && ((x.rows && !x.key) || x.card < 1 || x.card >= (1ll << 31) || x.rows >= (1ull << 32))) {
+            gpudb::setThreadError(who + " needs a key column, 1 <= card < 2^31 and fewer than 2^32 rows");
             return GPUDB_E_INVALID;
         }
         if (grouped(x.tmpl) && x.groups > (1ull << 30)) {
@@ -872,7 +968,7 @@ int gpudb_batch_execute(gpudb_batch* b, int use_graph, double* ms, uint32_t* err
     if (use_graph) {
         if (!b->graphExec) {
             B_CHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), GPUDB_E_CUDA);
-            const int st = enqueue(b);
+            const int st = enqueue(b, false);
             cudaGraph_t g = nullptr;
             const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
             if (st != GPUDB_OK) {
@@ -884,12 +980,21 @@ int gpudb_batch_execute(gpudb_batch* b, int use_graph, double* ms, uint32_t* err
             B_CHECK(cudaGraphInstantiate(&b->graphExec, g, 0), GPUDB_E_CUDA);
         }
         B_CHECK(cudaGraphLaunch(b->graphExec, b->stream), GPUDB_E_CUDA);
+        b->stagesValid = false;
     } else {
-        if (int st = enqueue(b)) return st;
+        if (int st = enqueue(b, true)) return st;
     }
     B_CHECK(cudaEventRecord(b->ev1, b->stream), GPUDB_E_CUDA);
     B_CHECK(cudaEventSynchronize(b->ev1), GPUDB_E_CUDA);
     if (ms) *ms = elapsed(b);
+    if (!use_graph) {
+        for (int i = 0; i < GPUDB_BATCH_STAGES; i++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, b->evStage[i], b->evStage[i + 1]);
+            b->stageMs[i] = t;
+        }
+        b->stagesValid = true;
+    }
     if (errors && n) std::memcpy(errors, b->errHost, sizeof(unsigned) * n);
     return GPUDB_OK;
 }
@@ -1082,7 +1187,7 @@ int gpudb_batch_result_groups(gpudb_batch* b, int qi, uint64_t cap, uint64_t* ng
     B_CHECK(cudaStreamSynchronize(b->stream), GPUDB_E_CUDA);
     for (unsigned long long j = 0; j < n; j++) {
         const Slot& s = table[slots[j]];
-        keys[j] = (int64_t)(s.key ^ kKeyBias);
+        keys[j] = (int64_t)decKey(s.key, d.card);
         counts[j] = (int64_t)s.count;
         sums[j] = (int64_t)s.sum;
     }
@@ -1108,5 +1213,15 @@ int gpudb_batch_result_topk(gpudb_batch* b, int qi, int64_t* keys, int64_t* vals
 }
 
 long long gpudb_batch_last_launches(gpudb_batch* b) { return b ? b->lastLaunches : 0; }
+
+int gpudb_batch_stage_ms(gpudb_batch* b, double* ms) {
+    if (!b || !ms) return GPUDB_E_INVALID;
+    if (!b->stagesValid) {
+        gpudb::setThreadError("batch: stage times need an execute without a graph");
+        return GPUDB_E_INVALID;
+    }
+    for (int i = 0; i < GPUDB_BATCH_STAGES; i++) ms[i] = b->stageMs[i];
+    return GPUDB_OK;
+}
 
 }  // extern "C"

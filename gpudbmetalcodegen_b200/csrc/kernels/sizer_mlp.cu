@@ -318,6 +318,8 @@ int gpudb_sizer_train(gpudb_sizer* s, const float* X, const float* Y, int n, int
     std::mt19937_64 rng(seed);
     std::vector<float> px((size_t)n * kIn), py((size_t)n * kOut);
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const long long totalSteps = (long long)epochs * ((n + batch - 1) / batch);
+    long long runStep = 0;
     float last = 0.0f;
     for (int ep = 0; ep < epochs; ep++) {
         std::shuffle(idx.begin(), idx.end(), rng);
@@ -336,8 +338,13 @@ int gpudb_sizer_train(gpudb_sizer* s, const float* X, const float* Y, int n, int
             if (int st = launchTrain(s, s->X + (size_t)off * kIn, s->Y + (size_t)off * kOut, cur, cur)) return st;
             s->step++;
             const float c1 = 1.0f - std::pow(b1, (float)s->step), c2 = 1.0f - std::pow(b2, (float)s->step);
-            adamStep<<<(kParams + 255) / 256, 256, 0, s->stream>>>(s->w, s->wbf, s->m, s->v, s->grad, lr, b1, b2, eps,
-                                                                    c1, c2);
+            // cosine decay of the learning rate over this call's steps
+            const float lrNow =
+                totalSteps > 1 ? lr * 0.5f * (1.0f + std::cos(3.14159265358979f * (float)runStep / (float)totalSteps))
+                               : lr;
+            runStep++;
+            adamStep<<<(kParams + 255) / 256, 256, 0, s->stream>>>(s->w, s->wbf, s->m, s->v, s->grad, lrNow, b1, b2,
+                                                                    eps, c1, c2);
         }
         SZ_CHECK(cudaGetLastError(), GPUDB_E_LAUNCH);
         float l = 0;

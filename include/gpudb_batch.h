@@ -43,7 +43,8 @@ int gpudb_sizer_set_params(gpudb_sizer* s, const float* in);
  * arrays, n x 16 and n x 2) with the current BF16 weights; gradients w.r.t.
  * the parameters are copied to grads_out. No update. */
 int gpudb_sizer_grads(gpudb_sizer* s, const float* X, const float* Y, int n, float* grads_out, float* loss_out);
-/* Adam training on the GPU: `epochs` passes over (X, Y) in shuffled batches. */
+/* Adam training on the GPU: `epochs` passes over (X, Y) in shuffled batches,
+ * learning rate `lr` decayed to 0 along a half cosine over the call's steps. */
 int gpudb_sizer_train(gpudb_sizer* s, const float* X, const float* Y, int n, int epochs, int batch, float lr,
                       uint64_t seed, float* final_loss);
 int gpudb_sizer_predict(gpudb_sizer* s, const float* X, int n, float* Y_out);
@@ -114,6 +115,10 @@ int gpudb_batch_collect(gpudb_batch* b, uint64_t* rows, void* host, uint64_t hos
                         double* ms);
 /* Launches of this library's kernels in the last execute. */
 long long gpudb_batch_last_launches(gpudb_batch* b);
+/* Device time of each step of the last execute run without a graph:
+ * zero fill, join build, agg / join probe, group-by, top-k chunks, top-k merge. */
+#define GPUDB_BATCH_STAGES 6
+int gpudb_batch_stage_ms(gpudb_batch* b, double* ms);
 
 #ifdef __cplusplus
 }

@@ -56,6 +56,13 @@ int gpudb_gen_mix(uint64_t seed, uint64_t nranks, double s, uint64_t dim_rows, u
                   int32_t* rank_u, int32_t* rank_z, int32_t* filter, int64_t* value, int32_t* fk, int threads);
 /* Mixed-workload dimension: key = row + 1, attr U[0,1000). */
 int gpudb_gen_mixdim(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* attr, int threads);
+/* Device twins of gpudb_gen_mix / gpudb_gen_mixdim: identical values written
+ * straight into device memory on `stream` (NULL = the default stream);
+ * return after the stream has finished. */
+int gpudb_gen_mix_device(uint64_t seed, uint64_t nranks, double s, uint64_t dim_rows, uint64_t row0, uint64_t n,
+                         int32_t* rank_u, int32_t* rank_z, int32_t* filter, int64_t* value, int32_t* fk,
+                         void* stream);
+int gpudb_gen_mixdim_device(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* attr, void* stream);
 
 #ifdef __cplusplus
 }

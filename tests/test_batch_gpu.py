@@ -230,3 +230,32 @@ def test_learned_sizer_gain(ctx, tables):
     assert learned.table_slots < bound.table_slots
     assert len(learned.overflowed) <= 2
     sizer.close()
+
+
+def test_device_generators_match_host():
+    import torch
+    from gpudbmetalcodegen_b200 import _lib
+    lib = _lib.load()
+    for s, row0, n in ((0.8, 0, 100_000), (1.3, 123_456_789, 77_777)):
+        host = W.gen_mix(n, nranks=1 << 20, s=s, dim_rows=5000, seed=9, row0=row0)
+        dev = {c: torch.empty(n, dtype={np.int32: torch.int32, np.int64: torch.int64}[dt], device="cuda")
+               for c, dt in W.MIX_COLUMNS.items()}
+        assert lib.gpudb_gen_mix_device(9, 1 << 20, s, 5000, row0, n, *(dev[c].data_ptr() for c in W.MIX_COLUMNS),
+                                        None) == 0
+        for c in W.MIX_COLUMNS:
+            assert np.array_equal(dev[c].cpu().numpy(), host[c]), c
+    md = W.gen_mixdim(30_000, seed=4)
+    k = torch.empty(30_000, dtype=torch.int32, device="cuda")
+    a = torch.empty(30_000, dtype=torch.int32, device="cuda")
+    assert lib.gpudb_gen_mixdim_device(4, 0, 30_000, k.data_ptr(), a.data_ptr(), None) == 0
+    assert np.array_equal(k.cpu().numpy(), md["md_key"]) and np.array_equal(a.cpu().numpy(), md["md_attr"])
+
+
+def test_stage_times(tables):
+    qs = mixed(tables, 16, seed=9)
+    b = B.Batch()
+    b.set_queries([tables.query_struct(q, groups=q.card) for q in qs])
+    b.execute(use_graph=False)
+    st = b.stage_ms()
+    assert set(st) == set(B.Batch.STAGES) and all(v >= 0 for v in st.values())
+    b.close()

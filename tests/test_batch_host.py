@@ -62,7 +62,8 @@ def test_unpack_results():
                        [0, 0, 0]], dtype=np.uint64).astype(np.int64)
     res = B.unpack_results(qs, np.array([1, 2, 2, 1], dtype=np.uint64), packed)
     assert res[0] == ("scalar", 7, big)
-    assert res[1][0] == "groups" and list(res[1][1]) == [2, 5] and list(res[1][3]) == [30, 10]
+    g = B.canonical(res[1])
+    assert g[0] == "groups" and list(g[1]) == [2, 5] and list(g[3]) == [30, 10]
     assert res[2] == ("topk", ((2, 30), (5, 10)))
     assert res[3] == ("scalar", 0, 0)
     assert B.same_result(res[1], B.canonical_groups([5, 2], [1, 3], [10, 30]))
@@ -121,3 +122,26 @@ def test_adam_oracle_first_step_is_signed_lr():
     g = np.array([1.0, -2.0, 0.5, -1e-3, 3.0])
     w1, m, v = M.adam_step(w, np.zeros(5), np.zeros(5), g, 1, lr=0.01)
     assert np.allclose(w1, -0.01 * np.sign(g), atol=1e-7)
+
+
+def test_invariant_divisor_method():
+    """The multiply-high division the batch kernels use for key % card
+    (Granlund & Montgomery 1994, Fig. 4.1), restated and checked exhaustively
+    at the edges and on random dividends / divisors below 2^31."""
+    import random
+
+    def div(n, d):
+        l = 0
+        while (1 << l) < d:
+            l += 1
+        m = ((1 << 32) * ((1 << l) - d)) // d + 1
+        assert m < (1 << 32)
+        t = (n * m) >> 32
+        return (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0)
+
+    rnd = random.Random(1)
+    ds = [1, 2, 3, 4, 5, 7, 100, 1023, 1024, 1025, (1 << 20) + 3, (1 << 31) - 1] + \
+        [rnd.randrange(1, 1 << 31) for _ in range(200)]
+    for d in ds:
+        for n in [0, 1, d - 1, d, d + 1, (1 << 31) - 1] + [rnd.randrange(0, 1 << 31) for _ in range(200)]:
+            assert div(n, d) == n // d, (n, d)
