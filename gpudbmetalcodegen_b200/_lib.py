@@ -63,6 +63,8 @@ _SIGNATURES = [
     ("gpudb_set_kernel_cache_dir", None, [C.c_char_p]),
     ("gpudb_register_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
     ("gpudb_upload_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
+    ("gpudb_register_host_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64,
+                                             C.c_int]),
     ("gpudb_register_rows", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
     ("gpudb_register_buffer", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
     ("gpudb_register_symbol", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),

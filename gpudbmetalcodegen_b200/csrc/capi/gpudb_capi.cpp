@@ -200,6 +200,17 @@ int gpudb_upload_column(gpudb_ctx* ctx, const char* table, const char* column, c
     }
 }
 
+int gpudb_register_host_column(gpudb_ctx* ctx, const char* table, const char* column, const void* host,
+                               uint64_t rows, int elem_bytes) {
+    if (!ctx || !table || !column || (!host && rows) || elem_bytes <= 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    try {
+        ctx->qc->ex.registerHostColumn(column, table, host, rows, (size_t)elem_bytes);
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, GPUDB_E_INVALID, e.what());
+    }
+}
+
 int gpudb_register_rows(gpudb_ctx* ctx, const char* table, uint64_t rows) {
     if (!ctx || !table) return fail(ctx, GPUDB_E_INVALID, "bad argument");
     ctx->qc->ex.registerTableRowCount(table, rows);

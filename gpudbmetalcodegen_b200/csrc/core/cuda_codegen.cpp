@@ -44,6 +44,28 @@ void CudaCodegen::addRawCode(const std::string& code) { cur("addRawCode").code +
 void CudaCodegen::addHelper(const std::string& code) { helperCode_ += code + "\n"; }
 std::string CudaCodegen::fresh(const std::string& stem) { return stem + std::to_string(freshCounter_++); }
 
+int CudaCodegen::pushScanHint(const ScanHint& h) {
+    scanHints_.push_back(h);
+    return (int)scanHints_.size() - 1;
+}
+
+void CudaCodegen::popScanHint() {
+    if (!scanHints_.empty()) {
+        prefetchVars_.erase((int)scanHints_.size() - 1);
+        scanHints_.pop_back();
+    }
+}
+
+void CudaCodegen::setPrefetchVar(int id, const std::string& var) {
+    if (var.empty()) prefetchVars_.erase(id);
+    else prefetchVars_[id] = var;
+}
+
+std::string CudaCodegen::prefetchVar(int id) const {
+    auto it = prefetchVars_.find(id);
+    return it == prefetchVars_.end() ? std::string() : it->second;
+}
+
 // ---------------------------------------------------------------------------
 // phases
 // ---------------------------------------------------------------------------

@@ -48,6 +48,25 @@ public:
     // Unique identifier for temporaries (e.g. "_t3").
     std::string fresh(const std::string& stem);
 
+    // ---- scan hints ------------------------------------------------------
+    // An operator pushes a hint before it calls its child's produce() and
+    // pops it afterwards, so the scan at the bottom of the chain sees, top
+    // down, what the operators above it will do with each row: a selection's
+    // guard, a bitmap probe's word it may load ahead (BitmapPrefetch), or a
+    // barrier (an operator that defines names the scan cannot evaluate).
+    struct ScanHint {
+        enum Kind { Guard, BitmapPrefetch, Barrier } kind;
+        std::string expr;    // guard predicate / probe key expression
+        std::string bitmap;  // BitmapPrefetch: bitmap buffer name
+    };
+    int pushScanHint(const ScanHint& h);
+    void popScanHint();
+    const std::vector<ScanHint>& scanHints() const { return scanHints_; }
+    // Set by the scan while it emits a row body whose bitmap word for hint
+    // `id` is already in a register; empty when not prefetched.
+    void setPrefetchVar(int id, const std::string& var);
+    std::string prefetchVar(int id) const;
+
     // ---- phases: one phase = one kernel --------------------------------
     void beginPhase(const std::string& phaseName);
     void endPhase();
@@ -136,6 +155,8 @@ private:
     CudaResultSchema resultSchema_;
     unsigned indentLevel_ = 1;
     int freshCounter_ = 0;
+    std::vector<ScanHint> scanHints_;
+    std::unordered_map<int, std::string> prefetchVars_;
 
     PhaseInfo& cur(const char* op);
     std::string indent() const { return std::string(indentLevel_ * 4, ' '); }

@@ -132,6 +132,22 @@ void CudaGenericExecutor::uploadColumn(const std::string& column, const std::str
     registerTableRowCount(table, rows);
 }
 
+void CudaGenericExecutor::registerHostColumn(const std::string& column, const std::string& table, const void* host,
+                                             size_t rows, size_t elemBytes) {
+    void* dptr = nullptr;
+    if (rows) {
+        const cudaError_t e = cudaHostGetDevicePointer(&dptr, const_cast<void*>(host), 0);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("host column '" + column + "': not pinned, mapped host memory (" +
+                                     cudaGetErrorString(e) + ")");
+        }
+    }
+    columns_[column] = {dptr, rows, elemBytes, ++generationCounter_, true};
+    registerTableRowCount(table, rows);
+    clearGraphs();
+}
+
 size_t CudaGenericExecutor::tableRows(const std::string& table) const {
     auto it = tableRows_.find(table);
     if (it != tableRows_.end()) return it->second;
@@ -281,6 +297,12 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
                 auto it = columns_.find(b.name);
                 if (it == columns_.end()) {
                     error = "required column '" + b.name + "' (table '" + b.tableName + "') is not registered";
+                    return false;
+                }
+                if (it->second.host && !b.late) {
+                    error = "phase '" + ph.name + "': column '" + b.name +
+                            "' is in host memory but every row reads it; only late-materialised columns may stay "
+                            "on the host (upload it instead)";
                     return false;
                 }
                 s = (uint64_t)(uintptr_t)it->second.ptr;

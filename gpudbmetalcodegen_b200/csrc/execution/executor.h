@@ -65,6 +65,11 @@ public:
     // device buffer (reused across calls when large enough) on the stream.
     void uploadColumn(const std::string& column, const std::string& table, const void* host, size_t rows,
                       size_t elemBytes);
+    // Column left in pinned, mapped host memory and read in place by the
+    // kernels (over the host link, at access time). Only a late-materialised
+    // binding may use it: rows that fail earlier selections never touch it.
+    void registerHostColumn(const std::string& column, const std::string& table, const void* host, size_t rows,
+                            size_t elemBytes);
 
     // --- execution -----------------------------------------------------------
     // Run phases [first, last) (last < 0 = all) `warmup` + `measured` times.
@@ -102,6 +107,7 @@ private:
         size_t rows = 0;
         size_t elemBytes = 0;
         uint64_t generation = 0;
+        bool host = false;  // pinned host memory read in place
     };
     uint64_t generationCounter_ = 0;
     struct Launch {

@@ -113,6 +113,19 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.setPhaseTileRows(tile);
 
     const std::string SB = S(stageBytes), ST = S(stages), TL = S(tile);
+    // The innermost bitmap probe above this scan, if no operator between
+    // them defines names: its words are loaded for prefetchRows rows ahead.
+    int pf = -1;
+    if (cfg_.prefetchRows > 0) {
+        const auto& hs = cg.scanHints();
+        for (int h = (int)hs.size() - 1; h >= 0; --h) {
+            if (hs[h].kind == CudaCodegen::ScanHint::Barrier) break;
+            if (hs[h].kind == CudaCodegen::ScanHint::BitmapPrefetch) {
+                pf = h;
+                break;
+            }
+        }
+    }
     cg.addComment("TMA-bulk staged scan of " + tableName_ + ": " + TL + "-row tiles, " + ST +
                   "-stage cp.async.bulk ring, " + S(txBytes) + " B per tile; warp 0 produces, the other warps consume");
     cg.addBlock("", [&]() {
@@ -183,12 +196,16 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                         cg.addLine("const " + c.cudaType + "* " + c.paramName + " = reinterpret_cast<const " + c.cudaType +
                                    "*>(_sb_st + " + S(off[k]) + ");");
                 }
-                cg.addBlock("for (int " + i + " = (int)threadIdx.x - 32; " + i + " < " + TL + "; " + i +
-                                " += (int)blockDim.x - 32)",
-                            [&]() {
-                                cg.addLine("const long long _row = _sb_base + " + i + "; (void)_row;");
-                                consume();
-                            });
+                if (pf < 0) {
+                    cg.addBlock("for (int " + i + " = (int)threadIdx.x - 32; " + i + " < " + TL + "; " + i +
+                                    " += (int)blockDim.x - 32)",
+                                [&]() {
+                                    cg.addLine("const long long _row = _sb_base + " + i + "; (void)_row;");
+                                    consume();
+                                });
+                } else {
+                    emitPrefetchedRows(cg, consume, pf, TL);
+                }
             });
             cg.addLine("__syncwarp();");
             cg.addLine("if ((threadIdx.x & 31u) == 0u) gpudb_mbar_arrive(_sb_empty + _s);");
@@ -203,6 +220,45 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                         cg.addLine("const long long _row = " + i + "; (void)_row;");
                         consume();
                     });
+    });
+}
+
+// Consumer row loop of a staged tile with the bitmap words of hint `pf`
+// loaded for prefetchRows rows before any of them is used: the loads are
+// independent, so each thread keeps several L2 requests in flight instead
+// of one per row.
+void CudaGridStrideScan::emitPrefetchedRows(CudaCodegen& cg, ConsumerFn consume, int pf, const std::string& TL) {
+    const int kPrefetchRows = cfg_.prefetchRows;
+    const auto hint = cg.scanHints()[pf];
+    std::string guard;
+    for (size_t h = pf + 1; h < cg.scanHints().size(); ++h)
+        if (cg.scanHints()[h].kind == CudaCodegen::ScanHint::Guard)
+            guard += " && (" + cg.scanHints()[h].expr + ")";
+    const std::string& i = idxVar_;
+    const std::string U = S(kPrefetchRows);
+    cg.addLine("const int _pf_step = (int)blockDim.x - 32;");
+    cg.addBlock("for (int _pf_i0 = (int)threadIdx.x - 32; _pf_i0 < " + TL + "; _pf_i0 += " + U + " * _pf_step)", [&]() {
+        cg.addLine("unsigned _pfw[" + U + "];");
+        cg.addLine("#pragma unroll");
+        cg.addBlock("for (int _pf_u = 0; _pf_u < " + U + "; ++_pf_u)", [&]() {
+            cg.addLine("const int " + i + " = _pf_i0 + _pf_u * _pf_step;");
+            cg.addLine("_pfw[_pf_u] = 0u;");
+            cg.addBlock("if (" + i + " < " + TL + guard + ")", [&]() {
+                cg.addLine("const long long _pf_k = (long long)(" + hint.expr + ");");
+                cg.addLine("if ((unsigned long long)(_pf_k >> 5) < (unsigned long long)len_" + hint.bitmap + ") _pfw[_pf_u] = __ldg(" +
+                           hint.bitmap + " + (_pf_k >> 5));");
+            });
+        });
+        cg.addLine("#pragma unroll");
+        cg.addBlock("for (int _pf_u = 0; _pf_u < " + U + "; ++_pf_u)", [&]() {
+            cg.addLine("const int " + i + " = _pf_i0 + _pf_u * _pf_step;");
+            cg.addBlock("if (" + i + " < " + TL + ")", [&]() {
+                cg.addLine("const long long _row = _sb_base + " + i + "; (void)_row;");
+                cg.setPrefetchVar(pf, "_pfw[_pf_u]");
+                consume();
+                cg.setPrefetchVar(pf, "");
+            });
+        });
     });
 }
 
@@ -253,7 +309,9 @@ CudaSelection::CudaSelection(std::unique_ptr<CudaOperator> child, const std::str
     : CudaUnaryOperator(std::move(child)), predicate_(predicate) {}
 
 void CudaSelection::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.pushScanHint({CudaCodegen::ScanHint::Guard, predicate_, ""});
     child_->produce(cg, [&]() { cg.addIf(predicate_, [&]() { consume(); }); });
+    cg.popScanHint();
 }
 
 std::string CudaSelection::describe() const { return "Selection(" + predicate_ + ")"; }
@@ -263,10 +321,12 @@ CudaComputeExpr::CudaComputeExpr(std::unique_ptr<CudaOperator> child, const std:
     : CudaUnaryOperator(std::move(child)), varName_(varName), varType_(varType), expression_(expression) {}
 
 void CudaComputeExpr::produce(CudaCodegen& cg, ConsumerFn consume) {
+    cg.pushScanHint({CudaCodegen::ScanHint::Barrier, "", ""});
     child_->produce(cg, [&]() {
         cg.addLine("const " + varType_ + " " + varName_ + " = " + expression_ + ";");
         consume();
     });
+    cg.popScanHint();
 }
 
 std::string CudaComputeExpr::describe() const { return "ComputeExpr(" + varName_ + " = " + expression_ + ")"; }
@@ -317,14 +377,19 @@ CudaBitmapProbe::CudaBitmapProbe(std::unique_ptr<CudaOperator> child, const std:
 void CudaBitmapProbe::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addBitmapReadParam(bitmapName_, "");
     cg.addBufferLengthParam("len_" + bitmapName_, bitmapName_);
+    // a (non-anti) probe lets the TMA scan load its bitmap words ahead
+    const int hint = anti_ ? -1 : cg.pushScanHint({CudaCodegen::ScanHint::BitmapPrefetch, keyExpr_, bitmapName_});
     child_->produce(cg, [&]() {
         const std::string k = cg.fresh("_pk");
         cg.addLine("const long long " + k + " = (long long)(" + keyExpr_ + ");");
         // Keys beyond the bitmap are simply absent (not an error on probe).
         const std::string inb = "(unsigned long long)(" + k + " >> 5) < (unsigned long long)len_" + bitmapName_;
-        const std::string t = "gpudb_bitmap_test(" + bitmapName_ + ", " + k + ")";
+        const std::string word = hint >= 0 ? cg.prefetchVar(hint) : std::string();
+        const std::string t = word.empty() ? "gpudb_bitmap_test(" + bitmapName_ + ", " + k + ")"
+                                           : "((" + word + " >> (unsigned)(" + k + " & 31)) & 1u)";
         cg.addIf(anti_ ? "!(" + inb + " && " + t + ")" : "(" + inb + ") && " + t, [&]() { consume(); });
     });
+    if (hint >= 0) cg.popScanHint();
 }
 
 std::string CudaBitmapProbe::describe() const {
@@ -370,6 +435,11 @@ CudaArrayLookup::CudaArrayLookup(std::unique_ptr<CudaOperator> child, const std:
 void CudaArrayLookup::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addReadBufferParam(arrayName_, resultType_);
     cg.addBufferLengthParam("len_" + arrayName_, arrayName_);
+    cg.pushScanHint({CudaCodegen::ScanHint::Barrier, "", ""});
+    struct Pop {
+        CudaCodegen& c;
+        ~Pop() { c.popScanHint(); }
+    } pop{cg};
     child_->produce(cg, [&]() {
         const std::string k = cg.fresh("_lk");
         cg.addLine("const long long " + k + " = (long long)(" + keyExpr_ + ");");
@@ -839,6 +909,11 @@ void CudaHashProbe::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addHashMapReadParam(table_ + "_keys", ko.store);
     for (const auto& p : payloadReads_) cg.addReadBufferParam(table_ + "_" + p.first, p.second);
     cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    cg.pushScanHint({CudaCodegen::ScanHint::Barrier, "", ""});
+    struct Pop {
+        CudaCodegen& c;
+        ~Pop() { c.popScanHint(); }
+    } pop{cg};
     child_->produce(cg, [&]() {
         cg.addLine("const long long " + slotVar_ + " = " + ko.find + "(" + table_ + "_keys, " + table_ + "_log2cap, " +
                    ko.cast + "(" + keyExpr_ + "), " + S(probeArg(layout_, maxProbe_)) + "u);");

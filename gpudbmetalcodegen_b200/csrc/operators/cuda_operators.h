@@ -48,6 +48,7 @@ struct ScanConfig {
     Mode mode = TmaBulk;
     int tileRows = 0;      // rows per TMA tile (multiple of 16); 0 = about 24 KB of staged columns
     int stages = 4;        // TMA ring depth (clamped to the shared-memory budget)
+    int prefetchRows = 0;  // rows whose probe bitmap words are loaded ahead (0 = off)
 };
 
 // ------------------------------------------------------------------
@@ -77,6 +78,11 @@ public:
     std::string describe() const override;
     const std::string& tableName() const { return tableName_; }
     const std::vector<ColumnDesc>& columns() const { return columns_; }
+
+private:
+    void emitPrefetchedRows(CudaCodegen& cg, ConsumerFn consume, int pf, const std::string& tileRows);
+
+public:
 
 private:
     std::string tableName_, rowVar_, idxVar_;

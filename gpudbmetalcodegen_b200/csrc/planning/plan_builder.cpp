@@ -97,7 +97,7 @@ std::string TuneConfig::toString() const {
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
-      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM;
+      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows;
     return o.str();
 }
 
@@ -121,11 +121,13 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "probe") t.maxProbe = std::stoi(v);
         else if (k == "late") t.lateMaterialize = std::stoi(v) != 0;
         else if (k == "occ") t.minBlocksPerSM = std::stoi(v);
+        else if (k == "pf") t.scan.prefetchRows = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
         throw std::runtime_error("tune: bs must be a multiple of 32 in [32,1024]");
     if (t.scan.tileRows < 0 || t.scan.tileRows % 16) throw std::runtime_error("tune: tile must be a multiple of 16 (0 = auto)");
+    if (t.scan.prefetchRows < 0 || t.scan.prefetchRows > 16) throw std::runtime_error("tune: pf must be in [0,16]");
     return t;
 }
 

@@ -202,6 +202,12 @@ class Context:
         self._keep.append(t)
         self.register_column(table, column, t.data_ptr(), t.numel(), t.element_size())
 
+    def register_host_column(self, table: str, column: str, host_ptr: int, rows: int, elem_bytes: int) -> None:
+        """A pinned host column (gpudb_host_alloc) read in place by kernels
+        that materialise it late; see gpudb_register_host_column."""
+        check(self._lib.gpudb_register_host_column(self.handle, table.encode(), column.encode(), C.c_void_p(host_ptr),
+                                                   rows, elem_bytes), self.handle)
+
     def upload_column(self, table: str, column: str, arr: np.ndarray) -> None:
         arr = np.ascontiguousarray(arr)
         check(self._lib.gpudb_upload_column(self.handle, table.encode(), column.encode(), arr.ctypes.data,

@@ -131,6 +131,13 @@ int gpudb_register_column(gpudb_ctx* ctx, const char* table, const char* column,
  * resident HBM; host memory from gpudb_host_alloc is pinned). */
 int gpudb_upload_column(gpudb_ctx* ctx, const char* table, const char* column, const void* host, uint64_t rows,
                         int elem_bytes);
+/* The reference's zero-copy column (newBuffer(ptr), the kernel reads host
+ * memory in place) for columns a plan reads late: `host` must be pinned
+ * (gpudb_host_alloc); kernels read it over the host link only for rows that
+ * survive the earlier selections. Executing a plan that reads it for every
+ * row fails (status < 0, message in gpudb_last_error) instead of streaming it. */
+int gpudb_register_host_column(gpudb_ctx* ctx, const char* table, const char* column, const void* host,
+                               uint64_t rows, int elem_bytes);
 /* registerTableRowCount. */
 int gpudb_register_rows(gpudb_ctx* ctx, const char* table, uint64_t rows);
 /* registerAllocatedBuffer: caller-owned device buffer (not freed). */

@@ -141,6 +141,39 @@ def test_max_key_pass(ctx):
     assert ctx.register_max_key("b_key") == O.max_i32(d["b_key"]) == 123_457
 
 
+def test_join_late_columns_read_in_place_from_host(ctx):
+    """Late-materialised columns left in pinned host memory (zero-copy) give
+    the same answer; a host column every row would read is refused before
+    any launch."""
+    import ctypes as C
+    from gpudbmetalcodegen_b200 import _lib
+    lib = _lib.load()
+    d, p = load_join(ctx, 200_000, 800_000, seed=21)
+    top, _, _ = O.join_topk(d, p, k=10)
+    held = []
+    for c in ("p_price", "p_discount", "p_fk"):
+        a = p[c]
+        ptr = lib.gpudb_host_alloc(a.nbytes)
+        np.ctypeslib.as_array((C.c_uint8 * a.nbytes).from_address(ptr))[:] = a.view(np.uint8)
+        held.append(ptr)
+    try:
+        ctx.register_host_column("probe", "p_price", held[0], p["p_price"].shape[0], 8)
+        ctx.register_host_column("probe", "p_discount", held[1], p["p_discount"].shape[0], 8)
+        res, t = ctx.run("template=join_topk")
+        assert t.device_error == 0 and res.rows == top
+        ctx.register_host_column("probe", "p_fk", held[2], p["p_fk"].shape[0], 4)
+        with pytest.raises(GpudbError):
+            ctx.run("template=join_topk")
+        with pytest.raises(GpudbError):  # pageable memory is not accepted
+            ctx.register_host_column("probe", "p_fk", p["p_fk"].ctypes.data, p["p_fk"].shape[0], 4)
+    finally:
+        for c in ("p_price", "p_discount", "p_fk"):
+            ctx.upload_column("probe", c, p[c])
+        ctx.synchronize()
+        for ptr in held:
+            lib.gpudb_host_free(C.c_void_p(ptr))
+
+
 def test_join_topk_full_size(ctx):
     d, p = load_join(ctx, W.DIM_ROWS, W.PROBE_ROWS, seed=W.SEED)
     top, groups, distinct = O.join_topk(d, p, k=10)
