@@ -329,18 +329,21 @@ def run_reference(args, w: Workload):
 # ---------------------------------------------------------------------------
 # mixed-query batches with the learned sizer
 # ---------------------------------------------------------------------------
-def mixed_oracle_seconds(args, queries, budget_s: float):
+def mixed_oracle_seconds(args, queries, budget_s: float, dim_rows=None, zipf=None):
     """The oracle (the reference's operator semantics restated on the CPU,
     all host cores) over the first queries of the batch until `budget_s`
     has passed; slices are regenerated on the host from the same seeds."""
     from gpudbmetalcodegen_b200 import workloads as W
     from oracle import oracle_py as O
     threads = os.cpu_count() or 1
-    md = W.gen_mixdim(args.mix_dim_rows, seed=W.SEED)
+    dim_rows = dim_rows or args.mix_dim_rows
+    zipf = zipf or W.MIX_ZIPF_S
+    seed = W.SEED if zipf is W.MIX_ZIPF_S else W.SEED + 5
+    md = W.gen_mixdim(dim_rows, seed=seed)
     done, spent = 0, 0.0
     for q in queries:
-        m = W.gen_mix(q.rows, nranks=W.MIX_NRANKS, s=W.MIX_ZIPF_S[q.table], dim_rows=args.mix_dim_rows,
-                      seed=W.SEED + 7919 * q.table, row0=q.row0)
+        m = W.gen_mix(q.rows, nranks=W.MIX_NRANKS, s=zipf[q.table], dim_rows=dim_rows,
+                      seed=seed + 7919 * q.table, row0=q.row0)
         t0 = time.perf_counter()
         if q.tmpl == "agg":
             O.mix_agg(m, q.thr, threads=threads)
@@ -446,7 +449,7 @@ def run_mixed(args):
         ev0.record(stream)
         w0 = time.perf_counter()
         for i in range(args.steps):
-            res, rep = learned.run(queries, copy=(i == args.steps - 1))
+            res, rep = learned.run(queries)
             reps.append(rep)
             launches += rep.launches + 2  # + the sample kernel and the predictor
         ev1.record(stream)
@@ -522,6 +525,105 @@ def run_mixed(args):
         pg.destroy_process_group()
 
 
+def run_serve(args):
+    """Config: a 120M-row table and a 30M-row dimension resident in HBM;
+    mixed queries (the mixed generator, slices of 1M-120M rows) arriving as
+    a Poisson process at each offered rate; the continuous-batching server
+    (learned sizing, HBM budget, two workers whose batches overlap) against
+    the plain one-query-at-a-time path on the same trace. Every served
+    answer is checked against the plain path's answer for the same query."""
+    import numpy as np
+    import torch
+    from gpudbmetalcodegen_b200 import Context, batch as B, serve as S, workloads as W
+
+    world, rank, local = dist_info()
+    if args.impl == "reference":
+        if rank == 0:
+            qs = W.gen_mixed_queries(args.serve_queries, seed=W.SEED + 5, table_rows=args.serve_rows, n_tables=1)
+            done, spent, threads = mixed_oracle_seconds(args, qs, budget_s=max(10.0, 2.0 * args.steps),
+                                                        dim_rows=args.serve_dim_rows, zipf=(W.ZIPF_S,))
+            v = done / spent
+            print(json.dumps({
+                "metric": "serve_queries_per_s", "value": v, "unit": "queries/s", "n_gpus": args.gpus, "steps": 1,
+                "warmup": 0, "ms_per_step": 1e3 * spent / done, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": "serve: mixed queries over a resident 120M-row table, one at a time"},
+                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": f"first {done} queries of the trace"},
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+                flush=True)
+        return
+    torch.cuda.set_device(local)
+    tables = B.MixTables(rows=args.serve_rows, zipf_s=(W.ZIPF_S,), nranks=W.MIX_NRANKS,
+                         dim_rows=args.serve_dim_rows, seed=W.SEED + 5)
+    log = B.ExecutionLog()
+    t0 = time.perf_counter()
+    B.log_executions(tables, W.gen_mixed_queries(args.train_executions, seed=W.SEED + 6,
+                                                 table_rows=args.serve_rows, n_tables=1), log, batch_size=1024)
+    sizer, sinfo = B.train_sizer(log, seed=1, epochs=args.sizer_epochs, batch=512, lr=3e-3)
+    sinfo["log_s"] = time.perf_counter() - t0
+    ctx = Context(local)
+    plain = B.PlainRunner(ctx, tables)
+    qs = W.gen_mixed_queries(args.serve_queries, seed=W.SEED + 5, table_rows=args.serve_rows, n_tables=1)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    # the plain path, each query alone: the first run of a query compiles its
+    # kernels (constants are part of the generated source), the second is
+    # timed with the kernel cache warm -- the service time of the queue
+    n_plain = min(args.serve_plain_queries, len(qs))
+    compile_s = []
+    for q in qs[:n_plain]:
+        t = time.perf_counter()
+        plain.run(q)
+        torch.cuda.synchronize()
+        compile_s.append(time.perf_counter() - t)
+    plain_res, _, service = S.serve_plain(plain, S.poisson_trace(qs[:n_plain], rate=rates[0], seed=11))
+    # every served answer is also checked against one exact-sized batch of all queries
+    ex = B.BatchRunner(tables, sizing="exact", plain=plain)
+    exact_res, _ = ex.run(qs)
+    ex.close()
+    srv = S.Server(tables, sizer, plain=plain, workers=args.serve_workers, hbm_budget=150e9)
+    srv.serve(S.poisson_trace(qs, rate=rates[-1], seed=12))  # warm the workers, their arenas and pools
+    per_rate, verified, clocks = [], True, None
+    launches = 0
+    for rate in rates:
+        trace = S.poisson_trace(qs, rate=rate, seed=11)
+        with ClockSampler(local) as clk:
+            res, rep = srv.serve(trace)
+        clocks = clk.summary()
+        ok_alone = all(B.same_result(a, b) for a, b in zip(res[:n_plain], plain_res))
+        ok_all = all(B.same_result(a, b) for a, b in zip(res, exact_res))
+        verified = verified and ok_alone and ok_all
+        _, prep, _ = S.serve_plain(plain, trace[:n_plain], service_s=service)
+        launches += 7 * rep.batches
+        per_rate.append({"offered_per_s": rate, "ours": rep.summary(),
+                         f"plain_one_at_a_time_first_{n_plain}": prep.summary(),
+                         "bit_exact_vs_alone": ok_alone, "bit_exact_vs_exact_batch": ok_all})
+    srv.close()
+    top = per_rate[-1]["ours"]
+    if rank == 0:
+        line = {"metric": "serve_queries_per_s", "value": top["queries_per_s"], "unit": "queries/s",
+                "n_gpus": world, "steps": len(rates), "warmup": 1, "ms_per_step": top["wall_s"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded)",
+                "config": {"workload": f"serve: {len(qs)} mixed queries per trace over a resident "
+                                       f"{args.serve_rows}-row table + {args.serve_dim_rows}-row dimension, Poisson "
+                                       f"arrivals, HBM budget 150 GB, {args.serve_workers} workers",
+                           "rates": rates, "parallelism": "replicas x1"},
+                "verified": verified, "per_rate": per_rate,
+                "plain_service_ms": {"warm_mean": float(service.mean() * 1e3),
+                                     "warm_p50": float(np.median(service) * 1e3),
+                                     "first_run_with_compile_mean": float(np.mean(compile_s) * 1e3),
+                                     "queries": n_plain},
+                "sizer": sinfo,
+                "e2e": {"value": top["queries_per_s"], "unit": "queries/s", "h2d_bytes_per_step": 128 * len(qs),
+                        "d2h_bytes_per_step": None,
+                        "note": "wall clock from first arrival to last answer on the host, at the highest offered rate"},
+                "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    sizer.close()
+    ctx.close()
+
+
 def load_traffic(kernel: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -539,7 +641,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="join_topk",
-                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed"])
+                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed", "serve"])
     ap.add_argument("--tune", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -555,10 +657,18 @@ def main():
     ap.add_argument("--train-executions", type=int, default=200_000)
     ap.add_argument("--sizer-epochs", type=int, default=30)
     ap.add_argument("--plain-passes", type=int, default=1)
+    ap.add_argument("--serve-rows", type=int, default=120_000_000)
+    ap.add_argument("--serve-dim-rows", type=int, default=30_000_000)
+    ap.add_argument("--serve-queries", type=int, default=1000)
+    ap.add_argument("--serve-rates", default="500,2000,8000")
+    ap.add_argument("--serve-workers", type=int, default=2)
+    ap.add_argument("--serve-plain-queries", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.workload == "mixed":
         return run_mixed(args)
+    if args.workload == "serve":
+        return run_serve(args)
     world, rank, local = dist_info()
     w = make_workload(args)
 

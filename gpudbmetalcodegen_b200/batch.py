@@ -20,7 +20,9 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import threading
 import time
+import weakref
 from dataclasses import dataclass, field, replace
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -30,6 +32,8 @@ from . import _lib
 from ._lib import check
 
 TEMPLATES = ("agg", "join", "groupby", "topk")
+AGG_AUTO, AGG_SHARED, AGG_GLOBAL_WARP, AGG_GLOBAL = 0, 1, 2, 3
+SHARED_MAX_GROUPS = 1024     # groups that fit the per-CTA shared table at load <= 1/2
 TPL = {name: i for i, name in enumerate(TEMPLATES)}
 DEVERR_HASH_OVERFLOW = 0x1
 SIZER_FEATURES = 16
@@ -44,7 +48,7 @@ class BatchQueryStruct(C.Structure):
                 ("value", C.c_void_p), ("fk", C.c_void_p), ("dim_key", C.c_void_p), ("dim_attr", C.c_void_p),
                 ("dim_rows", C.c_uint64), ("dim_max_key", C.c_int64), ("groups", C.c_uint64),
                 ("key_min", C.c_int64), ("key_max", C.c_int64), ("filter_min", C.c_int32),
-                ("filter_max", C.c_int32)]
+                ("filter_max", C.c_int32), ("agg_mode", C.c_int32)]
 
 
 @dataclass(frozen=True)
@@ -189,6 +193,66 @@ def query_bytes(q: MixQuery, dim_rows: int) -> int:
 
 
 # ---------------------------------------------------------------------------
+# pinned result buffers
+# ---------------------------------------------------------------------------
+class PinnedPool:
+    """Pinned host buffers handed out as numpy arrays that own them: when
+    the last view of a buffer is dropped it returns to the pool, so batch
+    results reach the caller without a host copy and the memory is reused."""
+
+    def __init__(self, alloc=None, free=None):
+        lib = None if alloc and free else _lib.load()
+        self._alloc = alloc or lib.gpudb_host_alloc
+        self._freefn = free or (lambda ptr: lib.gpudb_host_free(C.c_void_p(ptr)))
+        self._free: List[Tuple[int, int]] = []  # (bytes, ptr)
+        self._lock = threading.Lock()
+        self._closed = False
+
+    def array(self, nbytes: int) -> np.ndarray:
+        """An int64 array of at least `nbytes` bytes in pinned memory."""
+        nbytes = max(64, nbytes)
+        with self._lock:
+            best = None
+            for k, (cap, ptr) in enumerate(self._free):
+                if cap >= nbytes and (best is None or cap < self._free[best][0]):
+                    best = k
+            if best is not None:
+                cap, ptr = self._free.pop(best)
+            else:
+                cap = int(nbytes * 1.25) + 4096
+                ptr = self._alloc(cap)
+                if not ptr:
+                    raise MemoryError(f"pinned host buffer of {cap} bytes")
+        buf = (C.c_int64 * (cap // 8)).from_address(ptr)
+        weakref.finalize(buf, self._release, cap, ptr)
+        return np.ctypeslib.as_array(buf)
+
+    def _release(self, cap: int, ptr: int) -> None:
+        with self._lock:
+            if self._closed:
+                self._freefn(ptr)
+            else:
+                self._free.append((cap, ptr))
+
+    def close(self) -> None:
+        with self._lock:
+            self._closed = True
+            for _, ptr in self._free:
+                self._freefn(ptr)
+            self._free.clear()
+
+
+_POOL: Optional[PinnedPool] = None
+
+
+def pinned_pool() -> PinnedPool:
+    global _POOL
+    if _POOL is None:
+        _POOL = PinnedPool()
+    return _POOL
+
+
+# ---------------------------------------------------------------------------
 # the C batch object
 # ---------------------------------------------------------------------------
 class Batch:
@@ -200,13 +264,11 @@ class Batch:
         check(self._lib.gpudb_batch_create(None, C.byref(h)))
         self.handle = h
         self.n = 0
-        self._pinned, self._pinned_bytes = None, 0
 
     def close(self) -> None:
         if self.handle:
             self._lib.gpudb_batch_free(self.handle)
             self.handle = None
-        self._free_pinned()
 
     def __del__(self):
         try:
@@ -222,6 +284,9 @@ class Batch:
 
     def set_groups(self, i: int, groups: int) -> None:
         check(self._lib.gpudb_batch_set_groups(self.handle, i, int(groups)))
+
+    def set_agg_mode(self, i: int, mode: int) -> None:
+        check(self._lib.gpudb_batch_set_agg_mode(self.handle, i, int(mode)))
 
     def set_tuning(self, block: int = 512, tile_rows: int = 16384, warp_aggregate: bool = True,
                    max_probe: int = 128) -> None:
@@ -248,28 +313,16 @@ class Batch:
 
     def collect(self) -> Tuple[np.ndarray, np.ndarray, float]:
         """(rows per query, packed int64 rows [total, 3], device+copy ms).
-        The packed rows live in a pinned buffer that the next collect reuses."""
+        The packed rows are copied once, by the device, into a pinned buffer
+        that the returned array owns (see PinnedPool)."""
         rows = np.zeros(max(1, self.n), dtype=np.uint64)
         need = C.c_uint64()
         ms = C.c_double()
         check(self._lib.gpudb_batch_collect(self.handle, rows.ctypes.data, None, 0, C.byref(need), None))
-        nbytes = max(24, need.value)
-        if nbytes > self._pinned_bytes:
-            self._free_pinned()
-            cap = int(nbytes * 1.25) + 4096
-            ptr = self._lib.gpudb_host_alloc(cap)
-            if not ptr:
-                raise MemoryError(f"pinned host buffer of {cap} bytes")
-            self._pinned, self._pinned_bytes = ptr, cap
-        check(self._lib.gpudb_batch_collect(self.handle, None, self._pinned, self._pinned_bytes,
-                                            C.byref(need), C.byref(ms)))
-        view = np.ctypeslib.as_array((C.c_int64 * (self._pinned_bytes // 8)).from_address(self._pinned))
-        return rows[:self.n], view[:need.value // 8].reshape(-1, 3), ms.value
-
-    def _free_pinned(self) -> None:
-        if self._pinned:
-            self._lib.gpudb_host_free(self._pinned)
-        self._pinned, self._pinned_bytes = None, 0
+        host = pinned_pool().array(need.value)
+        check(self._lib.gpudb_batch_collect(self.handle, None, host.ctypes.data, host.nbytes, C.byref(need),
+                                            C.byref(ms)))
+        return rows[:self.n], host[:need.value // 8].reshape(-1, 3), ms.value
 
     def result_scalar(self, i: int) -> Tuple[int, int]:
         c, lo, hi = C.c_int64(), C.c_uint64(), C.c_int64()
@@ -304,9 +357,10 @@ class Batch:
 
 
 def unpack_results(queries: Sequence[MixQuery], rows: np.ndarray, packed: np.ndarray,
-                   copy: bool = True) -> List[tuple]:
+                   copy: bool = False) -> List[tuple]:
     """Results from gpudb_batch_collect's packed rows (group-by rows as
-    "groups_raw" blocks; views into `packed` unless `copy`)."""
+    "groups_raw" blocks: views into `packed`, which they keep alive, unless
+    `copy`)."""
     if copy:
         packed = packed.copy()
     out = []
@@ -338,6 +392,7 @@ class Sizer:
         check(self._lib.gpudb_sizer_create(device, seed, C.byref(h)))
         self.handle = h
         self.nparams = int(self._lib.gpudb_sizer_param_count())
+        self._lock = threading.Lock()  # one device workspace: calls from threads take turns
 
     def close(self) -> None:
         if self.handle:
@@ -353,22 +408,25 @@ class Sizer:
     @property
     def params(self) -> np.ndarray:
         p = np.zeros(self.nparams, dtype=np.float32)
-        check(self._lib.gpudb_sizer_get_params(self.handle, p.ctypes.data))
+        with self._lock:
+            check(self._lib.gpudb_sizer_get_params(self.handle, p.ctypes.data))
         return p
 
     @params.setter
     def params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, dtype=np.float32)
         assert p.shape == (self.nparams,)
-        check(self._lib.gpudb_sizer_set_params(self.handle, p.ctypes.data))
+        with self._lock:
+            check(self._lib.gpudb_sizer_set_params(self.handle, p.ctypes.data))
 
     def grads(self, X: np.ndarray, Y: np.ndarray) -> Tuple[np.ndarray, float]:
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.ascontiguousarray(Y, dtype=np.float32)
         g = np.zeros(self.nparams, dtype=np.float32)
         loss = C.c_float()
-        check(self._lib.gpudb_sizer_grads(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], g.ctypes.data,
-                                          C.byref(loss)))
+        with self._lock:
+            check(self._lib.gpudb_sizer_grads(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], g.ctypes.data,
+                                              C.byref(loss)))
         return g, loss.value
 
     def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 20, batch: int = 256, lr: float = 2e-3,
@@ -376,15 +434,17 @@ class Sizer:
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.ascontiguousarray(Y, dtype=np.float32)
         loss = C.c_float()
-        check(self._lib.gpudb_sizer_train(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], epochs, batch,
-                                          lr, seed, C.byref(loss)))
+        with self._lock:
+            check(self._lib.gpudb_sizer_train(self.handle, X.ctypes.data, Y.ctypes.data, X.shape[0], epochs, batch,
+                                              lr, seed, C.byref(loss)))
         return loss.value
 
     def predict(self, X: np.ndarray) -> np.ndarray:
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.zeros((X.shape[0], SIZER_OUTPUTS), dtype=np.float32)
         if X.shape[0]:
-            check(self._lib.gpudb_sizer_predict(self.handle, X.ctypes.data, X.shape[0], Y.ctypes.data))
+            with self._lock:
+                check(self._lib.gpudb_sizer_predict(self.handle, X.ctypes.data, X.shape[0], Y.ctypes.data))
         return Y
 
     def save(self, path) -> None:
@@ -409,6 +469,20 @@ def groups_from_prediction(q: MixQuery, y0: float, margin: float) -> int:
     g = (2.0 ** (float(y0) * CARD_SCALE) - 1.0) * margin
     bound = max(1, min(q.card, q.rows))
     return int(min(bound, max(1, math.ceil(g))))
+
+
+SKEW_SHARE = 0.004           # sample share of the most frequent key that counts as skew
+
+
+def agg_mode_for(groups: int, features: Optional[np.ndarray]) -> int:
+    """Aggregation strategy of a group-by from its expected group count and
+    the 4096-row sample (measured on B200, 60M rows: shared memory wins for
+    up to ~1K groups and for skewed keys at any cardinality, where hot keys
+    would serialise global atomics; the global table wins 2-3x for
+    unskewed keys beyond a few thousand groups)."""
+    if groups <= SHARED_MAX_GROUPS or features is None:
+        return AGG_SHARED
+    return AGG_SHARED if features[12] >= SKEW_SHARE else AGG_GLOBAL
 
 
 def sample_estimate(features: np.ndarray) -> np.ndarray:
@@ -484,6 +558,7 @@ class PlainRunner:
         for c, t in tables.dim.items():
             ctx.register_column("mixdim", c, t.data_ptr(), t.numel(), t.element_size())
         self.count_passes = 0
+        self._lock = threading.Lock()  # one engine context: queries from threads take turns
 
     def _register_slice(self, q: MixQuery) -> None:
         cols = ["m_filter", "m_value"] + (["m_fk"] if q.tmpl == "join" else []) + ([q.key] if q.grouped else [])
@@ -498,6 +573,10 @@ class PlainRunner:
         return int(res.rows[0][0])
 
     def run(self, q: MixQuery) -> tuple:
+        with self._lock:
+            return self._run(q)
+
+    def _run(self, q: MixQuery) -> tuple:
         self._register_slice(q)
         spec = f"template={self.SPEC[q.tmpl]};thr={q.thr}"
         if q.tmpl == "join":
@@ -544,16 +623,17 @@ class BatchRunner:
 
     def __init__(self, tables: MixTables, sizing: str = "learned", sizer: Optional[Sizer] = None,
                  plain: Optional[PlainRunner] = None, margin: float = 1.5, use_graph: bool = True,
-                 tuning: Optional[dict] = None):
+                 tuning: Optional[dict] = None, agg_mode: Optional[int] = None):
         if sizing == "learned" and sizer is None:
             raise ValueError("learned sizing needs a trained Sizer")
         self.tables, self.sizing, self.sizer, self.plain = tables, sizing, sizer, plain
-        self.margin, self.use_graph = margin, use_graph
+        self.margin, self.use_graph, self.agg_mode = margin, use_graph, agg_mode
         self.batch = Batch()
         if tuning:
             self.batch.set_tuning(**tuning)
         self._key = None
         self._groups = None
+        self._features = None
 
     def close(self) -> None:
         self.batch.close()
@@ -562,6 +642,7 @@ class BatchRunner:
         b = self.batch
         if self.sizing == "learned":
             X, report.features_ms = b.features()
+            self._features = X
             t = time.perf_counter()
             Y = self.sizer.predict(X)
             report.predict_ms = 1e3 * (time.perf_counter() - t)
@@ -574,10 +655,10 @@ class BatchRunner:
             return [max(1, min(q.card, q.rows)) if q.grouped else 1 for q in queries]
         raise ValueError(f"unknown sizing '{self.sizing}'")
 
-    def run(self, queries: Sequence[MixQuery], copy: bool = True) -> Tuple[List[tuple], BatchReport]:
-        """Results of group-by queries are "groups_raw" blocks; with
-        copy=False they are views of a pinned buffer that the next run on
-        this runner overwrites."""
+    def run(self, queries: Sequence[MixQuery], copy: bool = False) -> Tuple[List[tuple], BatchReport]:
+        """Results of group-by queries are "groups_raw" blocks: views of the
+        pinned buffer the device wrote them into (it returns to the pool once
+        no view is left), or private copies with copy=True."""
         t0 = time.perf_counter()
         report = BatchReport(self.sizing, len(queries))
         key = tuple(queries)
@@ -585,11 +666,16 @@ class BatchRunner:
         if key != self._key:
             b.set_queries([self.tables.query_struct(q) for q in queries])
             self._key, self._groups = key, None
+        self._features = None
         groups = self.size(queries, report)
-        if groups != self._groups:
-            for i, g in enumerate(groups):
+        modes = [(self.agg_mode if self.agg_mode is not None else
+                  agg_mode_for(g, None if self._features is None else self._features[i])) if q.grouped else AGG_AUTO
+                 for i, (g, q) in enumerate(zip(groups, queries))]
+        if (groups, modes) != self._groups:
+            for i, (g, m) in enumerate(zip(groups, modes)):
                 b.set_groups(i, g)
-            self._groups = groups
+                b.set_agg_mode(i, m)
+            self._groups = (groups, modes)
         report.table_slots = sum(1 << max(4, math.ceil(math.log2(2 * g))) for g, q in zip(groups, queries)
                                  if q.grouped)
         report.execute_ms, err = b.execute(self.use_graph)

@@ -71,6 +71,7 @@ struct QDesc {
     unsigned* bitmap;
     Slot* ht;
     int log2cap, maxProbe;
+    int aggMode;  // GPUDB_AGG_SHARED / GPUDB_AGG_GLOBAL_WARP / GPUDB_AGG_GLOBAL
     unsigned* slots;
     long long* tk_part;  // [tk_chunks][kTopK] of (value, key)
     long long tk_chunks;
@@ -153,12 +154,12 @@ __device__ __forceinline__ void blockAdd2(long long c, long long s, unsigned lon
     }
 }
 
-__device__ __forceinline__ long long slotFor(Slot* ht, int log2cap, unsigned enc, unsigned maxProbe, unsigned* err,
-                                             bool* fresh) {
+// Linear probing from slot `s`, whose key word `cur` is already loaded.
+__device__ __forceinline__ long long slotFrom(Slot* ht, int log2cap, unsigned enc, unsigned long long s, unsigned cur,
+                                              unsigned maxProbe, unsigned* err, bool* fresh) {
     const unsigned long long mask = (1ull << log2cap) - 1ull;
-    unsigned long long s = gpudb_hash_slot((unsigned long long)enc, log2cap);
     for (unsigned p = 0; p < maxProbe; ++p) {
-        const unsigned cur = *((volatile unsigned*)&ht[s].key);
+        if (p) cur = *((volatile unsigned*)&ht[s].key);
         if (cur == enc) return (long long)s;
         if (cur == 0u) {
             const unsigned prev = atomicCAS(&ht[s].key, 0u, enc);
@@ -174,14 +175,15 @@ __device__ __forceinline__ long long slotFor(Slot* ht, int log2cap, unsigned enc
     return -1;
 }
 
-// Add (count, sum) to a group of the query's global table; a group created
-// here is appended to the slot list (one atomic per warp for the positions).
-__device__ __forceinline__ void globalAdd(const QDesc& q, bool live, unsigned enc, unsigned long long c,
-                                          unsigned long long v) {
+// Add (count, sum) to a group of the query's global table, starting from
+// home slot `s0` whose key word `cur` is loaded; a group created here is
+// appended to the slot list (one atomic per warp for the positions).
+__device__ __forceinline__ void globalAddFrom(const QDesc& q, bool live, unsigned enc, unsigned long long s0,
+                                              unsigned cur, unsigned long long c, unsigned long long v) {
     bool fresh = false;
     long long slot = -1;
     if (live) {
-        slot = slotFor(q.ht, q.log2cap, enc, (unsigned)q.maxProbe, q.err, &fresh);
+        slot = slotFrom(q.ht, q.log2cap, enc, s0, cur, (unsigned)q.maxProbe, q.err, &fresh);
         if (slot >= 0) {
             atomicAdd(&q.ht[slot].count, (unsigned)c);
             atomicAdd(&q.ht[slot].sum, v);
@@ -189,6 +191,13 @@ __device__ __forceinline__ void globalAdd(const QDesc& q, bool live, unsigned en
     }
     const unsigned long long pos = gpudb_warp_reserve(q.nslots, fresh);
     if (fresh) q.slots[pos] = (unsigned)slot;
+}
+
+__device__ __forceinline__ void globalAdd(const QDesc& q, bool live, unsigned enc, unsigned long long c,
+                                          unsigned long long v) {
+    const unsigned long long s0 = gpudb_hash_slot((unsigned long long)enc, q.log2cap);
+    const unsigned cur = live ? *((volatile unsigned*)&q.ht[s0].key) : 0u;
+    globalAddFrom(q, live, enc, s0, cur, c, v);
 }
 
 // ---- JOIN build: bitmap of dim keys with attr < attr_lt -------------------
@@ -265,8 +274,17 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
 }
 
 // ---- GROUPBY / TOPK: filter -> key % card -> hash table (count, sum) -------
+// Per query, the strategy the host picked from the expected group count and
+// the sample's key repetition:
+//   SHARED      warp aggregation, then the CTA's shared-memory table (flushed
+//               to the global table at the end of the work item);
+//   GLOBAL_WARP warp aggregation, then the global table;
+//   GLOBAL      the global table directly.
+// On the global path the home-slot key words of a thread's kUnroll rows are
+// loaded together, so an existing group costs one L2 round trip per
+// kUnroll rows, then fire-and-forget atomics.
 __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
-                                               unsigned long long* counter, int warpAgg) {
+                                               unsigned long long* counter) {
     __shared__ long long s_item;
     __shared__ unsigned sKey[kSmemSlots];
     __shared__ unsigned sCnt[kSmemSlots];
@@ -286,6 +304,9 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const long long* __restrict__ value = q.value;
         const int thr = q.thr;
         const long long card = q.card;
+        const int mode = q.aggMode;
+        Slot* ht = q.ht;
+        const int log2cap = q.log2cap;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
         for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
@@ -299,44 +320,77 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
                 v[u] = p ? __ldcs(value + b + u * step) : 0;
             }
+            unsigned enc[kUnroll];
+            bool live[kUnroll];
+            unsigned long long c[kUnroll], val[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
-                if (f[u] >= thr) continue;
-                const unsigned enc = encKey(keyMod(kr[u], q), card);
-                unsigned long long c = 1, val = (unsigned long long)v[u];
-                if (warpAgg) {
+                live[u] = f[u] < thr;
+                enc[u] = live[u] ? encKey(keyMod(kr[u], q), card) : 0u;
+                c[u] = 1ull;
+                val[u] = (unsigned long long)v[u];
+            }
+            if (mode != GPUDB_AGG_GLOBAL) {
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    if (!live[u]) continue;
                     const unsigned am = __activemask();
-                    const unsigned peers = __match_any_sync(am, enc);
-                    c = gpudb_peer_sum(am, peers, c);
-                    val = gpudb_peer_sum(am, peers, val);
-                    if ((int)(threadIdx.x & 31u) != __ffs(peers) - 1) continue;
+                    const unsigned peers = __match_any_sync(am, enc[u]);
+                    c[u] = gpudb_peer_sum(am, peers, c[u]);
+                    val[u] = gpudb_peer_sum(am, peers, val[u]);
+                    live[u] = (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
                 }
-                // shared-memory table first
-                unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc, 11);
-                bool done = false;
+            }
+            if (mode == GPUDB_AGG_SHARED) {
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    if (!live[u]) continue;
+                    unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], 11);
+                    bool done = false;
 #pragma unroll 1
-                for (int p = 0; p < kSmemProbe; ++p) {
-                    unsigned cur = vKey[h];
-                    if (cur == 0u) cur = atomicCAS(&sKey[h], 0u, enc) == 0u ? enc : vKey[h];
-                    if (cur == enc) {
-                        atomicAdd(&sCnt[h], (unsigned)c);
-                        atomicAdd(&sSum[h], val);
-                        done = true;
-                        break;
+                    for (int p = 0; p < kSmemProbe; ++p) {
+                        unsigned cur = vKey[h];
+                        if (cur == 0u) cur = atomicCAS(&sKey[h], 0u, enc[u]) == 0u ? enc[u] : vKey[h];
+                        if (cur == enc[u]) {
+                            atomicAdd(&sCnt[h], (unsigned)c[u]);
+                            atomicAdd(&sSum[h], val[u]);
+                            done = true;
+                            break;
+                        }
+                        h = (h + 1u) & (kSmemSlots - 1);
                     }
-                    h = (h + 1u) & (kSmemSlots - 1);
+                    if (!done) globalAdd(q, true, enc[u], c[u], val[u]);
                 }
-                if (!done) globalAdd(q, true, enc, c, val);
+            } else {
+                unsigned long long s0[kUnroll];
+                unsigned cur[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    s0[u] = gpudb_hash_slot((unsigned long long)enc[u], log2cap);
+                    cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
+                        atomicAdd(&ht[s0[u]].count, (unsigned)c[u]);
+                        atomicAdd(&ht[s0[u]].sum, val[u]);
+                        live[u] = false;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
             }
         }
-        __syncthreads();
-        // flush the shared table into the query's global table
-        for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
-            const unsigned k = sKey[i];
-            globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
-            sKey[i] = 0u;
-            sCnt[i] = 0u;
-            sSum[i] = 0ull;
+        if (mode == GPUDB_AGG_SHARED) {
+            __syncthreads();
+            // flush the shared table into the query's global table
+            for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
+                const unsigned k = sKey[i];
+                globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
+                sKey[i] = 0u;
+                sCnt[i] = 0u;
+                sSum[i] = 0ull;
+            }
         }
     }
 }
@@ -472,15 +526,25 @@ __global__ void __launch_bounds__(1024) kStats(const QDesc* __restrict__ qs, Wor
 }
 
 // ---- 4096-row feature sample: one CTA per query ----------------------------
+// Evenly spaced rows of the slice: rows sampled, rows passing the filter,
+// distinct group keys among them and the multiplicity of the most frequent
+// key (the skew signal that picks the aggregation strategy).
 constexpr int kSample = 4096, kSampleSlots = 8192;
-__global__ void kSampleStats(const QDesc* __restrict__ qs, unsigned long long* out /* [n][3] */) {
+constexpr int kSampleSmem = kSampleSlots * (8 + 4);
+__global__ void kSampleStats(const QDesc* __restrict__ qs, unsigned long long* out /* [n][4] */) {
     extern __shared__ unsigned long long setKeys[];
+    unsigned* setCnt = reinterpret_cast<unsigned*>(setKeys + kSampleSlots);
     __shared__ unsigned long long s_pass, s_distinct;
+    __shared__ unsigned s_top;
     const QDesc& q = qs[blockIdx.x];
-    for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) setKeys[i] = GPUDB_EMPTY64;
+    for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) {
+        setKeys[i] = GPUDB_EMPTY64;
+        setCnt[i] = 0u;
+    }
     if (threadIdx.x == 0) {
         s_pass = 0;
         s_distinct = 0;
+        s_top = 0;
     }
     __syncthreads();
     const long long m = q.rows < kSample ? q.rows : kSample;
@@ -494,23 +558,30 @@ __global__ void kSampleStats(const QDesc* __restrict__ qs, unsigned long long* o
         unsigned h = (unsigned)gpudb_hash_slot(k, 13);
         for (int p = 0; p < kSampleSlots; ++p) {
             const unsigned long long cur = setKeys[h];
-            if (cur == k) break;
+            bool mine = cur == k;
             if (cur == GPUDB_EMPTY64) {
                 const unsigned long long prev = atomicCAS(setKeys + h, GPUDB_EMPTY64, k);
-                if (prev == GPUDB_EMPTY64) {
-                    atomicAdd(&s_distinct, 1ull);
-                    break;
-                }
-                if (prev == k) break;
+                if (prev == GPUDB_EMPTY64) atomicAdd(&s_distinct, 1ull);
+                mine = prev == GPUDB_EMPTY64 || prev == k;
+            }
+            if (mine) {
+                atomicAdd(setCnt + h, 1u);
+                break;
             }
             h = (h + 1) & (kSampleSlots - 1);
         }
     }
     __syncthreads();
+    unsigned top = 0;
+    for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) top = max(top, setCnt[i]);
+    for (int o = 16; o > 0; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&s_top, top);
+    __syncthreads();
     if (threadIdx.x == 0) {
-        out[3 * blockIdx.x] = (unsigned long long)m;
-        out[3 * blockIdx.x + 1] = s_pass;
-        out[3 * blockIdx.x + 2] = s_distinct;
+        out[4 * blockIdx.x] = (unsigned long long)m;
+        out[4 * blockIdx.x + 1] = s_pass;
+        out[4 * blockIdx.x + 2] = s_distinct;
+        out[4 * blockIdx.x + 3] = s_top;
     }
 }
 
@@ -605,18 +676,22 @@ bool grouped(int tmpl) { return tmpl == GPUDB_TPL_GROUPBY || tmpl == GPUDB_TPL_T
         }                                                                                          \
     } while (0)
 
+// Grow-only device buffer from the stream-ordered pool allocator: growing
+// it never synchronises the device (cudaFree would), so batches of other
+// streams keep running while this one resizes; 25 % headroom on growth.
 struct DeviceBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    int reserve(size_t want) {
+    int reserve(size_t want, cudaStream_t st) {
         if (want <= bytes) return GPUDB_OK;
-        release();
-        B_CHECK(cudaMalloc(&p, want), GPUDB_E_ALLOC);
-        bytes = want;
+        release(st);
+        const size_t cap = want + want / 4 + 256;
+        B_CHECK(cudaMallocAsync(&p, cap, st), GPUDB_E_ALLOC);
+        bytes = cap;
         return GPUDB_OK;
     }
-    void release() {
-        if (p) cudaFree(p);
+    void release(cudaStream_t st) {
+        if (p) cudaFreeAsync(p, st);
         p = nullptr;
         bytes = 0;
     }
@@ -692,8 +767,8 @@ int plan(gpudb_batch* b) {
         }
         z = al256(z);
     }
-    if (int st = b->arena.reserve(z)) return st;
-    if (int st = b->scratch.reserve(std::max<size_t>(sc, 256))) return st;
+    if (int st = b->arena.reserve(z, b->stream)) return st;
+    if (int st = b->scratch.reserve(std::max<size_t>(sc, 256), b->stream)) return st;
     b->zeroBytes = z;
     char* zb = static_cast<char*>(b->arena.p);
     char* sb = static_cast<char*>(b->scratch.p);
@@ -719,6 +794,10 @@ int plan(gpudb_batch* b) {
         d.dim_attr = q.dim_attr;
         d.dim_rows = (long long)q.dim_rows;
         d.maxProbe = b->maxProbe;
+        // aggregation strategy: the caller's choice, else the shared-memory
+        // table (with spill to the global one), which is never far off
+        d.aggMode = q.agg_mode != GPUDB_AGG_AUTO ? q.agg_mode : GPUDB_AGG_SHARED;
+        if (!b->warpAgg && d.aggMode == GPUDB_AGG_GLOBAL_WARP) d.aggMode = GPUDB_AGG_GLOBAL;
         char* p = zb + zOff[i];
         d.agg = reinterpret_cast<unsigned long long*>(p);
         d.topk_n = d.agg + 3;
@@ -781,7 +860,7 @@ int plan(gpudb_batch* b) {
     };
     const auto oB = putList(lBuild, pBuild), oA = putList(lAgg, pAgg), oG = putList(lGroup, pGroup),
                oT = putList(lTopk, pTopk), oS = putList(lAll, pAll), oC = putList(lCollect, pCollect);
-    if (int st = b->meta.reserve(host.size())) return st;
+    if (int st = b->meta.reserve(host.size(), b->stream)) return st;
     B_CHECK(cudaMemcpyAsync(b->meta.p, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream), GPUDB_E_CUDA);
     char* m = static_cast<char*>(b->meta.p);
     auto wl = [&](std::pair<size_t, size_t> o, size_t nq) {
@@ -800,8 +879,9 @@ int plan(gpudb_batch* b) {
         if (b->errHost) cudaFreeHost(b->errHost);
         b->errHost = nullptr;
         b->errCap = 0;
-        B_CHECK(cudaHostAlloc((void**)&b->errHost, sizeof(unsigned) * n, cudaHostAllocDefault), GPUDB_E_ALLOC);
-        b->errCap = n;
+        const size_t cap = std::max<size_t>(4096, 2 * (size_t)n);
+        B_CHECK(cudaHostAlloc((void**)&b->errHost, sizeof(unsigned) * cap, cudaHostAllocDefault), GPUDB_E_ALLOC);
+        b->errCap = cap;
     }
     B_CHECK(cudaStreamSynchronize(b->stream), GPUDB_E_CUDA);
     dropGraph(b);
@@ -838,7 +918,7 @@ int enqueue(gpudb_batch* b, bool stages) {
     mark(3);
     if (b->wlGroup.nq) {
         kGroup<<<gridFor(b, (const void*)kGroup, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlGroup, b->tile,
-                                                                                      b->counters + 2, b->warpAgg);
+                                                                                      b->counters + 2);
         launches++;
     }
     mark(4);
@@ -884,8 +964,7 @@ int gpudb_batch_create(gpudb_ctx* ctx, gpudb_batch** out) {
     B_CHECK(cudaEventCreate(&b->ev0), GPUDB_E_CUDA);
     B_CHECK(cudaEventCreate(&b->ev1), GPUDB_E_CUDA);
     for (auto& e : b->evStage) B_CHECK(cudaEventCreate(&e), GPUDB_E_CUDA);
-    B_CHECK(cudaFuncSetAttribute(kSampleStats, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(kSampleSlots * sizeof(unsigned long long))),
+    B_CHECK(cudaFuncSetAttribute(kSampleStats, cudaFuncAttributeMaxDynamicSharedMemorySize, kSampleSmem),
             GPUDB_E_LAUNCH);
     *out = b.release();
     return GPUDB_OK;
@@ -896,7 +975,8 @@ void gpudb_batch_free(gpudb_batch* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     dropGraph(b);
-    for (DeviceBuf* d : {&b->arena, &b->scratch, &b->meta, &b->stats, &b->sample, &b->collect}) d->release();
+    for (DeviceBuf* d : {&b->arena, &b->scratch, &b->meta, &b->stats, &b->sample, &b->collect}) d->release(b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->errHost) cudaFreeHost(b->errHost);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -923,6 +1003,10 @@ int gpudb_batch_set_queries(gpudb_batch* b, const gpudb_batch_query* q, int n) {
             gpudb::setThreadError(who + " asks for more than 2^30 groups");
             return GPUDB_E_INVALID;
         }
+        if (x.agg_mode < GPUDB_AGG_AUTO || x.agg_mode > GPUDB_AGG_GLOBAL) {
+            gpudb::setThreadError(who + " has an unknown agg_mode");
+            return GPUDB_E_INVALID;
+        }
         if (x.tmpl == GPUDB_TPL_TOPK && (x.k < 1 || x.k > kTopK)) {
             gpudb::setThreadError(who + " needs 1 <= k <= 16");
             return GPUDB_E_INVALID;
@@ -943,6 +1027,16 @@ int gpudb_batch_set_groups(gpudb_batch* b, int qi, uint64_t groups) {
     if (!b || qi < 0 || qi >= (int)b->queries.size() || groups > (1ull << 30)) return GPUDB_E_INVALID;
     if (b->queries[qi].groups != groups) {
         b->queries[qi].groups = groups;
+        b->dirty = true;
+    }
+    return GPUDB_OK;
+}
+
+int gpudb_batch_set_agg_mode(gpudb_batch* b, int qi, int mode) {
+    if (!b || qi < 0 || qi >= (int)b->queries.size() || mode < GPUDB_AGG_AUTO || mode > GPUDB_AGG_GLOBAL)
+        return GPUDB_E_INVALID;
+    if (b->queries[qi].agg_mode != mode) {
+        b->queries[qi].agg_mode = mode;
         b->dirty = true;
     }
     return GPUDB_OK;
@@ -1011,7 +1105,7 @@ int gpudb_batch_exact_stats(gpudb_batch* b, uint64_t* passing, uint64_t* distinc
     for (const auto& q : b->queries)
         if (grouped(q.tmpl)) words += (size_t)q.card / 32 + 1;
     const size_t bytes = 8 + 16 * (size_t)n + 4 * words;
-    if (int st = b->stats.reserve(bytes)) return st;
+    if (int st = b->stats.reserve(bytes, b->stream)) return st;
     unsigned long long* counter = static_cast<unsigned long long*>(b->stats.p);
     unsigned long long* pass = counter + 1;
     unsigned long long* dist = pass + n;
@@ -1056,19 +1150,20 @@ int gpudb_batch_features(gpudb_batch* b, float* f, double* ms) {
         if (int st = plan(b)) return st;
     const int n = (int)b->queries.size();
     if (n == 0) return GPUDB_OK;
-    if (int st = b->sample.reserve(24 * (size_t)n)) return st;
+    if (int st = b->sample.reserve(32 * (size_t)n, b->stream)) return st;
     unsigned long long* out = static_cast<unsigned long long*>(b->sample.p);
     B_CHECK(cudaEventRecord(b->ev0, b->stream), GPUDB_E_CUDA);
-    kSampleStats<<<n, 256, kSampleSlots * sizeof(unsigned long long), b->stream>>>(b->dDesc, out);
+    kSampleStats<<<n, 256, kSampleSmem, b->stream>>>(b->dDesc, out);
     B_CHECK(cudaGetLastError(), GPUDB_E_LAUNCH);
     B_CHECK(cudaEventRecord(b->ev1, b->stream), GPUDB_E_CUDA);
-    std::vector<unsigned long long> h(3 * (size_t)n);
-    B_CHECK(cudaMemcpyAsync(h.data(), out, 24 * (size_t)n, cudaMemcpyDeviceToHost, b->stream), GPUDB_E_CUDA);
+    std::vector<unsigned long long> h(4 * (size_t)n);
+    B_CHECK(cudaMemcpyAsync(h.data(), out, 32 * (size_t)n, cudaMemcpyDeviceToHost, b->stream), GPUDB_E_CUDA);
     B_CHECK(cudaStreamSynchronize(b->stream), GPUDB_E_CUDA);
     if (ms) *ms = elapsed(b);
     for (int i = 0; i < n; i++) {
         const auto& q = b->queries[i];
-        const double m = (double)h[3 * i], pass = (double)h[3 * i + 1], dist = (double)h[3 * i + 2];
+        const double m = (double)h[4 * i], pass = (double)h[4 * i + 1], dist = (double)h[4 * i + 2],
+                     top = (double)h[4 * i + 3];
         const double rows = (double)q.rows;
         // key domain under the modulus, from the key column's min / max
         const double span = (double)q.key_max - (double)q.key_min + 1.0;
@@ -1091,7 +1186,7 @@ int gpudb_batch_features(gpudb_batch* b, float* f, double* ms) {
         x[9] = (float)(std::log2(dist + 1.0) / 12.0);              // sample distinct count
         x[10] = (float)(std::log2(expPass + 1.0) / 27.0);          // estimated passing rows
         x[11] = (float)(std::log2((expPass + 1.0) / card) / 30.0);
-        x[12] = (float)(m / 4096.0);                               // sample size
+        x[12] = (float)(pass > 0 ? top / pass : 0.0);              // share of the most frequent sample key
         x[13] = (float)(std::log2(pass + 1.0) / 12.0);             // sample passing count
         x[14] = (float)(std::log2(uniformDistinct + 1.0) / 24.0);  // uniform-key estimate of the groups
         x[15] = 1.0f;
@@ -1121,7 +1216,7 @@ int gpudb_batch_collect(gpudb_batch* b, uint64_t* rows, void* host, uint64_t hos
                    : q.tmpl == GPUDB_TPL_TOPK  ? (size_t)kTopK
                                                : 1;
     }
-    if (int st = b->collect.reserve(head + 24 * maxRows)) return st;
+    if (int st = b->collect.reserve(head + 24 * maxRows, b->stream)) return st;
     unsigned long long* dRows = static_cast<unsigned long long*>(b->collect.p);
     unsigned long long* dOffs = dRows + n;
     unsigned long long* counter = dOffs + n + 1;

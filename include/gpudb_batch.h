@@ -76,17 +76,25 @@ typedef struct {
     /* column statistics (zone-map min / max of the slice's table), features only */
     int64_t key_min, key_max;
     int32_t filter_min, filter_max;
+    int32_t agg_mode;     /* GROUPBY / TOPK aggregation strategy, GPUDB_AGG_*     */
 } gpudb_batch_query;
+
+#define GPUDB_AGG_AUTO 0         /* SHARED                                           */
+#define GPUDB_AGG_SHARED 1       /* warp + per-CTA shared-memory table, flushed       */
+#define GPUDB_AGG_GLOBAL_WARP 2  /* warp aggregation, then the global table          */
+#define GPUDB_AGG_GLOBAL 3       /* the global table directly (mostly distinct keys) */
 
 int gpudb_batch_create(gpudb_ctx* ctx, gpudb_batch** out);
 void gpudb_batch_free(gpudb_batch* b);
 /* Describe the batch; allocates / reuses one device arena for every
  * query's outputs and hash tables. */
 int gpudb_batch_set_queries(gpudb_batch* b, const gpudb_batch_query* q, int n);
-/* Change one query's table sizing (before the next execute). */
+/* Change one query's table sizing / aggregation strategy (before the next
+ * execute). */
 int gpudb_batch_set_groups(gpudb_batch* b, int q, uint64_t groups);
+int gpudb_batch_set_agg_mode(gpudb_batch* b, int q, int agg_mode);
 /* Tuning of the persistent kernels: block size, rows per work item, warp
- * aggregation, hash probe bound. */
+ * aggregation (0 turns GLOBAL_WARP into GLOBAL), hash probe bound. */
 int gpudb_batch_set_tuning(gpudb_batch* b, int block, int tile_rows, int warp_aggregate, int max_probe);
 /* Run every query; per-query device error words go to errors[n] (bit
  * GPUDB_DEVERR_HASH_OVERFLOW = the table was undersized). With use_graph the

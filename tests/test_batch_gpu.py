@@ -91,6 +91,16 @@ def test_batch_tunings_and_bound_sizing(tables, tuning):
     r.close()
 
 
+@pytest.mark.parametrize("mode", [B.AGG_SHARED, B.AGG_GLOBAL_WARP, B.AGG_GLOBAL])
+def test_every_aggregation_strategy(tables, mode):
+    qs = [q for q in edge_queries(tables.rows) + mixed(tables, 80, seed=21) if q.grouped]
+    r = B.BatchRunner(tables, sizing="exact", agg_mode=mode)
+    got, rep = r.run(qs)
+    assert rep.overflowed == []
+    assert_all_equal(got, [oracle_result(tables, q) for q in qs], qs)
+    r.close()
+
+
 def test_exact_stats_match_numpy(tables):
     qs = edge_queries(tables.rows) + mixed(tables, 24, seed=3)
     b = B.Batch()

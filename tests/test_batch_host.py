@@ -145,3 +145,32 @@ def test_invariant_divisor_method():
     for d in ds:
         for n in [0, 1, d - 1, d, d + 1, (1 << 31) - 1] + [rnd.randrange(0, 1 << 31) for _ in range(200)]:
             assert div(n, d) == n // d, (n, d)
+
+
+def test_pinned_pool_recycles_buffers_when_views_die():
+    import gc
+    held = {}
+
+    def alloc(n):  # host memory stands in for pinned memory here
+        b = C.create_string_buffer(n)
+        held[C.addressof(b)] = b
+        return C.addressof(b)
+
+    pool = B.PinnedPool(alloc=alloc, free=lambda p: held.pop(p))
+    a = pool.array(1000)
+    assert a.nbytes >= 1000 and a.dtype == np.int64
+    a[:] = 7
+    v = a[10:20]          # a view keeps the buffer alive
+    del a
+    gc.collect()
+    assert pool._free == []
+    assert (v == 7).all()
+    del v
+    gc.collect()
+    assert len(pool._free) == 1
+    b = pool.array(500)   # reuses the freed buffer
+    assert len(pool._free) == 0
+    del b
+    gc.collect()
+    pool.close()
+    assert pool._free == [] and held == {}
