@@ -642,7 +642,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="join_topk",
                     choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed", "serve"])
-    ap.add_argument("--tune", default="")
+    ap.add_argument("--tune", default="auto", help='tuning string, "" for the defaults, or "auto"')
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
@@ -694,7 +694,24 @@ def main():
     w.generate()
     ctx = Context(local)
     w.register(ctx)
-    q = ctx.prepare(w.spec, args.tune)
+    tuner = None
+    tune = args.tune
+    if tune == "auto":
+        # the autotuner's choice for this template and table size (tuned
+        # now, untimed, when the device has none stored)
+        from gpudbmetalcodegen_b200 import autotune
+        cache = autotune.TuneCache()
+        tpl = dict(kv.split("=", 1) for kv in w.spec.split(";")).get("template")
+        rows = ctx.largest_table_rows()
+        if cache.get(tpl, rows) is None:
+            t0 = time.perf_counter()
+            tlog = []
+            autotune.tune_query(ctx, w.spec, rows, cache=cache, log=tlog)
+            tuner = {"tuned_s": time.perf_counter() - t0, "candidates": len(tlog) + 1}
+        e = cache.data.get(cache.key(tpl, rows), {})
+        tuner = {**(tuner or {}), "chosen": e.get("tune"), "tuned_ms": e.get("ms"), "default_ms": e.get("default_ms")}
+        tune = ctx.resolve_tune(w.spec, "auto")
+    q = ctx.prepare(w.spec, tune)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr)
 
     verified = None
@@ -807,6 +824,8 @@ def main():
         cfg = w.config()
         cfg.update({"l2": "inputs larger than the 126 MB L2; no flush", "tune": q.tune or "default",
                     "parallelism": f"replicas x{world}"})
+        if tuner:
+            cfg["autotune"] = tuner
         line = {"metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "config": cfg,

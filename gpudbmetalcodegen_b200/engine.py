@@ -155,6 +155,8 @@ class Context:
         self.handle = h
         self._queries: Dict[tuple, Query] = {}
         self._keep: List[Any] = []
+        self._table_rows: Dict[str, int] = {}
+        self._tune_cache = None
 
     # ---- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -194,6 +196,7 @@ class Context:
     def register_column(self, table: str, column: str, dptr: int, rows: int, elem_bytes: int) -> None:
         check(self._lib.gpudb_register_column(self.handle, table.encode(), column.encode(), C.c_void_p(dptr), rows,
                                               elem_bytes), self.handle)
+        self._table_rows[table] = rows
 
     def register_tensor(self, table: str, column: str, t) -> None:
         """Register a contiguous CUDA torch tensor as a resident column."""
@@ -212,6 +215,7 @@ class Context:
         arr = np.ascontiguousarray(arr)
         check(self._lib.gpudb_upload_column(self.handle, table.encode(), column.encode(), arr.ctypes.data,
                                             arr.shape[0], NP_ELEM[arr.dtype]), self.handle)
+        self._table_rows[table] = arr.shape[0]
         # the copy is stream-ordered: keep the host array alive until it completed
         self.synchronize()
 
@@ -245,7 +249,22 @@ class Context:
         check(self._lib.gpudb_set_use_graphs(self.handle, int(on)), self.handle)
 
     # ---- queries -------------------------------------------------------------
+    def largest_table_rows(self) -> int:
+        return max(self._table_rows.values(), default=0)
+
+    def resolve_tune(self, spec: str, tune: str) -> str:
+        """tune="auto": the autotuner's stored choice for this template at the
+        size of the largest registered table ("" when none is stored)."""
+        if tune != "auto":
+            return tune
+        from .autotune import TuneCache
+        if self._tune_cache is None:
+            self._tune_cache = TuneCache()
+        template = dict(kv.split("=", 1) for kv in spec.split(";") if "=" in kv).get("template", "")
+        return self._tune_cache.get(template, self.largest_table_rows()) or ""
+
     def prepare(self, spec: str, tune: str = "") -> Query:
+        tune = self.resolve_tune(spec, tune)
         key = (spec, tune)
         q = self._queries.get(key)
         if q is None:

@@ -1,0 +1,35 @@
+"""The autotuner's search and cache (no GPU)."""
+from gpudbmetalcodegen_b200 import autotune as A
+
+
+def test_coordinate_descent_finds_the_separable_minimum():
+    space = {"a": [3, 1, 2, 4], "b": ["x", "y", "z"], "c": [0, 1]}
+    cost = {"a": {1: 5, 2: 1, 3: 3, 4: 9}, "b": {"x": 4, "y": 1, "z": 2}, "c": {0: 1, 1: 0}}
+    calls = []
+
+    def measure(cfg):
+        calls.append(dict(cfg))
+        if cfg["b"] == "z" and cfg["c"] == 1:
+            return None  # an invalid candidate is never chosen
+        return sum(cost[k][v] for k, v in cfg.items()) + 10
+
+    log = []
+    best, t, t0 = A.coordinate_descent(space, measure, rounds=3, log=log)
+    assert best == {"a": 2, "b": "y", "c": 1} and t == 12 and t0 == 3 + 4 + 1 + 10
+    assert len(calls) == len({tuple(sorted(c.items())) for c in calls})  # nothing measured twice
+    assert len(log) == len(calls) - 1
+
+
+def test_noise_margin_keeps_the_default():
+    best, t, t0 = A.coordinate_descent({"a": [1, 2]}, lambda c: 100.0 if c["a"] == 1 else 99.0)
+    assert best == {"a": 1} and t == t0 == 100.0
+
+
+def test_cache_round_trip_and_size_buckets(tmp_path):
+    assert A.size_bucket(6_001_215) == A.size_bucket(10_000_000) != A.size_bucket(60_000_000)
+    c = A.TuneCache(tmp_path / "dev.json")
+    assert c.get("q1", 6_001_215) is None
+    c.put("q1", 6_001_215, "bs=256;stages=2", 0.04, 0.05)
+    again = A.TuneCache(tmp_path / "dev.json")
+    assert again.get("q1", 7_000_000) == "bs=256;stages=2"
+    assert again.get("q1", 100_000_000) is None

@@ -244,3 +244,20 @@ def test_mix_templates_parity(ctx, mix_small, thr):
         assert np.array_equal(np.array(res.column("sum")), s)
         res, _ = ctx.run(f"template=mix_topk;thr={thr};card={card};key={key_col};k=7")
         assert res.rows == O.topk(k, s, 7)
+
+
+def test_autotuner_never_changes_an_answer(ctx, tmp_path):
+    from gpudbmetalcodegen_b200 import autotune as A
+    f = W.gen_fact(2_000_000, seed=19)
+    ctx.upload_table("fact", f)
+    cache = A.TuneCache(tmp_path / "dev.json")
+    log = []
+    space = {"bs": ["512", "256"], "tile": ["0", "1024"], "stages": ["4", "2"], "keyed": ["0", "1", "4"]}
+    tune, best, default = A.tune_query(ctx, "template=q1", ctx.largest_table_rows(), space=space, cache=cache,
+                                       log=log, reps=3, rounds=1)
+    assert best <= default and len(log) >= 4
+    res, _ = ctx.run("template=q1", tune)
+    assert_q1_equal(res, O.q1(f))
+    assert cache.get("q1", 2_000_000) == tune
+    ctx._tune_cache = cache
+    assert ctx.prepare("template=q1", "auto").tune == tune
