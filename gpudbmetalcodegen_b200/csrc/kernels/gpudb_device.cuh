@@ -169,6 +169,44 @@ __device__ __forceinline__ unsigned long long gpudb_warp_reserve(unsigned long l
 }
 
 // ------------------------------------------------------------------
+// V consecutive elements of a staged column (shared memory, aligned to
+// sizeof(T) * V) into registers with as few wide loads as possible.
+// ------------------------------------------------------------------
+template <typename T, int V>
+__device__ __forceinline__ void gpudb_vload(const void* src, T (&out)[V]) {
+    constexpr int B = (int)sizeof(T) * V;
+    if constexpr (B % 16 == 0) {
+        union {
+            int4 v[B / 16];
+            T t[V];
+        } u;
+#pragma unroll
+        for (int c = 0; c < B / 16; ++c) u.v[c] = reinterpret_cast<const int4*>(src)[c];
+#pragma unroll
+        for (int j = 0; j < V; ++j) out[j] = u.t[j];
+    } else if constexpr (B == 8) {
+        union {
+            uint2 v;
+            T t[V];
+        } u;
+        u.v = *reinterpret_cast<const uint2*>(src);
+#pragma unroll
+        for (int j = 0; j < V; ++j) out[j] = u.t[j];
+    } else if constexpr (B == 4) {
+        union {
+            unsigned v;
+            T t[V];
+        } u;
+        u.v = *reinterpret_cast<const unsigned*>(src);
+#pragma unroll
+        for (int j = 0; j < V; ++j) out[j] = u.t[j];
+    } else {
+#pragma unroll
+        for (int j = 0; j < V; ++j) out[j] = reinterpret_cast<const T*>(src)[j];
+    }
+}
+
+// ------------------------------------------------------------------
 // TMA bulk copy (cp.async.bulk, 1-D, CTA-local destination) + mbarrier
 // ------------------------------------------------------------------
 __device__ __forceinline__ unsigned gpudb_smem_addr(const void* p) {
@@ -215,6 +253,12 @@ __device__ __forceinline__ void gpudb_bulk_g2s_stream(void* dst, const void* src
         "%4;" ::"r"(gpudb_smem_addr(dst)),
         "l"(src), "r"(bytes), "r"(gpudb_smem_addr(bar)), "l"(policy)
         : "memory");
+}
+
+// Bring `bytes` (multiple of 16, 16-byte aligned source) into L2 ahead of a
+// later copy; no shared memory, no completion to wait for.
+__device__ __forceinline__ void gpudb_bulk_prefetch_l2(const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ unsigned long long gpudb_policy_evict_first() {

@@ -113,6 +113,15 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.setPhaseTileRows(tile);
 
     const std::string SB = S(stageBytes), ST = S(stages), TL = S(tile);
+    // Vector mode: V consecutive rows per consumer thread, every staged
+    // column read with wide loads (its stage region is 128-byte aligned and
+    // a group of V rows starts at a multiple of V * width).
+    int vec = cfg_.vectorRows;
+    if (vec > 1) {
+        const bool pow2 = (vec & (vec - 1)) == 0 && vec <= 8;
+        if (!pow2 || tile % vec != 0)
+            throw std::runtime_error("CudaGridStrideScan: vector rows must be 2, 4 or 8 and divide the tile");
+    }
     // The innermost bitmap probe above this scan, if no operator between
     // them defines names: its words are loaded for prefetchRows rows ahead.
     int pf = -1;
@@ -175,6 +184,33 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                         cg.addLine("gpudb_bulk_g2s_stream(_st + " + S(off[k]) + ", " + columns_[k].paramName + " + _sb_t * " +
                                    TL + "ll, " + S(tile * w) + "u, _sb_full + _s, _sb_pol);");
                     }
+                    if (cfg_.l2Prefetch > 0) {
+                        // keep the l2Prefetch rounds after the ring's in L2 (into L2 only)
+                        cg.addLine("const long long _pf_t = _sb_t + (long long)" + S(stages + cfg_.l2Prefetch - 1) +
+                                   " * gridDim.x;");
+                        cg.addBlock("if (_pf_t < _sb_ntiles)", [&]() {
+                            for (size_t k = 0; k < columns_.size(); k++) {
+                                if (columns_[k].late) continue;
+                                const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
+                                cg.addLine("gpudb_bulk_prefetch_l2(" + columns_[k].paramName + " + _pf_t * " + TL + "ll, " +
+                                           S(tile * w) + "u);");
+                            }
+                        });
+                        cg.addBlock("if (_sb_j == 0)", [&]() {  // the first rounds beyond the ring
+                            cg.addBlock("for (int _pr = 1; _pr < " + S(cfg_.l2Prefetch) + "; ++_pr)", [&]() {
+                                cg.addLine("const long long _pq = _sb_t + (long long)(" + S(stages) +
+                                           " + _pr - 1) * gridDim.x;");
+                                cg.addBlock("if (_pq < _sb_ntiles)", [&]() {
+                                    for (size_t k = 0; k < columns_.size(); k++) {
+                                        if (columns_[k].late) continue;
+                                        const long long w = (long long)cudaTypeBytes(columns_[k].cudaType);
+                                        cg.addLine("gpudb_bulk_prefetch_l2(" + columns_[k].paramName + " + _pq * " + TL +
+                                                   "ll, " + S(tile * w) + "u);");
+                                    }
+                                });
+                            });
+                        });
+                    }
                 });
             });
         }, " else {");
@@ -196,7 +232,9 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                         cg.addLine("const " + c.cudaType + "* " + c.paramName + " = reinterpret_cast<const " + c.cudaType +
                                    "*>(_sb_st + " + S(off[k]) + ");");
                 }
-                if (pf < 0) {
+                if (vec > 1) {
+                    emitVectorRows(cg, consume, pf, tile, off);  // releases the stage itself
+                } else if (pf < 0) {
                     cg.addBlock("for (int " + i + " = (int)threadIdx.x - 32; " + i + " < " + TL + "; " + i +
                                     " += (int)blockDim.x - 32)",
                                 [&]() {
@@ -207,8 +245,10 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                     emitPrefetchedRows(cg, consume, pf, TL);
                 }
             });
-            cg.addLine("__syncwarp();");
-            cg.addLine("if ((threadIdx.x & 31u) == 0u) gpudb_mbar_arrive(_sb_empty + _s);");
+            if (vec <= 1) {
+                cg.addLine("__syncwarp();");
+                cg.addLine("if ((threadIdx.x & 31u) == 0u) gpudb_mbar_arrive(_sb_empty + _s);");
+            }
         });
         cg.decreaseIndent();
         cg.addLine("}");
@@ -257,6 +297,88 @@ void CudaGridStrideScan::emitPrefetchedRows(CudaCodegen& cg, ConsumerFn consume,
                 cg.setPrefetchVar(pf, "_pfw[_pf_u]");
                 consume();
                 cg.setPrefetchVar(pf, "");
+            });
+        });
+    });
+}
+
+// Consumer row loop of a staged tile in groups of V consecutive rows. Each
+// thread first copies all its groups' staged values from shared memory
+// into registers (wide loads) and releases the stage, then runs the rows:
+// the ring is refilled while rows with slow follow-up work (late-column
+// reads, hash inserts) are still in flight, so one such row no longer
+// holds the whole tile. Register arrays shadow the column names, so row
+// expressions `col[i]` read registers; late columns are offset to the
+// group. With a bitmap-probe hint and pf > 0, a group's V bitmap words are
+// loaded together before any of its rows uses one.
+void CudaGridStrideScan::emitVectorRows(CudaCodegen& cg, ConsumerFn consume, int pf, int tile,
+                                        const std::vector<long long>& off) {
+    const int V = cfg_.vectorRows;
+    const int consumers = cg.currentThreadgroupSize() - 32;
+    const int groups = tile / V;
+    const int G = (groups + consumers - 1) / consumers;  // groups per consumer thread (compile time)
+    const std::string& i = idxVar_;
+    const std::string VS = S(V), GS = S(G);
+    cg.addLine("const int _v_step = (int)blockDim.x - 32;");
+    // load phase
+    for (size_t k = 0; k < columns_.size(); k++) {
+        const auto& c = columns_[k];
+        if (!c.late) cg.addLine(c.cudaType + " _vr_" + c.paramName + "[" + GS + "][" + VS + "];");
+    }
+    cg.addLine("#pragma unroll");
+    cg.addBlock("for (int _g = 0; _g < " + GS + "; ++_g)", [&]() {
+        cg.addLine("const int _vg = (int)threadIdx.x - 32 + _g * _v_step;");
+        cg.addBlock("if (_vg < " + S(groups) + ")", [&]() {
+            for (size_t k = 0; k < columns_.size(); k++) {
+                const auto& c = columns_[k];
+                if (c.late) continue;
+                const long long w = (long long)cudaTypeBytes(c.cudaType);
+                cg.addLine("gpudb_vload<" + c.cudaType + ", " + VS + ">(_sb_st + " + S(off[k]) + " + (long long)_vg * " +
+                           S(w * V) + ", _vr_" + c.paramName + "[_g]);");
+            }
+        });
+    });
+    cg.addComment("the staged values are in registers: release the stage now");
+    cg.addLine("__syncwarp();");
+    cg.addLine("if ((threadIdx.x & 31u) == 0u) gpudb_mbar_arrive(_sb_empty + _s);");
+    // row phase
+    cg.addLine("#pragma unroll");
+    cg.addBlock("for (int _g = 0; _g < " + GS + "; ++_g)", [&]() {
+        cg.addLine("const int _vg = (int)threadIdx.x - 32 + _g * _v_step;");
+        cg.addBlock("if (_vg < " + S(groups) + ")", [&]() {
+            cg.addLine("const long long _vbase = _sb_base + (long long)_vg * " + VS + ";");
+            for (size_t k = 0; k < columns_.size(); k++) {
+                const auto& c = columns_[k];
+                if (c.late)
+                    cg.addLine("const " + c.cudaType + "* " + c.paramName + " = _lt_" + c.paramName + " + _vbase;");
+                else
+                    cg.addLine("const " + c.cudaType + "* " + c.paramName + " = _vr_" + c.paramName + "[_g];");
+            }
+            std::string pfVar;
+            if (pf >= 0 && cfg_.prefetchRows > 0) {
+                const auto hint = cg.scanHints()[pf];
+                std::string guard;
+                for (size_t h = pf + 1; h < cg.scanHints().size(); ++h)
+                    if (cg.scanHints()[h].kind == CudaCodegen::ScanHint::Guard)
+                        guard += " && (" + cg.scanHints()[h].expr + ")";
+                cg.addLine("unsigned _pfw[" + VS + "];");
+                cg.addLine("#pragma unroll");
+                cg.addBlock("for (int " + i + " = 0; " + i + " < " + VS + "; ++" + i + ")", [&]() {
+                    cg.addLine("_pfw[" + i + "] = 0u;");
+                    cg.addBlock("if (true" + guard + ")", [&]() {
+                        cg.addLine("const long long _pf_k = (long long)(" + hint.expr + ");");
+                        cg.addLine("if ((unsigned long long)(_pf_k >> 5) < (unsigned long long)len_" + hint.bitmap +
+                                   ") _pfw[" + i + "] = __ldg(" + hint.bitmap + " + (_pf_k >> 5));");
+                    });
+                });
+                pfVar = "_pfw[" + i + "]";
+            }
+            cg.addLine("#pragma unroll");
+            cg.addBlock("for (int " + i + " = 0; " + i + " < " + VS + "; ++" + i + ")", [&]() {
+                cg.addLine("const long long _row = _vbase + " + i + "; (void)_row;");
+                if (!pfVar.empty()) cg.setPrefetchVar(pf, pfVar);
+                consume();
+                if (!pfVar.empty()) cg.setPrefetchVar(pf, "");
             });
         });
     });
@@ -959,9 +1081,20 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
         cg.addLine("__syncthreads();");
     }
     const std::string list = table_ + "_slotlist", nlist = table_ + "_nslots";
+    // Groups created by this CTA are listed in shared memory first and
+    // appended to the global slot list with one atomic per CTA at the end;
+    // a per-group atomic on the single global counter would serialise in L2.
+    constexpr int kSlotBuf = 1024;
     if (slotList_) {
         cg.addBufferParam(list, "unsigned", cap, false);
         cg.addAtomicBufferParam(nlist, "unsigned long long", "1");
+        const int bo = cg.allocDynamicSmem(kSlotBuf * 4 + 16);
+        cg.addLine("unsigned* _gl_buf = reinterpret_cast<unsigned*>(gpudb_smem + " + S(bo) + ");");
+        cg.addLine("unsigned* _gl_n = _gl_buf + " + S(kSlotBuf) + ";");
+        cg.addLine("unsigned long long* _gl_base = reinterpret_cast<unsigned long long*>(_gl_buf + " + S(kSlotBuf + 2) +
+                   ");");
+        cg.addLine("if (threadIdx.x == 0) *_gl_n = 0u;");
+        cg.addLine("__syncthreads();");
     }
     auto globalUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
         if (slotList_) cg.addLine("bool _gnew = false;");
@@ -971,7 +1104,11 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
             for (int j = 0; j < na; j++)
                 cg.addLine("atomicAdd(" + table_ + "_" + aggs_[j].name + " + _gslot, (unsigned long long)" + vals[j] + ");");
             if (slotList_)
-                cg.addLine("if (_gnew) " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;  // group created");
+                cg.addBlock("if (_gnew)", [&]() {  // group created
+                    cg.addLine("const unsigned _gp = atomicAdd(_gl_n, 1u);");
+                    cg.addLine("if (_gp < " + S(kSlotBuf) + "u) _gl_buf[_gp] = (unsigned)_gslot;");
+                    cg.addLine("else " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;");
+                });
         });
     };
     child_->produce(cg, [&]() {
@@ -1016,6 +1153,17 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
             std::vector<std::string> vals;
             for (int j = 0; j < na; j++) vals.push_back("_gs_v[" + S(j) + " * " + S(1 << L) + " + _w]");
             globalUpdate("(_fk)", vals);
+        });
+    }
+    if (slotList_) {
+        cg.addComment("append this CTA's created groups to the global slot list");
+        cg.addLine("__syncthreads();");
+        cg.addBlock("", [&]() {
+            cg.addLine("const unsigned _gn = min(*_gl_n, " + S(kSlotBuf) + "u);");
+            cg.addLine("if (threadIdx.x == 0) *_gl_base = _gn ? atomicAdd(" + nlist + ", (unsigned long long)_gn) : 0ull;");
+            cg.addLine("__syncthreads();");
+            cg.addLine("for (unsigned _w = threadIdx.x; _w < _gn; _w += blockDim.x) " + list +
+                       "[*_gl_base + _w] = _gl_buf[_w];");
         });
     }
     auto& hs = cg.resultSchema();

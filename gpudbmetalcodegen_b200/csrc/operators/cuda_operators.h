@@ -49,6 +49,8 @@ struct ScanConfig {
     int tileRows = 0;      // rows per TMA tile (multiple of 16); 0 = about 24 KB of staged columns
     int stages = 4;        // TMA ring depth (clamped to the shared-memory budget)
     int prefetchRows = 0;  // rows whose probe bitmap words are loaded ahead (0 = off)
+    int vectorRows = 0;    // consecutive rows per consumer thread, loaded with wide shared loads (0/1 = off)
+    int l2Prefetch = 0;    // tiles beyond the ring the producer prefetches into L2 (0 = off)
 };
 
 // ------------------------------------------------------------------
@@ -81,6 +83,7 @@ public:
 
 private:
     void emitPrefetchedRows(CudaCodegen& cg, ConsumerFn consume, int pf, const std::string& tileRows);
+    void emitVectorRows(CudaCodegen& cg, ConsumerFn consume, int pf, int tile, const std::vector<long long>& off);
 
 public:
 

@@ -97,7 +97,7 @@ std::string TuneConfig::toString() const {
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
-      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows;
+      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch;
     return o.str();
 }
 
@@ -122,6 +122,8 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "late") t.lateMaterialize = std::stoi(v) != 0;
         else if (k == "occ") t.minBlocksPerSM = std::stoi(v);
         else if (k == "pf") t.scan.prefetchRows = std::stoi(v);
+        else if (k == "vec") t.scan.vectorRows = std::stoi(v);
+        else if (k == "l2pf") t.scan.l2Prefetch = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 REL = 1e-12
 
 Q1_TUNES = ["", "scan=direct", "bs=256;tile=1024;stages=2", "bs=1024;tile=2048;stages=3", "bs=128;tile=512;stages=8",
-            "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3"]
+            "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3", "vec=4", "vec=2;bs=256", "vec=8;tile=2048"]
 
 
 def assert_q1_equal(res, expect):
@@ -39,7 +39,7 @@ def test_q1_parity(ctx, fact_small, tune):
     assert_q1_equal(res, O.q1(fact_small))
 
 
-@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=1024;tile=4096;stages=2"])
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=1024;tile=4096;stages=2", "vec=4", "vec=8;bs=256"])
 def test_q6_parity(ctx, fact_small, tune):
     ctx.upload_table("fact", fact_small)
     res, _ = ctx.run("template=q6", tune)
@@ -103,7 +103,8 @@ def load_join(ctx, nd, npr, seed=3):
     return d, p
 
 
-@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0", "late=0", "bs=1024;tile=2048;stages=3"])
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0", "late=0", "bs=1024;tile=2048;stages=3",
+                                  "vec=4", "vec=4;pf=4", "vec=8;late=0", "pf=4"])
 def test_join_topk_parity(ctx, tune):
     d, p = load_join(ctx, 200_000, 800_000)
     top, groups, distinct = O.join_topk(d, p, k=10)
@@ -185,7 +186,8 @@ def test_join_topk_full_size(ctx):
 # ---------------------------------------------------------------------------
 # skewed group-by and hash join
 # ---------------------------------------------------------------------------
-GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0"]
+GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0",
+            "vec=4", "vec=2;smem=0"]
 
 
 @pytest.fixture(scope="module")
@@ -258,6 +260,6 @@ def test_autotuner_never_changes_an_answer(ctx, tmp_path):
     assert best <= default and len(log) >= 4
     res, _ = ctx.run("template=q1", tune)
     assert_q1_equal(res, O.q1(f))
-    assert cache.get("q1", 2_000_000) == tune
+    assert cache.get("q1", ctx.largest_table_rows()) == tune
     ctx._tune_cache = cache
     assert ctx.prepare("template=q1", "auto").tune == tune
