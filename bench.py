@@ -502,12 +502,15 @@ def run_mixed(args):
                 "plain_per_query": {"queries_per_s": len(queries) / plain_s, "ms_per_batch": plain_s * 1e3,
                                     "count_passes": plain.count_passes},
                 "batched_exact": {"queries_per_s": len(queries) / exact_s, "ms_per_batch": exact_s * 1e3,
-                                  "stats_ms": exact_rep.stats_ms},
+                                  "stats_ms": exact_rep.stats_ms, "execute_ms": exact_rep.execute_ms,
+                                  "collect_ms": exact_rep.collect_ms, "overflowed": len(exact_rep.overflowed),
+                                  "fallback_s": exact_rep.fallback_s},
                 "batched_learned": {"queries_per_s": len(queries) / (wall_ms / 1e3), "ms_per_batch": wall_ms,
                                     "execute_ms": statistics.median(r.execute_ms for r in reps),
                                     "features_ms": statistics.median(r.features_ms for r in reps),
                                     "collect_ms": statistics.median(r.collect_ms for r in reps),
                                     "overflowed": len(reps[-1].overflowed),
+                                    "fallback_s": statistics.median(r.fallback_s for r in reps),
                                     "table_slots": reps[-1].table_slots},
                 "speedup_vs_plain": (len(queries) / (wall_ms / 1e3)) / (len(queries) / plain_s),
                 "rows_per_s": total_rows * world / (step_ms / 1e3),
