@@ -627,6 +627,27 @@ def run_serve(args):
     ctx.close()
 
 
+def run_aggmodes(args):
+    """The batched group-by stage per aggregation strategy, cardinality and
+    key skew: one 60M-row query at 50 % selectivity each."""
+    import torch
+    from gpudbmetalcodegen_b200 import autotune, batch as B, workloads as W
+    world, rank, local = dist_info()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "a measurement of this build's strategies only"}))
+        return
+    torch.cuda.set_device(local)
+    rows = args.zprobe_rows // 2
+    tables = B.MixTables(rows=rows, zipf_s=(W.ZIPF_S,), nranks=W.MIX_NRANKS, dim_rows=1_000_000, seed=W.SEED)
+    table = autotune.measure_agg_modes(tables, rows)
+    if rank == 0:
+        print(json.dumps({"metric": "group_stage_ms_per_strategy", "value": None, "unit": "ms", "n_gpus": 1,
+                          "steps": 3, "warmup": 1, "higher_is_better": False, "dtype": "int64",
+                          "data": "synthetic (seeded)", "config": {"workload": f"aggmodes: {rows} rows, thr 5000"},
+                          "table": table}), flush=True)
+
+
 def load_traffic(kernel: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -644,7 +665,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="join_topk",
-                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed", "serve"])
+                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed", "serve", "aggmodes"])
     ap.add_argument("--tune", default="auto", help='tuning string, "" for the defaults, or "auto"')
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -672,6 +693,8 @@ def main():
         return run_mixed(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "aggmodes":
+        return run_aggmodes(args)
     world, rank, local = dist_info()
     w = make_workload(args)
 

@@ -204,3 +204,35 @@ def tune_batch(runner_factory: Callable[[dict], object], queries, space: Optiona
             r.close()
 
     return coordinate_descent(space, measure, rounds=rounds, log=log)
+
+
+def measure_agg_modes(tables, rows: int, cards=(16, 1024, 8192, 65536, 524288, 4194304),
+                      keys=("m_rank_u", "m_rank_z"), thr: int = 5000, reps: int = 3) -> List[dict]:
+    """Device time of the batched group-by stage for one query of `rows`
+    rows per aggregation strategy, over key cardinalities and key skew
+    (uniform m_rank_u / Zipf m_rank_z): the measurements behind the
+    strategy policy of the batched path."""
+    from . import batch as B
+    out = []
+    for key in keys:
+        for card in cards:
+            q = B.MixQuery("groupby", 0, 0, rows, thr, key=key, card=card)
+            row = {"key": key, "card": card}
+            for mode, name in ((B.AGG_SHARED, "shared"), (B.AGG_GLOBAL_WARP, "global_warp"),
+                               (B.AGG_GLOBAL, "global")):
+                b = B.Batch()
+                try:
+                    b.set_queries([tables.query_struct(q)])
+                    _, d, _ = b.exact_stats()
+                    b.set_groups(0, max(1, int(d[0])))
+                    b.set_agg_mode(0, mode)
+                    ts = []
+                    for _ in range(reps + 1):
+                        b.execute(use_graph=False)
+                        ts.append(b.stage_ms()["group"])
+                    row[name + "_ms"] = min(ts[1:])
+                    row["groups"] = int(d[0])
+                finally:
+                    b.close()
+            out.append(row)
+    return out
