@@ -33,3 +33,14 @@ def test_cache_round_trip_and_size_buckets(tmp_path):
     again = A.TuneCache(tmp_path / "dev.json")
     assert again.get("q1", 7_000_000) == "bs=256;stages=2"
     assert again.get("q1", 100_000_000) is None
+
+
+def test_seeds_reach_joint_moves():
+    # only the joint move (a=1, b=1) is better: one parameter at a time never finds it
+    space = {"a": [0, 1], "b": [0, 1]}
+    t = {(0, 0): 10.0, (1, 0): 12.0, (0, 1): 12.0, (1, 1): 5.0}
+    measure = lambda c: t[(c["a"], c["b"])]
+    best, bt, t0 = A.coordinate_descent(space, measure)
+    assert best == {"a": 0, "b": 0}
+    best, bt, t0 = A.coordinate_descent(space, measure, seeds=[{"a": 1, "b": 1}, {"zzz": 3}])
+    assert best == {"a": 1, "b": 1} and bt == 5.0 and t0 == 10.0
