@@ -44,7 +44,8 @@ SPACES = {
     "q6": SCAN_SPACE,
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
-    "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"]},
+    "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
+                 "smem": ["10", "0", "8"], "warp": ["1", "0"]},
 }
 # Joint moves coordinate descent cannot make one parameter at a time (a
 # shallower TMA ring frees the shared memory that a higher occupancy needs):
@@ -54,7 +55,7 @@ SEEDS = {
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
     "join_topk": [{"stages": "2", "warp": "0"}, {"tile": "1024", "warp": "0"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"}],
-    "hashjoin": [{"stages": "2"}],
+    "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"}],
 }
 BATCH_SPACE = {
     "block": [512, 256, 1024],
