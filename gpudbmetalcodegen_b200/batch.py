@@ -51,6 +51,9 @@ class BatchQueryStruct(C.Structure):
                 ("filter_max", C.c_int32), ("agg_mode", C.c_int32)]
 
 
+QUERY_DTYPE = np.dtype(BatchQueryStruct)  # the same layout as a numpy record
+
+
 @dataclass(frozen=True)
 class MixQuery:
     """One query of the mixed workload over a slice of a resident mix table."""
@@ -93,6 +96,32 @@ def same_result(a, b) -> bool:
     if a[0] == "groups":
         return all(np.array_equal(x, y) for x, y in zip(a[1:], b[1:]))
     return tuple(a[1:]) == tuple(b[1:])
+
+
+def _mix64(x: np.ndarray) -> np.ndarray:
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def result_fingerprint(r) -> tuple:
+    """An order-independent 64-bit fingerprint of a result (a multiset hash
+    of its group rows, vectorised; exact tuples for scalar / top-k), so
+    large answers can be checked without keeping or sorting them."""
+    if r[0] == "scalar":
+        return r
+    if r[0] == "topk":
+        return r
+    if r[0] == "groups_raw":
+        k, c, sm = r[1][:, 0], r[1][:, 1], r[1][:, 2]
+    else:
+        k, c, sm = r[1], r[2], r[3]
+    with np.errstate(over="ignore"):
+        k = np.asarray(k).astype(np.uint64)
+        c = np.asarray(c).astype(np.uint64)
+        sm = np.asarray(sm).astype(np.uint64)
+        h = _mix64(k * np.uint64(0x9E3779B97F4A7C15) ^ _mix64(c + np.uint64(1)) ^ _mix64(sm ^ np.uint64(0x5851F42D)))
+        return ("groups", int(k.size), int(h.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(h) if h.size else 0))
 
 
 def describe_difference(a, b) -> str:
@@ -176,6 +205,43 @@ class MixTables:
                              key_min=kmin, key_max=kmax, filter_min=st["m_filter"][0],
                              filter_max=st["m_filter"][1])
         return s
+
+    def query_array(self, queries: Sequence[MixQuery]) -> np.ndarray:
+        """All queries as one array of gpudb_batch_query (groups 1, AUTO
+        strategy), built column-wise."""
+        n = len(queries)
+        a = np.zeros(max(1, n), dtype=QUERY_DTYPE)[:n]
+        if n == 0:
+            return a
+        tb = np.array([q.table for q in queries], dtype=np.int64)
+        r0 = np.array([q.row0 for q in queries], dtype=np.int64)
+        zipf = np.array([q.key == "m_rank_z" for q in queries])
+        a["tmpl"] = [TPL[q.tmpl] for q in queries]
+        a["thr"] = [q.thr for q in queries]
+        a["card"] = [max(1, q.card) for q in queries]
+        a["k"] = [q.k for q in queries]
+        a["attr_lt"] = [q.attr_lt for q in queries]
+        a["rows"] = [q.rows for q in queries]
+
+        def base(col):
+            return np.array([t[col].data_ptr() for t in self.tables], dtype=np.int64)[tb]
+
+        a["key"] = np.where(zipf, base("m_rank_z"), base("m_rank_u")) + 4 * r0
+        a["filter"] = base("m_filter") + 4 * r0
+        a["value"] = base("m_value") + 8 * r0
+        a["fk"] = base("m_fk") + 4 * r0
+        a["dim_key"] = self.dim["md_key"].data_ptr()
+        a["dim_attr"] = self.dim["md_attr"].data_ptr()
+        a["dim_rows"] = self.dim_rows
+        a["dim_max_key"] = self.dim_max_key
+        a["groups"] = 1
+        kmin = np.array([[st["m_rank_u"][0], st["m_rank_z"][0]] for st in self.stats], dtype=np.int64)
+        kmax = np.array([[st["m_rank_u"][1], st["m_rank_z"][1]] for st in self.stats], dtype=np.int64)
+        a["key_min"] = kmin[tb, zipf.astype(np.int64)]
+        a["key_max"] = kmax[tb, zipf.astype(np.int64)]
+        a["filter_min"] = np.array([st["m_filter"][0] for st in self.stats])[tb]
+        a["filter_max"] = np.array([st["m_filter"][1] for st in self.stats])[tb]
+        return a
 
     def bytes(self) -> int:
         return sum(t.numel() * t.element_size() for tab in self.tables for t in tab.values()) + \
@@ -276,7 +342,15 @@ class Batch:
         except Exception:
             pass
 
-    def set_queries(self, structs: Sequence[BatchQueryStruct]) -> None:
+    def set_queries(self, structs) -> None:
+        """Describe the batch: a sequence of BatchQueryStruct, or an array
+        of QUERY_DTYPE (MixTables.query_array)."""
+        if isinstance(structs, np.ndarray):
+            arr = np.ascontiguousarray(structs, dtype=QUERY_DTYPE)
+            self._structs = arr
+            check(self._lib.gpudb_batch_set_queries(self.handle, arr.ctypes.data if arr.size else None, arr.size))
+            self.n = arr.size
+            return
         arr = (BatchQueryStruct * max(1, len(structs)))(*structs)
         self._structs = arr
         check(self._lib.gpudb_batch_set_queries(self.handle, arr, len(structs)))
@@ -664,7 +738,8 @@ class BatchRunner:
         key = tuple(queries)
         b = self.batch
         if key != self._key:
-            b.set_queries([self.tables.query_struct(q) for q in queries])
+            self._arr = self.tables.query_array(queries)
+            b.set_queries(self._arr)
             self._key, self._groups = key, None
         self._features = None
         groups = self.size(queries, report)
@@ -672,9 +747,9 @@ class BatchRunner:
                   agg_mode_for(g, None if self._features is None else self._features[i])) if q.grouped else AGG_AUTO
                  for i, (g, q) in enumerate(zip(groups, queries))]
         if (groups, modes) != self._groups:
-            for i, (g, m) in enumerate(zip(groups, modes)):
-                b.set_groups(i, g)
-                b.set_agg_mode(i, m)
+            self._arr["groups"] = groups
+            self._arr["agg_mode"] = modes
+            b.set_queries(self._arr)  # one call re-plans the arena
             self._groups = (groups, modes)
         report.table_slots = sum(1 << max(4, math.ceil(math.log2(2 * g))) for g, q in zip(groups, queries)
                                  if q.grouped)

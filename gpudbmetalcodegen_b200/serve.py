@@ -65,6 +65,7 @@ class ServeReport:
     overflowed: int = 0
     peak_reserved_bytes: int = 0
     overlap_s: float = 0.0  # time with two or more batches in flight
+    busy: dict = field(default_factory=dict)  # summed per-batch components (s)
 
     @property
     def qps(self) -> float:
@@ -77,7 +78,7 @@ class ServeReport:
                 "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "batches": self.batches,
                 "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
                 "overflow_reruns": self.overflowed, "peak_reserved_gb": self.peak_reserved_bytes / 1e9,
-                "overlap_s": self.overlap_s, "wall_s": self.wall_s}
+                "overlap_s": self.overlap_s, "wall_s": self.wall_s, "busy_s": self.busy}
 
 
 class Server:
@@ -99,15 +100,20 @@ class Server:
         for r in self.runners:
             r.close()
 
-    def serve(self, trace: Sequence[Request]) -> tuple:
-        """Replay `trace` in real time; returns (results by request id, report)."""
+    def serve(self, trace: Sequence[Request], on_result=None) -> tuple:
+        """Replay `trace` in real time; returns (results by request id,
+        report). With `on_result(id, result)` each answer is handed over as
+        it completes (from the worker thread, as a view of the pinned buffer
+        it arrived in) and not kept; otherwise answers are copied out."""
         import torch
         n = len(trace)
         results: List[Optional[tuple]] = [None] * n
         done_at = np.zeros(n)
         cv = threading.Condition()
         state = {"next": 0, "arrived": 0, "completed": 0, "reserved": 0, "peak": 0, "inflight": 0,
-                 "overlap": 0.0, "mark": None, "batches": [], "overflowed": 0, "error": None}
+                 "overlap": 0.0, "mark": None, "batches": [], "overflowed": 0, "error": None,
+                 "busy": {"batch_wall": 0.0, "execute": 0.0, "features": 0.0, "predict": 0.0, "collect": 0.0,
+                          "fallback": 0.0}}
         cost = [query_hbm_bytes(r.query, self.tables.dim_max_key) for r in trace]
         t0 = time.perf_counter()
 
@@ -147,13 +153,19 @@ class Server:
                         state["mark"] = now
                     state["inflight"] += 1
                 try:
-                    res, rep = runner.run([trace[i].query for i in take])
+                    # kept answers leave the pinned buffer at once, so it returns
+                    # to the pool however long callers keep them
+                    res, rep = runner.run([trace[i].query for i in take], copy=on_result is None)
                 except Exception as e:  # surfaced to the caller
                     with cv:
                         state["error"] = e
                         cv.notify_all()
                     return
                 t_done = time.perf_counter() - t0
+                if on_result is not None:
+                    for j, i in enumerate(take):
+                        on_result(i, res[j])
+                    res = [None] * len(take)
                 with cv:
                     for j, i in enumerate(take):
                         results[i] = res[j]
@@ -162,6 +174,13 @@ class Server:
                     state["reserved"] -= bytes_
                     state["batches"].append(len(take))
                     state["overflowed"] += len(rep.overflowed)
+                    bz = state["busy"]
+                    bz["batch_wall"] += rep.wall_s
+                    bz["execute"] += rep.execute_ms / 1e3
+                    bz["features"] += rep.features_ms / 1e3
+                    bz["predict"] += rep.predict_ms / 1e3
+                    bz["collect"] += rep.collect_ms / 1e3
+                    bz["fallback"] += rep.fallback_s
                     state["inflight"] -= 1
                     if state["inflight"] < 2 and state["mark"] is not None:
                         state["overlap"] += time.perf_counter() - state["mark"]
@@ -190,7 +209,7 @@ class Server:
         rate = n / trace[-1].arrival if n and trace[-1].arrival > 0 else 0.0
         rep = ServeReport(rate=rate, requests=n, wall_s=wall, latencies_s=lat, batches=len(state["batches"]),
                           batch_sizes=state["batches"], overflowed=state["overflowed"],
-                          peak_reserved_bytes=state["peak"], overlap_s=state["overlap"])
+                          peak_reserved_bytes=state["peak"], overlap_s=state["overlap"], busy=state["busy"])
         return results, rep
 
 

@@ -269,3 +269,13 @@ def test_stage_times(tables):
     st = b.stage_ms()
     assert set(st) == set(B.Batch.STAGES) and all(v >= 0 for v in st.values())
     b.close()
+
+
+def test_query_array_equals_structs(tables):
+    qs = edge_queries(tables.rows) + mixed(tables, 30, seed=17)
+    arr = tables.query_array(qs)
+    for i, q in enumerate(qs):
+        st = tables.query_struct(q)
+        for name, _ in B.BatchQueryStruct._fields_:
+            a, s = arr[i][name], getattr(st, name)
+            assert int(a) == int(s or 0), (i, name, a, s)

@@ -174,3 +174,19 @@ def test_pinned_pool_recycles_buffers_when_views_die():
     gc.collect()
     pool.close()
     assert pool._free == [] and held == {}
+
+
+def test_query_dtype_matches_the_struct():
+    assert B.QUERY_DTYPE.itemsize == C.sizeof(B.BatchQueryStruct)
+    for name, _ in B.BatchQueryStruct._fields_:
+        assert B.QUERY_DTYPE.fields[name][1] == getattr(B.BatchQueryStruct, name).offset
+
+
+def test_result_fingerprint_is_order_independent_and_sensitive():
+    raw = np.array([[5, 1, 10], [2, 3, 30], [9, 2, 7]], dtype=np.int64)
+    a = ("groups_raw", raw)
+    b = B.canonical_groups([9, 5, 2], [2, 1, 3], [7, 10, 30])
+    assert B.result_fingerprint(a) == B.result_fingerprint(b)
+    c = ("groups_raw", np.array([[5, 1, 10], [2, 3, 31], [9, 2, 7]], dtype=np.int64))
+    assert B.result_fingerprint(a) != B.result_fingerprint(c)
+    assert B.result_fingerprint(("scalar", 3, 4)) == ("scalar", 3, 4)

@@ -40,6 +40,12 @@ def test_served_results_equal_queries_alone(setup, rate):
     assert s["requests"] == len(qs) and sum(rep.batch_sizes) == len(qs)
     assert np.all(rep.latencies_s > 0)
     assert s["p99_ms"] >= s["p50_ms"] > 0
+    # the same trace with answers handed over as they complete
+    fps = {}
+    srv = S.Server(tables, sizer, plain=plain, workers=2, hbm_budget=150e9)
+    _, rep2 = srv.serve(trace, on_result=lambda i, r: fps.__setitem__(i, B.result_fingerprint(r)))
+    srv.close()
+    assert [fps[i] for i in range(len(qs))] == [B.result_fingerprint(r) for r in alone]
 
 
 def test_budget_too_small_is_an_error(setup):
