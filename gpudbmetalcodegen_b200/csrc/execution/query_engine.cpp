@@ -1,5 +1,7 @@
 #include "query_engine.h"
 
+#include <algorithm>
+
 #include <chrono>
 #include <regex>
 #include <set>
@@ -39,7 +41,8 @@ std::string describePlan(const PreparedQuery& q) {
     }
     for (const auto& s : q.plan.sizing)
         o << "  sizing " << s.symbol << " after phase " << s.afterPhase << " from "
-          << (s.counterBuffer.empty() ? "'" + s.fallbackExpr + "'" : "counter " + s.counterBuffer) << "\n";
+          << (s.counterBuffer.empty() ? "'" + s.fallbackExpr + "'" : "counter " + s.counterBuffer)
+          << (s.minCounterBuffer.empty() ? "" : " (min with " + s.minCounterBuffer + ")") << "\n";
     return o.str();
 }
 
@@ -156,6 +159,14 @@ int runQuery(QueryContext& qc, PreparedQuery& q, int warmup, int measured, bool 
             if (!qc.ex.readBuffer(st.counterBuffer, &v, 8)) {
                 err = "sizing: counter '" + st.counterBuffer + "' unavailable";
                 return -2;
+            }
+            if (!st.minCounterBuffer.empty()) {
+                uint64_t w = 0;
+                if (!qc.ex.readBuffer(st.minCounterBuffer, &w, 8)) {
+                    err = "sizing: counter '" + st.minCounterBuffer + "' unavailable";
+                    return -2;
+                }
+                v = std::min(v, w);
             }
             qc.ex.registerSymbol(st.symbol, v);
         }

@@ -409,7 +409,13 @@ CudaSlotListScan::CudaSlotListScan(const std::string& listBuffer, const std::str
                                    const std::string& idxVar)
     : list_(listBuffer), count_(countBuffer), idxVar_(idxVar) {}
 
+void CudaSlotListScan::addGatherColumn(const std::string& paramName, const std::string& cudaType,
+                                       const std::string& table) {
+    gathers_.push_back({paramName, cudaType, table});
+}
+
 void CudaSlotListScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    for (const auto& g : gathers_) cg.addColumnParam(g.name, g.type, g.table, true);
     cg.addReadBufferParam(list_, "unsigned");
     cg.addReadBufferParam(count_, "unsigned long long");
     cg.addBufferLengthParam("len_" + list_, list_);
@@ -966,8 +972,50 @@ void CudaMaterialize::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addAtomicBufferParam(counterName_, "unsigned long long", "1");
     for (const auto& c : columns_) cg.addBufferParam(c.arrayName, c.type, capacityExpr_, false);
     cg.addSizeScalarParam("cap_" + counterName_, "long long", capacityExpr_);
-    cg.registerMaterializeOutput(counterName_);
-    for (const auto& c : columns_) cg.registerOutputColumn(c.displayName, c.arrayName, c.type);
+    if (!intermediate_) {
+        cg.registerMaterializeOutput(counterName_);
+        for (const auto& c : columns_) cg.registerOutputColumn(c.displayName, c.arrayName, c.type);
+    }
+    const bool ctaBuffered = intermediate_ && columns_.size() == 1 && cudaTypeBytes(columns_[0].type) == 4;
+    if (ctaBuffered) {
+        constexpr int kBuf = 2048;
+        const auto& c = columns_[0];
+        const int bo = cg.allocDynamicSmem(kBuf * 4 + 16);
+        cg.addLine(c.type + "* _mb_buf = reinterpret_cast<" + c.type + "*>(gpudb_smem + " + S(bo) + ");");
+        cg.addLine("unsigned* _mb_n = reinterpret_cast<unsigned*>(_mb_buf + " + S(kBuf) + ");");
+        cg.addLine("unsigned long long* _mb_base = reinterpret_cast<unsigned long long*>(_mb_buf + " + S(kBuf + 2) + ");");
+        cg.addLine("if (threadIdx.x == 0) *_mb_n = 0u;");
+        cg.addLine("__syncthreads();");
+        child_->produce(cg, [&]() {
+            cg.addLine("const unsigned _mp = atomicAdd(_mb_n, 1u);");
+            cg.addBlock("if (_mp < " + S(kBuf) + "u)", [&]() {
+                cg.addLine("_mb_buf[_mp] = (" + c.type + ")(" + c.valueExpr + ");");
+            }, " else {");
+            cg.increaseIndent();
+            cg.addLine("const unsigned long long _pos = atomicAdd(" + counterName_ + ", 1ull);");
+            cg.addLine("if (_pos < (unsigned long long)cap_" + counterName_ + ") " + c.arrayName + "[_pos] = (" + c.type +
+                       ")(" + c.valueExpr + ");");
+            cg.addLine("else gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+            cg.decreaseIndent();
+            cg.addLine("}");
+            consume();
+        });
+        cg.addComment("append this CTA's rows with one atomic");
+        cg.addLine("__syncthreads();");
+        cg.addBlock("", [&]() {
+            cg.addLine("const unsigned _mn = min(*_mb_n, " + S(kBuf) + "u);");
+            cg.addLine("if (threadIdx.x == 0) *_mb_base = _mn ? atomicAdd(" + counterName_ +
+                       ", (unsigned long long)_mn) : 0ull;");
+            cg.addLine("__syncthreads();");
+            cg.addBlock("for (unsigned _w = threadIdx.x; _w < _mn; _w += blockDim.x)", [&]() {
+                cg.addLine("const unsigned long long _pos = *_mb_base + _w;");
+                cg.addLine("if (_pos < (unsigned long long)cap_" + counterName_ + ") " + c.arrayName +
+                           "[_pos] = _mb_buf[_w];");
+                cg.addLine("else gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+            });
+        });
+        return;
+    }
     child_->produce(cg, [&]() {
         cg.addLine("const unsigned long long _pos = gpudb_warp_reserve(" + counterName_ + ", true);");
         cg.addBlock("if (_pos < (unsigned long long)cap_" + counterName_ + ")", [&]() {

@@ -111,11 +111,18 @@ private:
 class CudaSlotListScan : public CudaOperator {
 public:
     CudaSlotListScan(const std::string& listBuffer, const std::string& countBuffer, const std::string& idxVar = "i");
+    // Table columns the rows read at the listed positions (a gather: the
+    // list holds row indices of `table`).
+    void addGatherColumn(const std::string& paramName, const std::string& cudaType, const std::string& table);
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
 private:
     std::string list_, count_, idxVar_;
+    struct Gather {
+        std::string name, type, table;
+    };
+    std::vector<Gather> gathers_;
 };
 
 // Selection: if (predicate) consume(). Reference: metal_operators.cpp:63-69.
@@ -330,12 +337,17 @@ public:
                     const std::string& capacityExpr);
     void addColumn(const std::string& arrayName, const std::string& type, const std::string& valueExpr,
                    const std::string& displayName = "");
+    // An intermediate result read by a later phase, not the plan's output.
+    // Its (single, 4-byte) column is gathered per CTA in shared memory and
+    // appended with one atomic per CTA: rows keep no order.
+    void setIntermediate(bool on) { intermediate_ = on; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
 private:
     std::string counterName_, capacityExpr_;
     std::vector<Column> columns_;
+    bool intermediate_ = false;
 };
 
 // ------------------------------------------------------------------

@@ -97,7 +97,8 @@ std::string TuneConfig::toString() const {
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
-      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch;
+      << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
+      << ";split=" << (splitJoin ? 1 : 0);
     return o.str();
 }
 
@@ -124,6 +125,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "pf") t.scan.prefetchRows = std::stoi(v);
         else if (k == "vec") t.scan.vectorRows = std::stoi(v);
         else if (k == "l2pf") t.scan.l2Prefetch = std::stoi(v);
+        else if (k == "split") t.splitJoin = std::stoi(v) != 0;
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -265,7 +267,33 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         appendPhase(plan, "JT_build", std::move(bm), tune);
     }
     const std::string cap = "2 * max(jt_groups, 1)";
-    {
+    if (tune.splitJoin) {
+        // The probe only lists the matched rows; a second phase gathers
+        // their price / discount and aggregates. A matched row's slow work
+        // (gathers, hash insert) then never holds a staged tile, and the
+        // group table is sized by min(qualifying build keys, matched rows).
+        {
+            auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune);
+            auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+            auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
+            auto mt = std::make_unique<CudaMaterialize>(std::move(pr), "jm_n", "n_probe");
+            mt->addColumn("jm_rows", "unsigned", "(unsigned)_row");
+            mt->setIntermediate(true);
+            appendPhase(plan, "JT_probe", std::move(mt), tune);
+        }
+        {
+            auto ls = std::make_unique<CudaSlotListScan>("jm_rows", "jm_n");
+            ls->addGatherColumn("p_fk", "int", "probe");
+            ls->addGatherColumn("p_price", "long long", "probe");
+            ls->addGatherColumn("p_discount", "long long", "probe");
+            auto gb = std::make_unique<CudaHashGroupBy>(std::move(ls), "jg", "p_fk[i]", "int", cap, HashLayout::Linear,
+                                                        tune.maxProbe);
+            gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
+            gb->setWarpAggregate(tune.warpAggregate);
+            gb->setSlotList(true);
+            appendPhase(plan, "JT_group", std::move(gb), tune);
+        }
+    } else {
         auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune, true, {"p_price", "p_discount"});
         auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
         auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
@@ -287,9 +315,15 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
     }
     CudaQueryPlan::SizingStep st;
     st.symbol = "jt_groups";
-    st.afterPhase = 1;
-    if (given) st.fallbackExpr = std::to_string(groups);
-    else st.counterBuffer = "jb_distinct";
+    st.afterPhase = tune.splitJoin ? 2 : 1;
+    if (given) {
+        st.fallbackExpr = std::to_string(groups);
+    } else if (tune.splitJoin) {
+        st.counterBuffer = "jm_n";  // every group has a matched row ...
+        st.minCounterBuffer = "jb_distinct";  // ... and a qualifying build key
+    } else {
+        st.counterBuffer = "jb_distinct";
+    }
     plan.sizing.push_back(st);
     plan.decorate.push_back([](CudaResultSchema& rs) {
         rs.topk.keyName = "key";

@@ -80,6 +80,7 @@ struct CudaQueryPlan {
         std::string symbol;       // symbol registered before phase `afterPhase`
         int afterPhase = 0;       // phases [0, afterPhase) produce it
         std::string counterBuffer;// u64 buffer holding the exact value
+        std::string minCounterBuffer;  // optional second bound: the smaller of the two
         std::string fallbackExpr; // when no counter: a size expression
     };
     std::vector<SizingStep> sizing;
@@ -103,6 +104,7 @@ struct TuneConfig {
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
     int maxProbe = 128;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
+    bool splitJoin = false;       // join_topk: probe materialises matched rows, a second phase aggregates
     std::string toString() const;
     static TuneConfig parse(const std::string& s);  // "bs=512;scan=tma;tile=1024;stages=4;..."
 };
