@@ -53,8 +53,7 @@ SPACES = {
 SEEDS = {
     "q1": [{"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
-    "join_topk": [{"stages": "2", "warp": "0"}, {"tile": "1024", "warp": "0"}, {"split": "1", "stages": "2"},
-                  {"split": "1", "tile": "1024"}],
+    "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"}],
     "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"}],
 }

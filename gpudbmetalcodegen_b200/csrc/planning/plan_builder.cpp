@@ -310,6 +310,7 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         auto tk = std::make_unique<CudaTopK>(std::move(lscan), "jt_top", "(long long)(int)jg_keys[i]",
                                              "(long long)jg_revenue[i]", (int)k);
         auto& ph = appendPhase(plan, "JT_topk", std::move(tk), tune);
+        ph.minBlocksPerSM = 1;  // the register-resident top-k lists must not be capped by an occupancy hint
         ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});
         ph.extraBuffers.push_back({"jg_revenue", "unsigned long long", true, false});
     }
@@ -483,6 +484,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
         auto tk = std::make_unique<CudaTopK>(std::move(lscan), "mt_top", "(long long)mg_keys[i]", "(long long)mg_sum[i]",
                                              (int)k);
         auto& ph = appendPhase(plan, "MIXG_topk", std::move(tk), tune);
+        ph.minBlocksPerSM = 1;  // the register-resident top-k lists must not be capped by an occupancy hint
         ph.extraBuffers.push_back({"mg_keys", "unsigned long long", true, false});
         ph.extraBuffers.push_back({"mg_sum", "unsigned long long", true, false});
         plan.decorate.push_back([](CudaResultSchema& rs) { rs.topk.valueName = "sum"; });
