@@ -301,6 +301,16 @@ __device__ __forceinline__ bool gpudb_mbar_wait(unsigned long long* bar, unsigne
 // metal_plan_builder.cpp:1598-1610, 1968-1982); here the build runs on the
 // GPU with atomicCAS and the bound is a parameter.
 // ------------------------------------------------------------------
+// log2 of the slot count for `groups` expected groups (load factor <= 1/2,
+// at least 16 slots), computed on the device from counters an earlier
+// kernel produced; never above the allocation's log2max.
+__device__ __forceinline__ int gpudb_device_log2cap(unsigned long long groups, int log2max) {
+    const unsigned long long want = groups * 2ull > 16ull ? groups * 2ull : 16ull;
+    int l = 4;
+    while (l < log2max && (1ull << l) < want) ++l;
+    return l;
+}
+
 __device__ __forceinline__ unsigned long long gpudb_hash_slot(unsigned long long key, int log2cap) {
     return (key * 0x9E3779B97F4A7C15ull) >> (64 - log2cap);
 }

@@ -1104,14 +1104,56 @@ void CudaHashGroupBy::addAggregate(const std::string& name, const std::string& v
     aggs_.push_back({name, valueExpr});
 }
 
+void CudaHashGroupBy::setDeviceCapacity(const std::string& groupsExpr, const std::string& boundExpr,
+                                        const std::vector<std::string>& counters) {
+    devGroups_ = groupsExpr;
+    devBound_ = boundExpr;
+    devCounters_ = counters;
+}
+
+CudaHashInit::CudaHashInit(const std::string& tableName, const std::string& keyType, HashLayout layout,
+                           const std::vector<std::string>& aggNames, const std::string& groupsExpr,
+                           const std::string& boundExpr, const std::vector<std::string>& counters)
+    : table_(tableName), keyType_(keyType), layout_(layout), aggs_(aggNames), groups_(groupsExpr), bound_(boundExpr),
+      counters_(counters) {}
+
+void CudaHashInit::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const KeyOps ko = keyOps(keyType_, layout_);
+    const std::string cap = hashSlotsExpr(bound_);
+    cg.addBufferParam(table_ + "_keys", ko.store, cap, false, 0);
+    for (const auto& a : aggs_) cg.addBufferParam(table_ + "_" + a, "unsigned long long", cap, false, 0);
+    for (const auto& c : counters_) cg.addReadBufferParam(c, "unsigned long long");
+    cg.addSizeScalarParam(table_ + "_log2max", "int", hashLog2Expr(bound_));
+    cg.addLine("const int _hi_log2 = gpudb_device_log2cap((unsigned long long)(" + groups_ + "), " + table_ +
+               "_log2max);");
+    cg.addBlock("for (long long _w = tid; _w < (1ll << _hi_log2); _w += tpg)", [&]() {
+        cg.addLine(table_ + "_keys[_w] = (" + ko.store + ")(~(" + ko.store + ")0);");
+        for (const auto& a : aggs_) cg.addLine(table_ + "_" + a + "[_w] = 0ull;");
+    });
+    consume();
+}
+
+std::string CudaHashInit::describe() const { return "HashInit(" + table_ + ", slots for " + groups_ + ")"; }
+
 void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
     if (aggs_.empty()) throw std::runtime_error("CudaHashGroupBy: no aggregates");
     const KeyOps ko = keyOps(keyType_, layout_);
-    const std::string cap = hashSlotsExpr(capExpr_);
+    const bool dev = !devGroups_.empty();
+    const std::string cap = hashSlotsExpr(dev ? devBound_ : capExpr_);
     const std::string keys = table_ + "_keys";
-    cg.addHashMapParam(keys, ko.store, cap);
-    for (const auto& a : aggs_) cg.addAtomicBufferParam(table_ + "_" + a.name, "unsigned long long", cap);
-    cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    if (dev) {
+        // allocated for the bound, initialised by the table's HashInit phase
+        cg.addBufferParam(keys, ko.store, cap, false, 0);
+        for (const auto& a : aggs_) cg.addBufferParam(table_ + "_" + a.name, "unsigned long long", cap, false, 0);
+        for (const auto& c : devCounters_) cg.addReadBufferParam(c, "unsigned long long");
+        cg.addSizeScalarParam(table_ + "_log2max", "int", hashLog2Expr(devBound_));
+        cg.addLine("const int " + table_ + "_log2cap = gpudb_device_log2cap((unsigned long long)(" + devGroups_ + "), " +
+                   table_ + "_log2max);");
+    } else {
+        cg.addHashMapParam(keys, ko.store, cap);
+        for (const auto& a : aggs_) cg.addAtomicBufferParam(table_ + "_" + a.name, "unsigned long long", cap);
+        cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    }
     const int na = (int)aggs_.size();
     const int L = smemLog2_;
     const bool smem = L > 0 && ko.store == "unsigned long long";

@@ -413,6 +413,13 @@ public:
     // Record every slot when its group is created in <table>_slotlist
     // (count in <table>_nslots): later phases visit only used slots.
     void setSlotList(bool on) { slotList_ = on; }
+    // Device-sized table: the buffers are allocated for `boundExpr` groups
+    // (a host size expression) and not filled by the executor; the slot
+    // count is computed in the kernel from `groupsExpr`, device code over
+    // the u64 counter buffers `counters` that earlier phases produced. A
+    // CudaHashInit phase with the same arguments must run first.
+    void setDeviceCapacity(const std::string& groupsExpr, const std::string& boundExpr,
+                           const std::vector<std::string>& counters);
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
@@ -427,6 +434,27 @@ private:
     bool warpAgg_ = true;
     int smemLog2_ = 0;
     bool slotList_ = false;
+    std::string devGroups_, devBound_;
+    std::vector<std::string> devCounters_;
+};
+
+// Initialises the slots a device-sized group-by table will use (keys
+// empty, aggregates zero) from the same counters, so no host round trip
+// sizes the table between the phases that count and the one that groups.
+class CudaHashInit : public CudaOperator {
+public:
+    CudaHashInit(const std::string& tableName, const std::string& keyType, HashLayout layout,
+                 const std::vector<std::string>& aggNames, const std::string& groupsExpr,
+                 const std::string& boundExpr, const std::vector<std::string>& counters);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string table_, keyType_;
+    HashLayout layout_;
+    std::vector<std::string> aggs_;
+    std::string groups_, bound_;
+    std::vector<std::string> counters_;
 };
 
 // Top-k (value desc, key asc) of the consumed (key, value) pairs.

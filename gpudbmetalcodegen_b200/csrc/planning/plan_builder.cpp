@@ -281,6 +281,16 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
             mt->setIntermediate(true);
             appendPhase(plan, "JT_probe", std::move(mt), tune);
         }
+        // No host round trip sizes the group table: it is allocated for
+        // min(probe rows, build keys) groups and JT_init / JT_group derive
+        // its slot count on the device from the two counters.
+        const std::string devGroups = "min(__ldcg(jm_n), __ldcg(jb_distinct))";
+        const std::string bound = "2 * max(min(n_probe, max_b_key + 1), 1)";
+        const std::vector<std::string> counters = {"jm_n", "jb_distinct"};
+        appendPhase(plan, "JT_init",
+                    std::make_unique<CudaHashInit>("jg", "int", HashLayout::Linear, std::vector<std::string>{"revenue"},
+                                                   devGroups, bound, counters),
+                    tune);
         {
             auto ls = std::make_unique<CudaSlotListScan>("jm_rows", "jm_n");
             ls->addGatherColumn("p_fk", "int", "probe");
@@ -291,6 +301,7 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
             gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
             gb->setWarpAggregate(tune.warpAggregate);
             gb->setSlotList(true);
+            gb->setDeviceCapacity(devGroups, bound, counters);
             appendPhase(plan, "JT_group", std::move(gb), tune);
         }
     } else {
@@ -314,18 +325,14 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});
         ph.extraBuffers.push_back({"jg_revenue", "unsigned long long", true, false});
     }
-    CudaQueryPlan::SizingStep st;
-    st.symbol = "jt_groups";
-    st.afterPhase = tune.splitJoin ? 2 : 1;
-    if (given) {
-        st.fallbackExpr = std::to_string(groups);
-    } else if (tune.splitJoin) {
-        st.counterBuffer = "jm_n";  // every group has a matched row ...
-        st.minCounterBuffer = "jb_distinct";  // ... and a qualifying build key
-    } else {
-        st.counterBuffer = "jb_distinct";
+    if (!tune.splitJoin) {
+        CudaQueryPlan::SizingStep st;
+        st.symbol = "jt_groups";
+        st.afterPhase = 1;
+        if (given) st.fallbackExpr = std::to_string(groups);
+        else st.counterBuffer = "jb_distinct";
+        plan.sizing.push_back(st);
     }
-    plan.sizing.push_back(st);
     plan.decorate.push_back([](CudaResultSchema& rs) {
         rs.topk.keyName = "key";
         rs.topk.valueName = "revenue";

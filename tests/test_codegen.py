@@ -62,6 +62,17 @@ def test_join_topk_three_phases_and_sizing_step():
     assert "from '1000'" in given
 
 
+def test_split_join_sizes_its_group_table_on_the_device():
+    q = engine.Query("template=join_topk", "split=1")
+    phases = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
+    assert phases == ["JT_build", "JT_probe", "JT_init", "JT_group", "JT_topk"]
+    assert "sizing jt_groups" not in q.plan  # no host round trip between the phases
+    init = q.source.split("// === Phase 2: JT_init ===")[1].split("// === Phase 3")[0]
+    group = q.source.split("// === Phase 3: JT_group ===")[1].split("// === Phase 4")[0]
+    for body in (init, group):
+        assert "gpudb_device_log2cap((unsigned long long)(min(__ldcg(jm_n), __ldcg(jb_distinct))), jg_log2max)" in body
+
+
 def test_spec_errors_are_reported():
     with pytest.raises(GpudbError) as e:
         engine.Query("template=nope")

@@ -111,12 +111,33 @@ def test_join_topk_parity(ctx, tune):
     res, t = ctx.run("template=join_topk", tune)
     assert t.device_error == 0
     assert res.rows == top
-    if "split=1" in tune:  # sized by min(matched rows, qualifying build keys)
-        assert groups <= ctx.get_symbol("jt_groups") <= distinct
+    if "split=1" in tune:
+        # sized on the device from min(matched rows, qualifying build keys):
+        # no host sizing symbol; the table holds exactly the joined groups
+        assert int(ctx.read_buffer("jg_nslots", np.uint64, 1)[0]) == groups
+        assert int(ctx.read_buffer("jb_distinct", np.uint64, 1)[0]) == distinct
     else:
         assert ctx.get_symbol("jt_groups") == distinct
     res, _ = ctx.run("template=join_topk;k=32")
     assert res.rows == O.join_topk(d, p, k=32)[0]
+
+
+@pytest.mark.parametrize("ship_gt,od_lt", [(10**6, 1170), (1170, 0), (2555, 1170), (1170, 1170)])
+def test_split_join_device_sizing_edges(ctx, ship_gt, od_lt):
+    """The split plan sizes its group table on the device: no matched rows,
+    no qualifying build keys, very few matches, and the default case, each
+    against the oracle, run twice through the same buffers (a smaller
+    second query must not see the first one's groups)."""
+    d, p = load_join(ctx, 50_000, 300_000, seed=9)
+    spec = f"template=join_topk;ship_gt={ship_gt};od_lt={od_lt}"
+    for tune in ("split=1", "split=1;stages=2;occ=3"):
+        top, groups, _ = O.join_topk(d, p, ship_gt=ship_gt, od_lt=od_lt, k=10)
+        big, _ = ctx.run("template=join_topk;ship_gt=0", tune)
+        assert big.rows == O.join_topk(d, p, ship_gt=0, k=10)[0]
+        res, t = ctx.run(spec, tune)
+        assert t.device_error == 0
+        assert res.rows == top
+        assert int(ctx.read_buffer("jg_nslots", np.uint64, 1)[0]) == groups
 
 
 def test_join_topk_ties_break_by_key(ctx):
