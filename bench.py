@@ -761,27 +761,31 @@ def main():
         res, _ = ctx.run(q)
         verified = w.matches(res)
 
-    # the timed steps replay each plan segment as a CUDA graph (fills and
-    # kernels, captured during the warm-up); the kernels' own times come from
-    # a second, ungraphed pass with an event around every launch
+    # the timed steps are enqueued back to back (no host wait between
+    # them), each replaying the plan as a CUDA graph (fills and kernels,
+    # captured during the warm-up); device errors are read once after the
+    # last step. The kernels' own times come from a second, ungraphed pass
+    # with an event around every launch.
+    kernels = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
     ctx.set_use_graphs(not args.no_graphs)
     for _ in range(args.warmup):
-        ctx.run(q, collect=False)
+        ctx.enqueue(q)
+    ctx.sync()
     phase_acc, names = {}, []
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    launches = 0
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
-            _, t = ctx.run(q, collect=False)
-            launches += t.launches
+            ctx.enqueue(q)
         ev1.record(stream)
         ev1.synchronize()
+    ctx.sync()
     torch.cuda.synchronize()
+    launches = len(kernels) * args.steps
     step_ms = ev0.elapsed_time(ev1) / args.steps
     ctx.set_use_graphs(False)
     phase_steps = max(5, min(args.steps, 20))
@@ -797,7 +801,6 @@ def main():
     rows_total = w.rows() * world
     value = rows_total / (step_ms / 1e3)
 
-    kernels = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
     phase_ms = {(kernels[i] if i < len(kernels) else str(i)): v / phase_steps for i, v in phase_acc.items()}
     kernel = w.kernel_for(q.tune) if hasattr(w, "kernel_for") else w.kernel
     kms = phase_ms.get(kernel)

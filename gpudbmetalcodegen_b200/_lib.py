@@ -91,6 +91,8 @@ _SIGNATURES = [
     ("gpudb_query_algorithmic_bytes", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]),
     ("gpudb_query_run", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p),
                                   C.POINTER(Timing)]),
+    ("gpudb_query_enqueue", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gpudb_ctx_sync", C.c_int, [C.c_void_p, C.POINTER(C.c_uint)]),
     ("gpudb_result_shape", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     ("gpudb_result_column", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_int)]),
     ("gpudb_result_get_int", C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_int64),

@@ -392,6 +392,42 @@ int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gp
     })
 }
 
+int gpudb_query_enqueue(gpudb_ctx* ctx, gpudb_query* q) {
+    if (!ctx || !q) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    GPUDB_GUARD(ctx, {
+        cudaSetDevice(ctx->qc->ex.device());
+        gpudb::ExecutionResult r;
+        std::string err;
+        ctx->qc->ex.setSkipZeroInit(false);
+        struct Deferred {
+            gpudb::CudaGenericExecutor& ex;
+            explicit Deferred(gpudb::CudaGenericExecutor& e) : ex(e) { ex.setDeferSync(true); }
+            ~Deferred() { ex.setDeferSync(false); }
+        } deferred(ctx->qc->ex);
+        const int rc = gpudb::runQuery(*ctx->qc, *q->q, 1, 0, false, r, err);
+        if (rc != 0) return fail(ctx, mapStatus(rc), err);
+        return GPUDB_OK;
+    })
+}
+
+int gpudb_ctx_sync(gpudb_ctx* ctx, unsigned* device_error) {
+    if (!ctx) return GPUDB_E_INVALID;
+    if (device_error) *device_error = 0;
+    GPUDB_GUARD(ctx, {
+        cudaSetDevice(ctx->qc->ex.device());
+        unsigned bits = 0;
+        std::string err;
+        if (!ctx->qc->ex.syncErrors(bits, err)) return fail(ctx, GPUDB_E_CUDA, err);
+        if (device_error) *device_error = bits;
+        if (bits) {
+            char b[64];
+            snprintf(b, sizeof b, "device error word 0x%x", bits);
+            return fail(ctx, GPUDB_E_DEVICE, b);
+        }
+        return GPUDB_OK;
+    })
+}
+
 // ---------------------------------------------------------------------------
 // results
 // ---------------------------------------------------------------------------

@@ -64,6 +64,8 @@ CudaGenericExecutor::~CudaGenericExecutor() {
 }
 
 void CudaGenericExecutor::clearGraphs() {
+    // deferred replays may still be running on the stream
+    if (pendingErr_ && stream_ && !graphs_.empty()) cudaStreamSynchronize(stream_);
     for (auto& [_, g] : graphs_) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         if (g.graph) cudaGraphDestroy(g.graph);
@@ -373,8 +375,16 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
         error = "bad phase range";
         return -2;
     }
-    if (measured < 1) measured = 1;
+    // a deferred run is one untimed pass; timed runs (the max-key pass's
+    // among them) always complete here
+    const bool defer = deferSync_ && measured <= 0;
     if (warmup < 0) warmup = 0;
+    if (defer) {
+        measured = 0;
+        warmup = std::max(warmup, 1);
+    } else if (measured < 1) {
+        measured = 1;
+    }
     cudaSetDevice(device_);
     const DriverApi& api = driverApi();
 
@@ -440,7 +450,8 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
         return true;
     };
 
-    if (cudaMemsetAsync(errWord_, 0, sizeof(unsigned), stream_) != cudaSuccess) {
+    // the word still holds the bits of deferred runs until they are read
+    if (!pendingErr_ && cudaMemsetAsync(errWord_, 0, sizeof(unsigned), stream_) != cudaSuccess) {
         error = "cannot clear the device error word";
         return -5;
     }
@@ -512,14 +523,33 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
             }
         }
     }
+    if (defer) {
+        pendingErr_ = true;
+        return 0;
+    }
+    unsigned bits = 0;
+    if (!syncErrors(bits, error)) return -7;
+    out.deviceError |= bits;
+    return 0;
+}
+
+bool CudaGenericExecutor::syncErrors(unsigned& bits, std::string& error) {
     cudaError_t e = cudaMemcpyAsync(errHost_, errWord_, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) {
         error = cudaErr("kernel execution", e);
-        return -7;
+        return false;
     }
-    out.deviceError |= *errHost_;
-    return 0;
+    bits = *errHost_;
+    if (pendingErr_) {
+        // read: the next run starts from a clear word
+        pendingErr_ = false;
+        if (cudaMemsetAsync(errWord_, 0, sizeof(unsigned), stream_) != cudaSuccess) {
+            error = "cannot clear the device error word";
+            return false;
+        }
+    }
+    return true;
 }
 
 }  // namespace gpudb

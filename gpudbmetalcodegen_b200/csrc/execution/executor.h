@@ -79,6 +79,13 @@ public:
 
     void setSkipZeroInit(bool skip) { skipZeroInit_ = skip; }
     void setUseGraphs(bool on) { useGraphs_ = on; }
+    // Deferred completion: an untimed execute() returns once its work is enqueued,
+    // without waiting or reading the device error word; the bits of such
+    // runs accumulate until syncErrors() (or a waiting execute) reads them.
+    void setDeferSync(bool on) { deferSync_ = on; }
+    // Waits for the stream and returns (and clears) the accumulated device
+    // error bits; false if the stream itself failed.
+    bool syncErrors(unsigned& bits, std::string& error);
 
     // --- buffers -------------------------------------------------------------
     bool readBuffer(const std::string& name, void* host, size_t bytes);
@@ -129,6 +136,8 @@ private:
     unsigned* errHost_ = nullptr;
     bool skipZeroInit_ = false;
     bool useGraphs_ = false;
+    bool deferSync_ = false;
+    bool pendingErr_ = false;  // deferred runs whose error bits are unread
     CudaSizeResolver resolver_;
     std::unordered_map<std::string, Column> columns_;
     std::unordered_map<std::string, size_t> tableRows_;

@@ -114,14 +114,18 @@ int runQuery(QueryContext& qc, PreparedQuery& q, int warmup, int measured, bool 
     try {
         loadQuery(q);
         // max-key sizing symbols referenced by any size expression
-        static const std::regex re("max_([A-Za-z][A-Za-z0-9_]*)");
-        std::set<std::string> cols;
-        for (const auto& ph : q.cg.getPhases())
-            for (const auto& b : ph.bindings) {
-                for (std::sregex_iterator it(b.sizeExpr.begin(), b.sizeExpr.end(), re), end; it != end; ++it)
-                    cols.insert((*it)[1]);
-            }
-        for (const auto& c : cols) registerMaxKey(qc, c);
+        if (!q.maxKeyColumnsFound) {
+            static const std::regex re("max_([A-Za-z][A-Za-z0-9_]*)");
+            std::set<std::string> cols;
+            for (const auto& ph : q.cg.getPhases())
+                for (const auto& b : ph.bindings) {
+                    for (std::sregex_iterator it(b.sizeExpr.begin(), b.sizeExpr.end(), re), end; it != end; ++it)
+                        cols.insert((*it)[1]);
+                }
+            q.maxKeyColumns.assign(cols.begin(), cols.end());
+            q.maxKeyColumnsFound = true;
+        }
+        for (const auto& c : q.maxKeyColumns) registerMaxKey(qc, c);
     } catch (const std::exception& e) {
         err = e.what();
         return -2;

@@ -23,6 +23,10 @@ struct PreparedQuery {
     std::vector<std::string> kernelNames;
     std::shared_ptr<RuntimeCompiler::CompiledQuery> compiled;
     double planMs = 0, codegenMs = 0, compileMs = 0;
+    // columns whose max-key symbol a size expression references (found
+    // once, on the first run)
+    std::vector<std::string> maxKeyColumns;
+    bool maxKeyColumnsFound = false;
 };
 
 // Everything that lives as long as a gpudb_ctx.

@@ -293,6 +293,22 @@ class Context:
                 self._lib.gpudb_result_free(res)
         return out, timing
 
+    def enqueue(self, spec_or_query, tune: str = "") -> None:
+        """Enqueue one execution and return without waiting (no timing, no
+        result). Device errors surface at the next sync() or run()."""
+        q = spec_or_query if isinstance(spec_or_query, Query) else self.prepare(spec_or_query, tune)
+        check(self._lib.gpudb_query_enqueue(self.handle, q.handle), self.handle)
+
+    def sync(self) -> None:
+        """Wait for enqueued executions; raises GpudbError (status
+        GPUDB_E_DEVICE, `device_error` set) if any raised a device error."""
+        bits = C.c_uint()
+        st = self._lib.gpudb_ctx_sync(self.handle, C.byref(bits))
+        if st != 0:
+            err = GpudbError(st, _lib.last_error(self.handle))
+            err.device_error = bits.value  # type: ignore[attr-defined]
+            raise err
+
     def algorithmic_bytes(self, query: Query) -> int:
         v = C.c_longlong()
         check(self._lib.gpudb_query_algorithmic_bytes(self.handle, query.handle, C.byref(v)), self.handle)

@@ -50,6 +50,20 @@ int gpudb_query_algorithmic_bytes(gpudb_ctx* ctx, gpudb_query* q, long long* byt
 int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gpudb_result** result,
                     gpudb_timing* timing);
 
+/* Enqueue one execution on the context's stream and return without
+ * waiting for it: no timing, no collection. Sizing passes that need a
+ * host round trip still wait at their counter reads; a plan without them
+ * runs as one stream-ordered launch (a CUDA graph replay when graphs are
+ * on), so consecutive enqueues keep the GPU busy back to back. Device
+ * errors accumulate until gpudb_ctx_sync (or the next gpudb_query_run)
+ * reads them. The reference runs one blocking execution per invocation
+ * (MetalGenericExecutor::execute); this is the pipelined form of it. */
+int gpudb_query_enqueue(gpudb_ctx* ctx, gpudb_query* q);
+/* Wait for everything enqueued on the context's stream; *device_error
+ * (may be NULL) receives the accumulated device error bits, which are
+ * then cleared. Returns GPUDB_E_DEVICE when any bit was set. */
+int gpudb_ctx_sync(gpudb_ctx* ctx, unsigned* device_error);
+
 /* ---- results (reference: GenericResult, metal_result_collector.h:19-38) */
 int gpudb_result_shape(gpudb_result* r, int* ncols, long long* nrows);
 int gpudb_result_column(gpudb_result* r, int col, char* name, size_t cap, int* type);

@@ -161,6 +161,35 @@ def test_join_topk_learned_size_overflow_is_reported(ctx):
     assert e.value.timing.device_error & DEVERR_HASH_OVERFLOW
 
 
+def test_enqueue_pipelines_runs_and_reports_errors_at_sync(ctx):
+    """Enqueued executions run back to back without a host wait; a device
+    error raised by one of them survives later clean runs until sync()
+    reads it, and sync() clears it."""
+    d, p = load_join(ctx, 200_000, 800_000)
+    top = O.join_topk(d, p, k=10)[0]
+    ctx.set_use_graphs(True)
+    try:
+        for tune in ("split=1", "split=1;stages=2;occ=3", ""):
+            q = ctx.prepare("template=join_topk", tune)
+            for _ in range(5):
+                ctx.enqueue(q)
+            ctx.sync()
+            res, t = ctx.run(q)
+            assert res.rows == top and t.device_error == 0
+        bad = ctx.prepare("template=join_topk;groups=4")
+        ok = ctx.prepare("template=join_topk", "split=1")
+        ctx.enqueue(bad)
+        ctx.enqueue(ok)
+        with pytest.raises(GpudbError) as e:
+            ctx.sync()
+        assert e.value.status == -7 and e.value.device_error & DEVERR_HASH_OVERFLOW
+        ctx.sync()
+        res, t = ctx.run(ok)
+        assert res.rows == top and t.device_error == 0
+    finally:
+        ctx.set_use_graphs(False)
+
+
 def test_max_key_pass(ctx):
     d, _ = load_join(ctx, 123_457, 1000)
     assert ctx.register_max_key("b_key") == O.max_i32(d["b_key"]) == 123_457
