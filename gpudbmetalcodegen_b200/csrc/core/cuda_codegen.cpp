@@ -99,6 +99,7 @@ void CudaCodegen::setPhaseDynamicSmem(int b) { cur("setPhaseDynamicSmem").dynami
 void CudaCodegen::setPhaseTileRows(int r) { cur("setPhaseTileRows").tileRows = r; }
 void CudaCodegen::setPhaseRowsPerThread(int r) { cur("setPhaseRowsPerThread").rowsPerThread = r > 0 ? r : 1; }
 void CudaCodegen::setPhaseMinBlocksPerSM(int n) { cur("setPhaseMinBlocksPerSM").minBlocksPerSM = n > 0 ? n : 1; }
+void CudaCodegen::setPhaseSmemCarveout(int percent) { cur("setPhaseSmemCarveout").smemCarveout = percent; }
 int CudaCodegen::currentThreadgroupSize() const {
     if (current_ < 0) throw std::runtime_error("currentThreadgroupSize: no active phase");
     return phases_[current_].threadgroupSize;

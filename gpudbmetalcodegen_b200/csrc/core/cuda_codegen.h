@@ -80,6 +80,7 @@ public:
     void setPhaseTileRows(int rows);
     void setPhaseRowsPerThread(int rows);
     void setPhaseMinBlocksPerSM(int n);
+    void setPhaseSmemCarveout(int percent);
     int currentThreadgroupSize() const;
 
     // ---- parameters ----------------------------------------------------
@@ -139,6 +140,7 @@ public:
         int tileRows = 0;
         int rowsPerThread = 1;
         int minBlocksPerSM = 1;
+        int smemCarveout = -1;  // preferred carveout percent, -1 = driver default
         std::vector<CudaParamBinding> bindings;
     };
     const std::vector<PhaseInfo>& getPhases() const { return phases_; }

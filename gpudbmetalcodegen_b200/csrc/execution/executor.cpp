@@ -271,6 +271,18 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
         }
         smemConfigured_[l.fn] = (int)l.smem;
     }
+    if (ph.smemCarveout >= 0 && l.smem > 0) {
+        auto cv = carveoutSet_.find(l.fn);
+        if (cv == carveoutSet_.end() || cv->second != ph.smemCarveout) {
+            const CUresult r = api.cuFuncSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT,
+                                                      ph.smemCarveout);
+            if (r != CUDA_SUCCESS) {
+                error = "phase '" + ph.name + "': cannot set the shared-memory carveout (" + cuErrorString(r) + ")";
+                return false;
+            }
+            carveoutSet_[l.fn] = ph.smemCarveout;
+        }
+    }
     int occ = 0;
     const CUresult r = api.cuOccupancyMaxActiveBlocksPerMultiprocessor(&occ, l.fn, (int)l.block, l.smem);
     if (r != CUDA_SUCCESS || occ <= 0) {

@@ -146,6 +146,7 @@ private:
     std::unordered_map<std::string, long long> scalarInts_;
     std::unordered_map<std::string, double> scalarFloats_;
     std::map<CUfunction, int> smemConfigured_;
+    std::map<CUfunction, int> carveoutSet_;
     std::vector<cudaEvent_t> events_;
     struct GraphEntry {
         cudaGraph_t graph = nullptr;

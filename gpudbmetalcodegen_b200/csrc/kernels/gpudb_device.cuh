@@ -508,11 +508,11 @@ __device__ __forceinline__ void gpudb_topk_push(long long (&vv)[K], long long (&
 }
 
 // Merge the 32 lanes' sorted lists into the warp's best K, in order, by K
-// rounds of a shuffle arg-max over the lanes' list heads. Every lane ends
-// with the merged list in (ov, ok). Full warp must participate.
+// rounds of a shuffle arg-max over the lanes' list heads (any K). Every
+// lane ends with the merged list in (ov, ok). Full warp must participate.
 template <int K>
-__device__ __forceinline__ void gpudb_topk_warp_merge(const long long (&vv)[K], const long long (&kk)[K],
-                                                      long long (&ov)[K], long long (&ok)[K]) {
+__device__ __forceinline__ void gpudb_topk_warp_merge_rounds(const long long (&vv)[K], const long long (&kk)[K],
+                                                             long long (&ov)[K], long long (&ok)[K]) {
     const unsigned lane = threadIdx.x & 31u;
     int head = 0;
 #pragma unroll 1
@@ -544,5 +544,81 @@ __device__ __forceinline__ void gpudb_topk_warp_merge(const long long (&vv)[K], 
                 ok[i] = bk;
             }
         if ((int)lane == bl && head < K) head++;
+    }
+}
+
+// A warp's best K (K <= 32) held one entry per lane: lane j holds the
+// j-th best. Offer one entry per lane: a ballot keeps those better than
+// the current K-th best, and each is inserted by one more ballot (its rank
+// = the entries better than it) and a shift of the lanes below it. Returns
+// the ballot of offered entries that beat the K-th best. Full warp.
+template <int K>
+__device__ __forceinline__ unsigned gpudb_topk_warp_offer(long long& rv, long long& rk, long long cv, long long ck) {
+    static_assert(K >= 1 && K <= 32, "a warp holds at most 32 entries");
+    const int lane = (int)(threadIdx.x & 31u);
+    const long long tv = __shfl_sync(0xffffffffu, rv, K - 1), tk = __shfl_sync(0xffffffffu, rk, K - 1);
+    const unsigned any = __ballot_sync(0xffffffffu, gpudb_topk_better(cv, ck, tv, tk));
+    if (!any) return 0u;
+    const long long hv = __shfl_sync(0xffffffffu, rv, 0), hk = __shfl_sync(0xffffffffu, rk, 0);
+    if (hv == GPUDB_TOPK_NONE_VAL && hk == GPUDB_TOPK_NONE_KEY && __popc(any) > 2) {
+        // empty list, several entries: a bitonic sort of the 32 offered
+        // entries (best first) gives the list at once
+        long long v = cv, k = ck;
+#pragma unroll
+        for (int w = 2; w <= 32; w <<= 1) {
+#pragma unroll
+            for (int j = w >> 1; j > 0; j >>= 1) {
+                const long long pv = __shfl_xor_sync(0xffffffffu, v, j), pk = __shfl_xor_sync(0xffffffffu, k, j);
+                const bool better = gpudb_topk_better(v, k, pv, pk);
+                // descending runs keep the better entry at the lower lane
+                const bool keep = (((lane & j) == 0) == ((lane & w) == 0)) ? better : !better;
+                if (!keep) {
+                    v = pv;
+                    k = pk;
+                }
+            }
+        }
+        rv = lane < K ? v : GPUDB_TOPK_NONE_VAL;
+        rk = lane < K ? k : GPUDB_TOPK_NONE_KEY;
+        return any;
+    }
+    unsigned m = any;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1u;
+        const long long xv = __shfl_sync(0xffffffffu, cv, src), xk = __shfl_sync(0xffffffffu, ck, src);
+        const int pos = __popc(__ballot_sync(0xffffffffu, lane < K && gpudb_topk_better(rv, rk, xv, xk)));
+        if (pos >= K) continue;  // the K-th best rose past it meanwhile
+        const long long uv = __shfl_up_sync(0xffffffffu, rv, 1), uk = __shfl_up_sync(0xffffffffu, rk, 1);
+        if (lane == pos) {
+            rv = xv;
+            rk = xk;
+        } else if (lane > pos && lane < K) {
+            rv = uv;
+            rk = uk;
+        }
+    }
+    return any;
+}
+
+// Same result for K <= 32 with far fewer instructions when most entries
+// cannot enter: round r offers every lane's r-th entry to the warp's
+// one-entry-per-lane list; the lanes' lists are sorted, so the first round
+// in which no entry beats the K-th best ends the merge.
+template <int K>
+__device__ __forceinline__ void gpudb_topk_warp_merge(const long long (&vv)[K], const long long (&kk)[K],
+                                                      long long (&ov)[K], long long (&ok)[K]) {
+    if constexpr (K > 32) {
+        gpudb_topk_warp_merge_rounds<K>(vv, kk, ov, ok);
+    } else {
+        long long rv = GPUDB_TOPK_NONE_VAL, rk = GPUDB_TOPK_NONE_KEY;
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+            if (!gpudb_topk_warp_offer<K>(rv, rk, vv[r], kk[r])) break;
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            ov[i] = __shfl_sync(0xffffffffu, rv, i);
+            ok[i] = __shfl_sync(0xffffffffu, rk, i);
+        }
     }
 }

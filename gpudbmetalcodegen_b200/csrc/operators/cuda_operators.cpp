@@ -414,16 +414,29 @@ void CudaSlotListScan::addGatherColumn(const std::string& paramName, const std::
     gathers_.push_back({paramName, cudaType, table});
 }
 
-void CudaSlotListScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+void CudaSlotListScan::addListColumn(const std::string& bufferName, const std::string& cudaType,
+                                     const std::string& varName) {
+    listColumns_.push_back({bufferName, cudaType, varName});
+}
+
+std::string CudaSlotListScan::declareList(CudaCodegen& cg) const {
     for (const auto& g : gathers_) cg.addColumnParam(g.name, g.type, g.table, true);
+    for (const auto& c : listColumns_) cg.addReadBufferParam(c.buffer, c.type);
     cg.addReadBufferParam(list_, "unsigned");
     cg.addReadBufferParam(count_, "unsigned long long");
     cg.addBufferLengthParam("len_" + list_, list_);
+    return "(long long)min(__ldcg(" + count_ + "), (unsigned long long)len_" + list_ + ")";
+}
+
+void CudaSlotListScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const std::string n = declareList(cg);
     const std::string& i = idxVar_;
-    cg.addLine("const long long _sl_n = (long long)min(__ldcg(" + count_ + "), (unsigned long long)len_" + list_ + ");");
+    cg.addLine("const long long _sl_n = " + n + ";");
     cg.addBlock("for (long long _sl = tid; _sl < _sl_n; _sl += tpg)", [&]() {
         cg.addLine("const long long " + i + " = (long long)__ldcg(" + list_ + " + _sl);");
         cg.addLine("const long long _row = " + i + "; (void)_row;");
+        for (const auto& c : listColumns_)
+            cg.addLine("const " + c.type + " " + c.var + " = __ldcg(" + c.buffer + " + _sl);");
         consume();
     });
 }
@@ -518,6 +531,17 @@ void CudaBitmapProbe::produce(CudaCodegen& cg, ConsumerFn consume) {
         cg.addIf(anti_ ? "!(" + inb + " && " + t + ")" : "(" + inb + ") && " + t, [&]() { consume(); });
     });
     if (hint >= 0) cg.popScanHint();
+    if (!popcount_.empty()) {
+        cg.addAtomicBufferParam(popcount_, "unsigned long long", "1");
+        cg.addComment("distinct keys of " + bitmapName_ + ": popcount of a grid-stride share of its words, one atomic per warp");
+        cg.addBlock("", [&]() {
+            cg.addLine("unsigned long long _pc = 0ull;");
+            cg.addLine("for (long long _w = tid; _w < len_" + bitmapName_ + "; _w += tpg) _pc += (unsigned long long)__popc(__ldg(" +
+                       bitmapName_ + " + _w));");
+            cg.addLine("_pc = gpudb_warp_sum_u64(_pc);");
+            cg.addLine("if ((threadIdx.x & 31u) == 0u && _pc) atomicAdd(" + popcount_ + ", _pc);");
+        });
+    }
 }
 
 std::string CudaBitmapProbe::describe() const {
@@ -976,26 +1000,38 @@ void CudaMaterialize::produce(CudaCodegen& cg, ConsumerFn consume) {
         cg.registerMaterializeOutput(counterName_);
         for (const auto& c : columns_) cg.registerOutputColumn(c.displayName, c.arrayName, c.type);
     }
-    const bool ctaBuffered = intermediate_ && columns_.size() == 1 && cudaTypeBytes(columns_[0].type) == 4;
+    bool ctaBuffered = intermediate_ && !columns_.empty() && columns_.size() <= 2;
+    for (const auto& c : columns_) ctaBuffered = ctaBuffered && cudaTypeBytes(c.type) == 4;
     if (ctaBuffered) {
-        constexpr int kBuf = 2048;
-        const auto& c = columns_[0];
-        const int bo = cg.allocDynamicSmem(kBuf * 4 + 16);
-        cg.addLine(c.type + "* _mb_buf = reinterpret_cast<" + c.type + "*>(gpudb_smem + " + S(bo) + ");");
-        cg.addLine("unsigned* _mb_n = reinterpret_cast<unsigned*>(_mb_buf + " + S(kBuf) + ");");
-        cg.addLine("unsigned long long* _mb_base = reinterpret_cast<unsigned long long*>(_mb_buf + " + S(kBuf + 2) + ");");
+        // 8 KB of shared memory: 2048 rows of one column or 1024 of two
+        const int nc = (int)columns_.size();
+        const int kBuf = 2048 / nc;
+        const int bo = cg.allocDynamicSmem(kBuf * 4 * nc + 16);
+        for (int k = 0; k < nc; k++)
+            cg.addLine(columns_[k].type + "* _mb_buf" + S(k) + " = reinterpret_cast<" + columns_[k].type +
+                       "*>(gpudb_smem + " + S(bo + k * kBuf * 4) + ");");
+        cg.addLine("unsigned* _mb_n = reinterpret_cast<unsigned*>(gpudb_smem + " + S(bo + nc * kBuf * 4) + ");");
+        cg.addLine("unsigned long long* _mb_base = reinterpret_cast<unsigned long long*>(gpudb_smem + " +
+                   S(bo + nc * kBuf * 4 + 8) + ");");
         cg.addLine("if (threadIdx.x == 0) *_mb_n = 0u;");
         cg.addLine("__syncthreads();");
         child_->produce(cg, [&]() {
             cg.addLine("const unsigned _mp = atomicAdd(_mb_n, 1u);");
             cg.addBlock("if (_mp < " + S(kBuf) + "u)", [&]() {
-                cg.addLine("_mb_buf[_mp] = (" + c.type + ")(" + c.valueExpr + ");");
+                for (int k = 0; k < nc; k++)
+                    cg.addLine("_mb_buf" + S(k) + "[_mp] = (" + columns_[k].type + ")(" + columns_[k].valueExpr + ");");
             }, " else {");
             cg.increaseIndent();
+            cg.addComment("the CTA's buffer is full: this row goes straight to the list");
             cg.addLine("const unsigned long long _pos = atomicAdd(" + counterName_ + ", 1ull);");
-            cg.addLine("if (_pos < (unsigned long long)cap_" + counterName_ + ") " + c.arrayName + "[_pos] = (" + c.type +
-                       ")(" + c.valueExpr + ");");
-            cg.addLine("else gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+            cg.addBlock("if (_pos < (unsigned long long)cap_" + counterName_ + ")", [&]() {
+                for (const auto& c : columns_)
+                    cg.addLine(c.arrayName + "[_pos] = (" + c.type + ")(" + c.valueExpr + ");");
+            }, " else {");
+            cg.increaseIndent();
+            cg.addLine("gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+            cg.decreaseIndent();
+            cg.addLine("}");
             cg.decreaseIndent();
             cg.addLine("}");
             consume();
@@ -1009,9 +1045,14 @@ void CudaMaterialize::produce(CudaCodegen& cg, ConsumerFn consume) {
             cg.addLine("__syncthreads();");
             cg.addBlock("for (unsigned _w = threadIdx.x; _w < _mn; _w += blockDim.x)", [&]() {
                 cg.addLine("const unsigned long long _pos = *_mb_base + _w;");
-                cg.addLine("if (_pos < (unsigned long long)cap_" + counterName_ + ") " + c.arrayName +
-                           "[_pos] = _mb_buf[_w];");
-                cg.addLine("else gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+                cg.addBlock("if (_pos < (unsigned long long)cap_" + counterName_ + ")", [&]() {
+                    for (int k = 0; k < nc; k++)
+                        cg.addLine(columns_[k].arrayName + "[_pos] = _mb_buf" + S(k) + "[_w];");
+                }, " else {");
+                cg.increaseIndent();
+                cg.addLine("gpudb_set_error(gpudb_err, GPUDB_ERR_CAPACITY);");
+                cg.decreaseIndent();
+                cg.addLine("}");
             });
         });
         return;
@@ -1288,6 +1329,10 @@ void CudaTopK::produce(CudaCodegen& cg, ConsumerFn consume) {
     cg.addBufferParam(out_ + "_pkeys", "long long", S((long long)k_ * maxBlocks_), false);
     cg.addBufferParam(out_ + "_pvals", "long long", S((long long)k_ * maxBlocks_), false);
     cg.addAtomicBufferParam(out_ + "_ticket", "unsigned", "1");
+    if (auto* list = dynamic_cast<CudaSlotListScan*>(child_.get())) {
+        produceOverList(cg, *list, consume);
+        return;
+    }
     cg.addLine("long long _tk_v[" + K + "], _tk_k[" + K + "];");
     cg.addLine("#pragma unroll");
     cg.addLine("for (int _q = 0; _q < " + K + "; ++_q) { _tk_v[_q] = GPUDB_TOPK_NONE_VAL; _tk_k[_q] = GPUDB_TOPK_NONE_KEY; }");
@@ -1341,6 +1386,112 @@ void CudaTopK::produce(CudaCodegen& cg, ConsumerFn consume) {
             });
             cg.addLine(out_ + "_count[0] = _cnt;");
             cg.addLine(out_ + "_ticket[0] = 0u;  // self-reset for the next launch");
+        });
+    });
+    auto& rs = cg.resultSchema();
+    rs.kind = CudaResultSchema::TOPK;
+    rs.topk.keyBuffer = out_ + "_keys";
+    rs.topk.valueBuffer = out_ + "_vals";
+    rs.topk.countBuffer = out_ + "_count";
+    rs.topk.k = k_;
+}
+
+// Top-k over a slot list (the groups a hash group-by created): every warp
+// walks the list 32 entries at a time and keeps its best K one per lane
+// (lane j holds the j-th best), so a thread carries two values instead of
+// two K-lists and an entry costs one ballot unless it beats the warp's
+// K-th best. Warps' lists meet in shared memory, blocks' lists in global
+// memory, and the last block to finish merges those the same way. A full
+// list's K-th value is a floor: K entries are at least that good, so an
+// entry valued below the highest such floor cannot enter and is never
+// offered to the block and grid merges (values equal to it still are).
+void CudaTopK::produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, ConsumerFn consume) {
+    const std::string K = S(k_);
+    const std::string n = list.declareList(cg);
+    const std::string& i = list.indexVar();
+    // highest full-list floor of all blocks, as value ^ sign bit (0 = none)
+    cg.addAtomicBufferParam(out_ + "_floor", "unsigned long long", "1");
+    cg.addLine("__shared__ unsigned long long _ts_floor;");
+    cg.addLine("if (threadIdx.x == 0) _ts_floor = 0ull;");
+    cg.addLine("__syncthreads();");
+    cg.addLine("const int _tl = (int)(threadIdx.x & 31u);");
+    cg.addLine("long long _tr_v = GPUDB_TOPK_NONE_VAL, _tr_k = GPUDB_TOPK_NONE_KEY;");
+    cg.addLine("const long long _tl_n = " + n + ";");
+    cg.addBlock("for (long long _tb = (tid >> 5) * 32; _tb < _tl_n; _tb += (tpg >> 5) * 32)", [&]() {
+        cg.addLine("long long _tc_v = GPUDB_TOPK_NONE_VAL, _tc_k = GPUDB_TOPK_NONE_KEY;");
+        cg.addBlock("if (_tb + _tl < _tl_n)", [&]() {
+            cg.addLine("const long long " + i + " = (long long)__ldcg(" + list.listBuffer() + " + _tb + _tl);");
+            cg.addLine("const long long _row = " + i + "; (void)_row;");
+            cg.addLine("_tc_v = (long long)(" + valueExpr_ + ");");
+            cg.addLine("_tc_k = (long long)(" + keyExpr_ + ");");
+            consume();
+        });
+        cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tc_v, _tc_k);");
+    });
+    cg.addLine("__shared__ long long _ts_v[32 * " + K + "], _ts_k[32 * " + K + "];");
+    cg.addLine("__shared__ bool _t_last;");
+    // (the biased floor of a full list, or 0)
+    const std::string fullFloor = "(_tl == " + S(k_ - 1) + " && !(_tr_k == GPUDB_TOPK_NONE_KEY && _tr_v == "
+                                  "GPUDB_TOPK_NONE_VAL) ? ((unsigned long long)_tr_v ^ 0x8000000000000000ull) : 0ull)";
+    // every warp's list -> warp 0 holds the block's best K
+    auto blockMerge = [&]() {
+        cg.addBlock("if (_tl < " + K + ")", [&]() {
+            cg.addLine("_ts_v[(threadIdx.x >> 5) * " + K + " + _tl] = _tr_v;");
+            cg.addLine("_ts_k[(threadIdx.x >> 5) * " + K + " + _tl] = _tr_k;");
+            cg.addLine("const unsigned long long _fl = " + fullFloor + ";");
+            cg.addLine("if (_fl > _ts_floor) atomicMax(&_ts_floor, _fl);");
+        });
+        cg.addLine("__syncthreads();");
+        cg.addBlock("if (threadIdx.x < 32u)", [&]() {
+            cg.addLine("_tr_v = GPUDB_TOPK_NONE_VAL; _tr_k = GPUDB_TOPK_NONE_KEY;");
+            cg.addLine("const long long _tfv = (long long)(_ts_floor ^ 0x8000000000000000ull);");
+            cg.addLine("const int _tn = (int)(blockDim.x >> 5) * " + K + ";");
+            cg.addBlock("for (int _e0 = 0; _e0 < _tn; _e0 += 32)", [&]() {
+                cg.addLine("const int _e = _e0 + _tl;");
+                cg.addLine("const bool _tin = _e < _tn && _ts_v[_e] >= _tfv;");
+                cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
+                cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ts_v[_e] : GPUDB_TOPK_NONE_VAL, "
+                           "_tin ? _ts_k[_e] : GPUDB_TOPK_NONE_KEY);");
+            });
+        });
+    };
+    blockMerge();
+    cg.addBlock("if (threadIdx.x < 32u)", [&]() {
+        cg.addBlock("if (_tl < " + K + ")", [&]() {
+            cg.addLine(out_ + "_pvals[blockIdx.x * " + K + " + _tl] = _tr_v;");
+            cg.addLine(out_ + "_pkeys[blockIdx.x * " + K + " + _tl] = _tr_k;");
+            cg.addLine("const unsigned long long _fl = " + fullFloor + ";");
+            cg.addLine("if (_fl) atomicMax(" + out_ + "_floor, _fl);");
+            cg.addLine("__threadfence();");
+        });
+        cg.addLine("__syncwarp();");
+        cg.addLine("if (_tl == 0) _t_last = (atomicAdd(" + out_ + "_ticket, 1u) == gridDim.x - 1u);");
+    });
+    cg.addLine("__syncthreads();");
+    cg.addBlock("if (_t_last)", [&]() {
+        cg.addLine("__threadfence();");
+        cg.addLine("_tr_v = GPUDB_TOPK_NONE_VAL; _tr_k = GPUDB_TOPK_NONE_KEY;");
+        cg.addLine("const long long _tgf = (long long)(__ldcg(" + out_ + "_floor) ^ 0x8000000000000000ull);");
+        cg.addLine("const int _tg = (int)gridDim.x * " + K + ";");
+        cg.addBlock("for (int _e0 = (int)(threadIdx.x & ~31u); _e0 < _tg; _e0 += (int)blockDim.x)", [&]() {
+            cg.addLine("const int _e = _e0 + _tl;");
+            cg.addLine("const long long _ev = _e < _tg ? __ldcg(" + out_ + "_pvals + _e) : GPUDB_TOPK_NONE_VAL;");
+            cg.addLine("const bool _tin = _e < _tg && _ev >= _tgf;");
+            cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
+            cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ev : GPUDB_TOPK_NONE_VAL, "
+                       "_tin ? __ldcg(" + out_ + "_pkeys + _e) : GPUDB_TOPK_NONE_KEY);");
+        });
+        // this block's own floor stays valid: its K entries are among those offered
+        blockMerge();
+        cg.addBlock("if (threadIdx.x < 32u)", [&]() {
+            cg.addLine("const bool _tf = _tl < " + K + " && !(_tr_k == GPUDB_TOPK_NONE_KEY && _tr_v == GPUDB_TOPK_NONE_VAL);");
+            cg.addLine("const unsigned _tm = __ballot_sync(0xffffffffu, _tf);");
+            cg.addLine("if (_tf) { " + out_ + "_vals[_tl] = _tr_v; " + out_ + "_keys[_tl] = _tr_k; }");
+            cg.addBlock("if (_tl == 0)", [&]() {
+                cg.addLine(out_ + "_count[0] = (unsigned long long)__popc(_tm);");
+                cg.addLine(out_ + "_ticket[0] = 0u;  // self-reset for the next launch");
+                cg.addLine(out_ + "_floor[0] = 0ull;");
+            });
         });
     });
     auto& rs = cg.resultSchema();

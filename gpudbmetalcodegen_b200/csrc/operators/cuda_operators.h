@@ -114,8 +114,17 @@ public:
     // Table columns the rows read at the listed positions (a gather: the
     // list holds row indices of `table`).
     void addGatherColumn(const std::string& paramName, const std::string& cudaType, const std::string& table);
+    // A buffer written next to the list (same positions): its entry for
+    // the current position is read into the local `varName`.
+    void addListColumn(const std::string& bufferName, const std::string& cudaType, const std::string& varName);
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
+    // For a parent that runs its own loop over the list: declares the
+    // list, its counter, its length and the gathered columns, and returns
+    // the expression of the number of listed entries.
+    std::string declareList(CudaCodegen& cg) const;
+    const std::string& listBuffer() const { return list_; }
+    const std::string& indexVar() const { return idxVar_; }
 
 private:
     std::string list_, count_, idxVar_;
@@ -123,6 +132,10 @@ private:
         std::string name, type, table;
     };
     std::vector<Gather> gathers_;
+    struct ListColumn {
+        std::string buffer, type, var;
+    };
+    std::vector<ListColumn> listColumns_;
 };
 
 // Selection: if (predicate) consume(). Reference: metal_operators.cpp:63-69.
@@ -167,11 +180,17 @@ class CudaBitmapProbe : public CudaUnaryOperator {
 public:
     CudaBitmapProbe(std::unique_ptr<CudaOperator> child, const std::string& bitmapName, const std::string& keyExpr,
                     bool anti = false);
+    // Also count the bitmap's set bits (its distinct keys) into the u64
+    // counter `counterName`: after the probe's rows, each thread popcounts
+    // a grid-stride share of the words, one atomic per warp. Lets the build
+    // set bits without reading them back.
+    void setPopcountInto(const std::string& counterName) { popcount_ = counterName; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
 private:
     std::string bitmapName_, keyExpr_;
+    std::string popcount_;
     bool anti_;
 };
 
@@ -338,8 +357,8 @@ public:
     void addColumn(const std::string& arrayName, const std::string& type, const std::string& valueExpr,
                    const std::string& displayName = "");
     // An intermediate result read by a later phase, not the plan's output.
-    // Its (single, 4-byte) column is gathered per CTA in shared memory and
-    // appended with one atomic per CTA: rows keep no order.
+    // Its 4-byte columns (one or two) are gathered per CTA in shared memory
+    // and appended with one atomic per CTA: rows keep no order.
     void setIntermediate(bool on) { intermediate_ = on; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
@@ -469,6 +488,7 @@ public:
     std::string describe() const override;
 
 private:
+    void produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, ConsumerFn consume);
     std::string out_, keyExpr_, valueExpr_;
     int k_, maxBlocks_;
 };

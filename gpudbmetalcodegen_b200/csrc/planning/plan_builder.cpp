@@ -98,7 +98,7 @@ std::string TuneConfig::toString() const {
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
-      << ";split=" << (splitJoin ? 1 : 0);
+      << ";split=" << (splitJoin ? 1 : 0) << ";carve=" << smemCarveout;
     return o.str();
 }
 
@@ -126,12 +126,14 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "vec") t.scan.vectorRows = std::stoi(v);
         else if (k == "l2pf") t.scan.l2Prefetch = std::stoi(v);
         else if (k == "split") t.splitJoin = std::stoi(v) != 0;
+        else if (k == "carve") t.smemCarveout = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
         throw std::runtime_error("tune: bs must be a multiple of 32 in [32,1024]");
     if (t.scan.tileRows < 0 || t.scan.tileRows % 16) throw std::runtime_error("tune: tile must be a multiple of 16 (0 = auto)");
     if (t.scan.prefetchRows < 0 || t.scan.prefetchRows > 16) throw std::runtime_error("tune: pf must be in [0,16]");
+    if (t.smemCarveout < -1 || t.smemCarveout > 100) throw std::runtime_error("tune: carve must be -1 or in [0,100]");
     return t;
 }
 
@@ -191,6 +193,7 @@ CudaQueryPlan::Phase& appendPhase(CudaQueryPlan& plan, const std::string& name, 
     ph.root = std::move(root);
     ph.threadgroupSize = tune.blockSize;
     ph.minBlocksPerSM = std::max(1, std::min(tune.minBlocksPerSM, 2048 / tune.blockSize));
+    ph.smemCarveout = tune.smemCarveout;
     plan.phases.push_back(std::move(ph));
     return plan.phases.back();
 }
@@ -263,7 +266,9 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
                                                                       " && b_order_day[i] < " + std::to_string(odLt));
         auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "jb_bitmap", "b_key[i]", "max_b_key / 32 + 1");
-        bm->setDistinctCounter("jb_distinct");
+        // the split plan counts the bitmap's keys after the build (in its
+        // probe), so the build sets bits without waiting on their old values
+        if (!tune.splitJoin) bm->setDistinctCounter("jb_distinct");
         appendPhase(plan, "JT_build", std::move(bm), tune);
     }
     const std::string cap = "2 * max(jt_groups, 1)";
@@ -276,8 +281,10 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
             auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune);
             auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
             auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
+            pr->setPopcountInto("jb_distinct");
             auto mt = std::make_unique<CudaMaterialize>(std::move(pr), "jm_n", "n_probe");
             mt->addColumn("jm_rows", "unsigned", "(unsigned)_row");
+            mt->addColumn("jm_fk", "int", "p_fk[i]");  // the group key rides along: no gather of it later
             mt->setIntermediate(true);
             appendPhase(plan, "JT_probe", std::move(mt), tune);
         }
@@ -293,10 +300,10 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
                     tune);
         {
             auto ls = std::make_unique<CudaSlotListScan>("jm_rows", "jm_n");
-            ls->addGatherColumn("p_fk", "int", "probe");
+            ls->addListColumn("jm_fk", "int", "_jm_fk");
             ls->addGatherColumn("p_price", "long long", "probe");
             ls->addGatherColumn("p_discount", "long long", "probe");
-            auto gb = std::make_unique<CudaHashGroupBy>(std::move(ls), "jg", "p_fk[i]", "int", cap, HashLayout::Linear,
+            auto gb = std::make_unique<CudaHashGroupBy>(std::move(ls), "jg", "_jm_fk", "int", cap, HashLayout::Linear,
                                                         tune.maxProbe);
             gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
             gb->setWarpAggregate(tune.warpAggregate);
@@ -533,6 +540,7 @@ CudaCodegen generateFromPlan(const CudaQueryPlan& plan) {
         cg.setPhaseThreadgroupSize(ph.threadgroupSize);
         cg.setPhaseSingleThread(ph.singleThread);
         cg.setPhaseMinBlocksPerSM(ph.minBlocksPerSM);
+        cg.setPhaseSmemCarveout(ph.smemCarveout);
         for (const auto& [n, sz] : ph.bitmapReads) cg.addBitmapReadParam(n, sz);
         for (const auto& [n, t] : ph.scalarParams) cg.addScalarParam(n, t);
         for (const auto& eb : ph.extraBuffers) {

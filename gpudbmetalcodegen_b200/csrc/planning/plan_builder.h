@@ -52,6 +52,7 @@ struct CudaQueryPlan {
         std::unique_ptr<CudaOperator> root;
         int threadgroupSize = 256;
         int minBlocksPerSM = 1;
+        int smemCarveout = -1;
         bool singleThread = false;
         std::vector<std::pair<std::string, std::string>> bitmapReads;   // (name, sizeExpr)
         std::vector<std::pair<std::string, std::string>> scalarParams;  // (name, type)
@@ -105,6 +106,10 @@ struct TuneConfig {
     int maxProbe = 128;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
     bool splitJoin = false;       // join_topk: probe materialises matched rows, a second phase aggregates
+    // Preferred shared-memory carveout (percent of the SM's maximum) of
+    // phases that use dynamic shared memory; -1 leaves it to the driver,
+    // which may then fit fewer staged-ring blocks per SM.
+    int smemCarveout = -1;
     std::string toString() const;
     static TuneConfig parse(const std::string& s);  // "bs=512;scan=tma;tile=1024;stages=4;..."
 };
