@@ -32,7 +32,7 @@ SCAN_SPACE = {
     "bs": ["512", "256", "1024"],
     "tile": ["0", "1024", "2048", "4096"],
     "stages": ["4", "2", "3", "6"],
-    "occ": ["1", "2", "3"],
+    "occ": ["1", "2", "3", "4"],
 }
 HASH_SPACE = {
     "layout": ["linear", "bucket8"],
@@ -53,7 +53,8 @@ SPACES = {
 SEEDS = {
     "q1": [{"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
-    "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"}],
+    "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
+                  {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"}],
     "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"}],
 }
