@@ -69,26 +69,31 @@ class ClockSampler:
             self.h = (nv.nvmlDeviceGetHandleByUUID(self.sel) if self.sel.startswith(("GPU-", "MIG-"))
                       else nv.nvmlDeviceGetHandleByIndex(int(self.sel)))
             self.smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self._sample()  # one sample at each end of the region, others every ~2 ms
             self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
             self.nv = None
         return self
 
-    def _run(self):
+    def _sample(self):
         nv = self.nv
+        try:
+            self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                 nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+        except Exception:
+            pass
+
+    def _run(self):
         while not self.stop.is_set():
-            try:
-                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
-                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
-            except Exception:
-                pass
+            self._sample()
             time.sleep(0.002)
 
     def __exit__(self, *a):
         self.stop.set()
         if self.nv:
             self.thread.join(timeout=2)
+            self._sample()
             try:
                 self.nv.nvmlShutdown()
             except Exception:
