@@ -263,7 +263,7 @@ class Skew(Workload):
         self.n = args.zprobe_rows
         self.nkeys = args.zkeys
         self.spec = f"template={which}"
-        self.kernel = "GB_aggregate" if which == "groupby" else "HJ_probe_sum"
+        self.kernel = "GB_aggregate" if which == "groupby" else "HJ_probe_count"
         self.description = (f"{which}: {self.n} probe rows, Zipf(1.1) keys over {self.nkeys}")
 
     def generate(self):

@@ -42,7 +42,7 @@ HASH_SPACE = {
 SPACES = {
     "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4"]},
     "q6": SCAN_SPACE,
-    "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["0", "1"]},
+    "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["0", "1"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
                  "smem": ["10", "0", "8"], "warp": ["1", "0"]},

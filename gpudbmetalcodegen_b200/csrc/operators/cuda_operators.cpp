@@ -558,7 +558,7 @@ CudaArrayStore::CudaArrayStore(std::unique_ptr<CudaOperator> child, const std::s
       arrayName_(arrayName), keyExpr_(keyExpr), valueExpr_(valueExpr), valueType_(valueType), sizeExpr_(sizeExpr) {}
 
 void CudaArrayStore::produce(CudaCodegen& cg, ConsumerFn consume) {
-    cg.addBufferParam(arrayName_, valueType_, sizeExpr_, true, 0xFF);
+    cg.addBufferParam(arrayName_, valueType_, sizeExpr_, !dense_, 0xFF);
     cg.addBufferLengthParam("len_" + arrayName_, arrayName_);
     child_->produce(cg, [&]() {
         const std::string k = cg.fresh("_ak");

@@ -208,11 +208,14 @@ public:
     CudaArrayStore(std::unique_ptr<CudaOperator> child, const std::string& arrayName, const std::string& keyExpr,
                    const std::string& valueExpr, const std::string& valueType = "int",
                    const std::string& sizeExpr = "");
+    // Every index of the array is stored by the phase: no -1 sentinel fill.
+    void setDense(bool on) { dense_ = on; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
 private:
     std::string arrayName_, keyExpr_, valueExpr_, valueType_, sizeExpr_;
+    bool dense_ = false;
 };
 
 class CudaArrayLookup : public CudaUnaryOperator {

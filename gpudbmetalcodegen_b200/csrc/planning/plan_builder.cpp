@@ -98,8 +98,16 @@ std::string TuneConfig::toString() const {
       << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
-      << ";split=" << (splitJoin ? 1 : 0) << ";carve=" << smemCarveout;
+      << ";split=" << (splitJoin ? 1 : 0) << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
+      << ";bvec=" << buildVectorRows;
     return o.str();
+}
+
+TuneConfig TuneConfig::forBuild() const {
+    TuneConfig t = *this;
+    if (buildBlockSize > 0) t.blockSize = buildBlockSize;
+    if (buildVectorRows > 0) t.scan.vectorRows = buildVectorRows;
+    return t;
 }
 
 TuneConfig TuneConfig::parse(const std::string& s) {
@@ -127,6 +135,8 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "l2pf") t.scan.l2Prefetch = std::stoi(v);
         else if (k == "split") t.splitJoin = std::stoi(v) != 0;
         else if (k == "carve") t.smemCarveout = std::stoi(v);
+        else if (k == "bbs") t.buildBlockSize = std::stoi(v);
+        else if (k == "bvec") t.buildVectorRows = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -134,6 +144,8 @@ TuneConfig TuneConfig::parse(const std::string& s) {
     if (t.scan.tileRows < 0 || t.scan.tileRows % 16) throw std::runtime_error("tune: tile must be a multiple of 16 (0 = auto)");
     if (t.scan.prefetchRows < 0 || t.scan.prefetchRows > 16) throw std::runtime_error("tune: pf must be in [0,16]");
     if (t.smemCarveout < -1 || t.smemCarveout > 100) throw std::runtime_error("tune: carve must be -1 or in [0,100]");
+    if (t.buildBlockSize != 0 && (t.buildBlockSize < 64 || t.buildBlockSize > 1024 || t.buildBlockSize % 32))
+        throw std::runtime_error("tune: bbs must be 0 or a multiple of 32 in [64,1024]");
     return t;
 }
 
@@ -262,14 +274,15 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
     const bool given = s.has("groups");
     const long long groups = s.num("groups", 0);
     {
-        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, tune);
+        const TuneConfig bt = tune.forBuild();
+        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, bt);
         auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
                                                                       " && b_order_day[i] < " + std::to_string(odLt));
         auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "jb_bitmap", "b_key[i]", "max_b_key / 32 + 1");
         // the split plan counts the bitmap's keys after the build (in its
         // probe), so the build sets bits without waiting on their old values
         if (!tune.splitJoin) bm->setDistinctCounter("jb_distinct");
-        appendPhase(plan, "JT_build", std::move(bm), tune);
+        appendPhase(plan, "JT_build", std::move(bm), bt);
     }
     const std::string cap = "2 * max(jt_groups, 1)";
     if (tune.splitJoin) {
@@ -382,18 +395,29 @@ CudaQueryPlan buildHashJoin(Spec& s, const TuneConfig& tune) {
         hb->addPayload("payload", "int", "zb_payload[i]");
         appendPhase(plan, "HJ_build", std::move(hb), tune);
     }
+    // The summed column is the build key's own payload, so the sum per key
+    // is payload × matches: the probe only counts matches per slot (one
+    // random slot touch per probe row instead of payload, sum and count),
+    // and a pass over the slots multiplies (eager aggregation).
+    const std::string slots = hashSlotsExpr(cap);
     {
         auto scan = makeScan(plan, "zprobe", {"z_key"}, tune);
         auto pr = std::make_unique<CudaHashProbe>(std::move(scan), "hj", "z_key[i]", "long long", cap, "_slot",
                                                   tune.hashLayout, tune.maxProbe);
-        pr->addPayloadRead("payload", "int");
-        auto ag = std::make_unique<CudaAtomicAgg>(std::move(pr), "hj_sum", "_slot", "(long long)hj_payload[_slot]",
-                                                  hashSlotsExpr(cap));
-        ag->addAggregate("hj_count", "1");
+        auto ag = std::make_unique<CudaAtomicAgg>(std::move(pr), "hj_count", "_slot", "1ll", slots);
         ag->setWarpAggregate(tune.warpAggregate);
         ag->setSharedCache(tune.smemPreAggLog2);
-        auto& ph = appendPhase(plan, "HJ_probe_sum", std::move(ag), tune);
+        auto& ph = appendPhase(plan, "HJ_probe_count", std::move(ag), tune);
         ph.extraBuffers.push_back({"hj_keys", "unsigned long long", true, false});
+    }
+    {
+        auto sc = std::make_unique<CudaBufferScan>("n_hj_slots", slots, "s");
+        auto st = std::make_unique<CudaArrayStore>(std::move(sc), "hj_sum", "s",
+                                                   "(long long)hj_payload[s] * (long long)hj_count[s]", "long long", slots);
+        st->setDense(true);
+        auto& ph = appendPhase(plan, "HJ_sum", std::move(st), tune);
+        ph.extraBuffers.push_back({"hj_payload", "int", true, false});
+        ph.extraBuffers.push_back({"hj_count", "unsigned long long", true, false});
     }
     plan.decorate.push_back([cap](CudaResultSchema& rs) {
         rs.kind = CudaResultSchema::HASH_AGG;

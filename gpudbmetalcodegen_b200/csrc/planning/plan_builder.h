@@ -110,6 +110,11 @@ struct TuneConfig {
     // phases that use dynamic shared memory; -1 leaves it to the driver,
     // which may then fit fewer staged-ring blocks per SM.
     int smemCarveout = -1;
+    // Block size and vector rows of a join's build phase when they should
+    // differ from the probe's (0 = same as the plan's).
+    int buildBlockSize = 0;
+    int buildVectorRows = 0;
+    TuneConfig forBuild() const;
     std::string toString() const;
     static TuneConfig parse(const std::string& s);  // "bs=512;scan=tma;tile=1024;stages=4;..."
 };
