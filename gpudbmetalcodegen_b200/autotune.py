@@ -35,7 +35,7 @@ SCAN_SPACE = {
     "occ": ["1", "2", "3", "4"],
 }
 HASH_SPACE = {
-    "layout": ["linear", "bucket8"],
+    "layout": ["linear", "bucket8", "packed"],
     "smem": ["10", "0", "8", "12"],
     "warp": ["1", "0"],
 }
@@ -55,7 +55,8 @@ SEEDS = {
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
     "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
                   {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],
-    "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"}],
+    "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"},
+                {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "layout": "packed"}],
     "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"}],
 }
 BATCH_SPACE = {

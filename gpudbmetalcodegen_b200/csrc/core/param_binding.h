@@ -157,6 +157,9 @@ struct CudaResultSchema {
         std::vector<Agg> aggs;
         std::vector<DerivedColumn> derived;
         bool sortByKey = true;
+        // > 0: packed slots of this many u64 words in keyBuffer, word 0 =
+        // ~key (0 empty), word 1 + j = aggregate j
+        int packedStride = 0;
     };
     HashAggInfo hashAgg;
 

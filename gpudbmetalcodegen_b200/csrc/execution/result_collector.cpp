@@ -232,15 +232,24 @@ GenericResult CudaResultCollector::collectHashAgg(const CudaResultSchema& s, con
     const bool k64 = h.keyType == "unsigned long long";
     std::vector<uint64_t> keys64;
     std::vector<uint32_t> keys32;
-    if (k64) {
+    std::vector<std::vector<uint64_t>> aggs(h.aggs.size(), std::vector<uint64_t>(cap));
+    if (h.packedStride > 0) {
+        const size_t st = (size_t)h.packedStride;
+        std::vector<uint64_t> w(cap * st);
+        if (!read(h.keyBuffer, w.data(), w.size() * 8)) throw std::runtime_error("collector: missing " + h.keyBuffer);
+        keys64.resize(cap);
+        for (uint64_t i = 0; i < cap; i++) {
+            keys64[i] = ~w[i * st];  // an empty slot (0) reads as the ~0 sentinel
+            for (size_t a = 0; a < h.aggs.size(); a++) aggs[a][i] = w[i * st + 1 + a];
+        }
+    } else if (k64) {
         keys64.resize(cap);
         if (!read(h.keyBuffer, keys64.data(), cap * 8)) throw std::runtime_error("collector: missing " + h.keyBuffer);
     } else {
         keys32.resize(cap);
         if (!read(h.keyBuffer, keys32.data(), cap * 4)) throw std::runtime_error("collector: missing " + h.keyBuffer);
     }
-    std::vector<std::vector<uint64_t>> aggs(h.aggs.size(), std::vector<uint64_t>(cap));
-    for (size_t a = 0; a < h.aggs.size(); a++)
+    for (size_t a = 0; a < h.aggs.size() && h.packedStride == 0; a++)
         if (!read(h.aggs[a].buffer, aggs[a].data(), cap * 8))
             throw std::runtime_error("collector: missing " + h.aggs[a].buffer);
     r.columns.push_back({h.keyName, "int"});

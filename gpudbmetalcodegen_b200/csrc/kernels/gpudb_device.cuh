@@ -344,6 +344,38 @@ __device__ __forceinline__ long long gpudb_ht_insert64(unsigned long long* keys,
     return -1;
 }
 
+// Packed group-by slots of 2^stride_log2 u64 words: word 0 holds ~key
+// (0 = empty; the all-ones key stays reserved as in the other layouts) and
+// the aggregates follow in the same sector. Returns the slot index, as
+// gpudb_ht_insert64 does.
+__device__ __forceinline__ long long gpudb_htp_insert64(unsigned long long* slots, int stride_log2, int log2cap,
+                                                        unsigned long long key, unsigned max_probe, unsigned* err,
+                                                        bool* fresh = nullptr) {
+    if (key == GPUDB_EMPTY64) {
+        gpudb_set_error(err, GPUDB_ERR_SENTINEL_KEY);
+        return -1;
+    }
+    const unsigned long long want = ~key;
+    const unsigned long long mask = (1ull << log2cap) - 1ull;
+    unsigned long long s = gpudb_hash_slot(key, log2cap);
+    for (unsigned p = 0; p < max_probe; ++p) {
+        unsigned long long* w = slots + (s << stride_log2);
+        const unsigned long long cur = *w;
+        if (cur == want) return (long long)s;
+        if (cur == 0ull) {
+            const unsigned long long prev = atomicCAS(w, 0ull, want);
+            if (prev == 0ull) {
+                if (fresh) *fresh = true;
+                return (long long)s;
+            }
+            if (prev == want) return (long long)s;
+        }
+        s = (s + 1ull) & mask;
+    }
+    gpudb_set_error(err, GPUDB_ERR_HASH_OVERFLOW);
+    return -1;
+}
+
 __device__ __forceinline__ long long gpudb_ht_find64(const unsigned long long* __restrict__ keys, int log2cap,
                                                      unsigned long long key, unsigned max_probe) {
     const unsigned long long mask = (1ull << log2cap) - 1ull;

@@ -13,7 +13,13 @@ std::string S(long long v) { return std::to_string(v); }
 struct KeyOps {
     std::string store, ins, find, empty, cast;
 };
-KeyOps keyOps(const std::string& keyType, HashLayout layout) {
+KeyOps keyOps(const std::string& keyType, HashLayout layout, bool packedOk = false) {
+    if (layout == HashLayout::Packed) {
+        if (!packedOk) throw std::runtime_error("the packed hash layout is for group-by tables only");
+        if (keyType != "long long" && keyType != "unsigned long long")
+            throw std::runtime_error("the packed hash layout needs 64-bit keys");
+        return {"unsigned long long", "gpudb_htp_insert64", "", "0ull", "(unsigned long long)"};
+    }
     if (keyType == "int" || keyType == "unsigned") {
         if (layout == HashLayout::Bucket8)
             throw std::runtime_error("Bucket8 hash layout needs 64-bit keys");
@@ -1178,11 +1184,19 @@ std::string CudaHashInit::describe() const { return "HashInit(" + table_ + ", sl
 
 void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
     if (aggs_.empty()) throw std::runtime_error("CudaHashGroupBy: no aggregates");
-    const KeyOps ko = keyOps(keyType_, layout_);
+    const KeyOps ko = keyOps(keyType_, layout_, true);
     const bool dev = !devGroups_.empty();
     const std::string cap = hashSlotsExpr(dev ? devBound_ : capExpr_);
-    const std::string keys = table_ + "_keys";
-    if (dev) {
+    const bool packed = layout_ == HashLayout::Packed;
+    int strideLog2 = 0;
+    while ((1 << strideLog2) < 1 + (int)aggs_.size()) ++strideLog2;
+    const std::string keys = packed ? table_ + "_slots" : table_ + "_keys";
+    if (packed) {
+        if (dev) throw std::runtime_error("CudaHashGroupBy: a device-sized table uses the linear layout");
+        // word 0 of a slot holds ~key (0 = empty), the aggregates follow
+        cg.addAtomicBufferParam(keys, "unsigned long long", "(" + cap + ") * " + S(1 << strideLog2));
+        cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    } else if (dev) {
         // allocated for the bound, initialised by the table's HashInit phase
         cg.addBufferParam(keys, ko.store, cap, false, 0);
         for (const auto& a : aggs_) cg.addBufferParam(table_ + "_" + a.name, "unsigned long long", cap, false, 0);
@@ -1229,11 +1243,15 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
     }
     auto globalUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
         if (slotList_) cg.addLine("bool _gnew = false;");
-        cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + table_ + "_log2cap, " + ko.cast + keyVar + ", " +
-                   S(probeArg(layout_, maxProbe_)) + "u, gpudb_err" + (slotList_ ? ", &_gnew" : "") + ");");
+        cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + (packed ? S(strideLog2) + ", " : "") +
+                   table_ + "_log2cap, " + ko.cast + keyVar + ", " + S(probeArg(layout_, maxProbe_)) + "u, gpudb_err" +
+                   (slotList_ ? ", &_gnew" : "") + ");");
         cg.addBlock("if (_gslot >= 0)", [&]() {
-            for (int j = 0; j < na; j++)
-                cg.addLine("atomicAdd(" + table_ + "_" + aggs_[j].name + " + _gslot, (unsigned long long)" + vals[j] + ");");
+            for (int j = 0; j < na; j++) {
+                const std::string dst = packed ? keys + " + ((unsigned long long)_gslot << " + S(strideLog2) + ") + " + S(1 + j)
+                                               : table_ + "_" + aggs_[j].name + " + _gslot";
+                cg.addLine("atomicAdd(" + dst + ", (unsigned long long)" + vals[j] + ");");
+            }
             if (slotList_)
                 cg.addBlock("if (_gnew)", [&]() {  // group created
                     cg.addLine("const unsigned _gp = atomicAdd(_gl_n, 1u);");
@@ -1303,11 +1321,13 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
     hs.hashAgg.keyType = ko.store;
     hs.hashAgg.capacitySymbol = cap;
     hs.hashAgg.aggs.clear();
-    for (const auto& a : aggs_) hs.hashAgg.aggs.push_back({a.name, table_ + "_" + a.name});
+    for (const auto& a : aggs_) hs.hashAgg.aggs.push_back({a.name, packed ? keys : table_ + "_" + a.name});
+    hs.hashAgg.packedStride = packed ? (1 << strideLog2) : 0;
 }
 
 std::string CudaHashGroupBy::describe() const {
-    return "HashGroupBy(" + table_ + ", key=" + keyExpr_ + (layout_ == HashLayout::Bucket8 ? ", bucket8" : ", linear") +
+    return "HashGroupBy(" + table_ + ", key=" + keyExpr_ +
+           (layout_ == HashLayout::Bucket8 ? ", bucket8" : layout_ == HashLayout::Packed ? ", packed" : ", linear") +
            (warpAgg_ ? ", warp-agg" : "") + (smemLog2_ ? ", smem-preagg" : "") + ") <- " + describeChain();
 }
 

@@ -375,7 +375,11 @@ private:
 // ------------------------------------------------------------------
 // GPU hash tables (new; the reference builds its tables on the host).
 // ------------------------------------------------------------------
-enum class HashLayout { Linear, Bucket8 };
+// Linear: a key array and one array per aggregate. Bucket8: 64-bit keys
+// probed 8 slots (one 64-byte line) at a time. Packed (group-by tables with
+// 64-bit keys only): key and aggregates share one slot of a power-of-two
+// number of words, so a row touches one 32-byte sector, not one per array.
+enum class HashLayout { Linear, Bucket8, Packed };
 
 // Slot count / log2 of a hash table requested with `capacityExpr` slots:
 // rounded up to a power of two, at least 16 (one bucket8 group twice).

@@ -95,7 +95,9 @@ std::string TuneConfig::toString() const {
     std::ostringstream o;
     o << "bs=" << blockSize << ";scan=" << (scan.mode == ScanConfig::TmaBulk ? "tma" : "direct")
       << ";tile=" << scan.tileRows << ";stages=" << scan.stages
-      << ";layout=" << (hashLayout == HashLayout::Bucket8 ? "bucket8" : "linear") << ";smem=" << smemPreAggLog2
+      << ";layout="
+      << (hashLayout == HashLayout::Bucket8 ? "bucket8" : hashLayout == HashLayout::Packed ? "packed" : "linear")
+      << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
       << ";split=" << (splitJoin ? 1 : 0) << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
@@ -123,7 +125,8 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "layout") {
             if (v == "linear") t.hashLayout = HashLayout::Linear;
             else if (v == "bucket8") t.hashLayout = HashLayout::Bucket8;
-            else throw std::runtime_error("tune: layout must be linear|bucket8");
+            else if (v == "packed") t.hashLayout = HashLayout::Packed;
+            else throw std::runtime_error("tune: layout must be linear|bucket8|packed");
         } else if (k == "smem") t.smemPreAggLog2 = std::stoi(v);
         else if (k == "warp") t.warpAggregate = std::stoi(v) != 0;
         else if (k == "keyed") t.keyedStrategy = std::stoi(v);

@@ -73,6 +73,14 @@ def test_split_join_sizes_its_group_table_on_the_device():
         assert "gpudb_device_log2cap((unsigned long long)(min(__ldcg(jm_n), __ldcg(jb_distinct))), jg_log2max)" in body
 
 
+def test_packed_layout_is_for_group_by_tables():
+    q = engine.Query("template=groupby", "layout=packed")
+    assert "packed" in q.plan and "zg_slots" in q.source and "gpudb_htp_insert64(" in q.source
+    with pytest.raises(GpudbError) as e:
+        engine.Query("template=hashjoin", "layout=packed")
+    assert "group-by tables only" in e.value.message
+
+
 def test_spec_errors_are_reported():
     with pytest.raises(GpudbError) as e:
         engine.Query("template=nope")

@@ -240,7 +240,7 @@ def test_join_topk_full_size(ctx):
 # skewed group-by and hash join
 # ---------------------------------------------------------------------------
 GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0",
-            "vec=4", "vec=2;smem=0"]
+            "vec=4", "vec=2;smem=0", "layout=packed", "layout=packed;smem=8;warp=0", "layout=packed;smem=0;warp=1"]
 
 
 @pytest.fixture(scope="module")
