@@ -194,13 +194,28 @@ class JoinTopK(Workload):
         qual = np.zeros(self.build_rows + 2, dtype=bool)
         keep = (dim["b_segment"] == 1) & (dim["b_order_day"] < 1170)
         qual[dim["b_key"][keep]] = True
-        matched = int(np.count_nonzero((probe["p_ship_day"] > 1170) & qual[probe["p_fk"]]))
+        passing = probe["p_ship_day"] > 1170
+        matched = int(np.count_nonzero(passing & qual[probe["p_fk"]]))
+        self.bitmap_lookups = int(np.count_nonzero(passing))
         late = "late=0" not in tune
         alg = self.probe_rows * 8 + matched * 16 if late else self.probe_rows * 24
         if "split=1" in tune:
             alg = self.probe_rows * 8
         return {"algorithmic_bytes": alg, "rows_reaching_aggregation": matched,
-                "all_columns_bytes": self.probe_rows * 24}
+                "all_columns_bytes": self.probe_rows * 24,
+                # every column the query references, each read once (build
+                # 9 B/row, probe 24 B/row), whatever late materialisation skips
+                "query_bytes": self.build_rows * 9 + self.probe_rows * 24}
+
+    def limiter(self, tune, kernel_ms, sm_mhz):
+        """The split probe's bound: each row passing the ship-day filter
+        looks up a random word of a bitmap far larger than L1, one L2 sector
+        request, at about one request per SM clock."""
+        if "split=1" not in tune or not kernel_ms or not sm_mhz:
+            return {}
+        floor_ms = self.bitmap_lookups / (148 * sm_mhz * 1e6) * 1e3
+        return {"limiter": "l1_miss_requests", "bitmap_lookups": self.bitmap_lookups,
+                "request_floor_ms": floor_ms, "request_frac": floor_ms / kernel_ms}
 
     def cpu_run(self, threads):
         from oracle import oracle_py as O
@@ -815,6 +830,12 @@ def main():
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "kernel_ms": kms,
                 "traffic": load_traffic(kernel), **ab}
+    if "query_bytes" in ab:
+        # whole query per step against the same peak, bytes counted as above
+        qg = ab["query_bytes"] / (step_ms / 1e3) / 1e9
+        roofline.update({"query_gbs": qg, "query_frac": qg / peak})
+    if hasattr(w, "limiter"):
+        roofline.update(w.limiter(q.tune, kms, clk.summary().get("sm_mhz")))
 
     # end to end through the C-ABI with pinned host buffers, per step: H2D
     # of every column the plan reads for all rows, the late-materialised
