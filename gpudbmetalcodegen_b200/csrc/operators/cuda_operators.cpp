@@ -431,7 +431,9 @@ std::string CudaSlotListScan::declareList(CudaCodegen& cg) const {
     cg.addReadBufferParam(list_, "unsigned");
     cg.addReadBufferParam(count_, "unsigned long long");
     cg.addBufferLengthParam("len_" + list_, list_);
-    return "(long long)min(__ldcg(" + count_ + "), (unsigned long long)len_" + list_ + ")";
+    // the count comes from an earlier kernel: every thread reads it through
+    // L1 rather than all warps queueing on its one L2 line
+    return "(long long)min(__ldg(" + count_ + "), (unsigned long long)len_" + list_ + ")";
 }
 
 void CudaSlotListScan::produce(CudaCodegen& cg, ConsumerFn consume) {

@@ -307,7 +307,9 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         // No host round trip sizes the group table: it is allocated for
         // min(probe rows, build keys) groups and JT_init / JT_group derive
         // its slot count on the device from the two counters.
-        const std::string devGroups = "min(__ldcg(jm_n), __ldcg(jb_distinct))";
+        // every thread reads the two counters: through L1 (written by
+        // earlier kernels), not as one L2 line hammered by all warps
+        const std::string devGroups = "min(__ldg(jm_n), __ldg(jb_distinct))";
         const std::string bound = "2 * max(min(n_probe, max_b_key + 1), 1)";
         const std::vector<std::string> counters = {"jm_n", "jb_distinct"};
         appendPhase(plan, "JT_init",

@@ -70,7 +70,7 @@ def test_split_join_sizes_its_group_table_on_the_device():
     init = q.source.split("// === Phase 2: JT_init ===")[1].split("// === Phase 3")[0]
     group = q.source.split("// === Phase 3: JT_group ===")[1].split("// === Phase 4")[0]
     for body in (init, group):
-        assert "gpudb_device_log2cap((unsigned long long)(min(__ldcg(jm_n), __ldcg(jb_distinct))), jg_log2max)" in body
+        assert "gpudb_device_log2cap((unsigned long long)(min(__ldg(jm_n), __ldg(jb_distinct))), jg_log2max)" in body
 
 
 def test_packed_layout_is_for_group_by_tables():
