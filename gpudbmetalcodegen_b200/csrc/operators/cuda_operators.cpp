@@ -1495,13 +1495,22 @@ void CudaTopK::produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, Co
         cg.addLine("_tr_v = GPUDB_TOPK_NONE_VAL; _tr_k = GPUDB_TOPK_NONE_KEY;");
         cg.addLine("const long long _tgf = (long long)(__ldcg(" + out_ + "_floor) ^ 0x8000000000000000ull);");
         cg.addLine("const int _tg = (int)gridDim.x * " + K + ";");
-        cg.addBlock("for (int _e0 = (int)(threadIdx.x & ~31u); _e0 < _tg; _e0 += (int)blockDim.x)", [&]() {
-            cg.addLine("const int _e = _e0 + _tl;");
-            cg.addLine("const long long _ev = _e < _tg ? __ldcg(" + out_ + "_pvals + _e) : GPUDB_TOPK_NONE_VAL;");
-            cg.addLine("const bool _tin = _e < _tg && _ev >= _tgf;");
-            cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
-            cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ev : GPUDB_TOPK_NONE_VAL, "
-                       "_tin ? __ldcg(" + out_ + "_pkeys + _e) : GPUDB_TOPK_NONE_KEY);");
+        // four batches' loads in flight per warp before any is offered
+        cg.addBlock("for (int _e0 = (int)(threadIdx.x & ~31u); _e0 < _tg; _e0 += 4 * (int)blockDim.x)", [&]() {
+            cg.addLine("long long _ev[4], _ek[4];");
+            cg.addLine("#pragma unroll");
+            cg.addBlock("for (int _u = 0; _u < 4; ++_u)", [&]() {
+                cg.addLine("const int _e = _e0 + _u * (int)blockDim.x + _tl;");
+                cg.addLine("_ev[_u] = _e < _tg ? __ldcg(" + out_ + "_pvals + _e) : GPUDB_TOPK_NONE_VAL;");
+                cg.addLine("_ek[_u] = _e < _tg ? __ldcg(" + out_ + "_pkeys + _e) : GPUDB_TOPK_NONE_KEY;");
+            });
+            cg.addLine("#pragma unroll");
+            cg.addBlock("for (int _u = 0; _u < 4; ++_u)", [&]() {
+                cg.addLine("const bool _tin = _e0 + _u * (int)blockDim.x + _tl < _tg && _ev[_u] >= _tgf;");
+                cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
+                cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ev[_u] : GPUDB_TOPK_NONE_VAL, "
+                           "_tin ? _ek[_u] : GPUDB_TOPK_NONE_KEY);");
+            });
         });
         // this block's own floor stays valid: its K entries are among those offered
         blockMerge();
