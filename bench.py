@@ -111,8 +111,8 @@ class ClockSampler:
 
 
 def dist_info():
-    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
-            int(os.environ.get("LOCAL_RANK", "0")))
+    from gpudbmetalcodegen_b200 import replicas
+    return replicas.dist_info()
 
 
 # ---------------------------------------------------------------------------
@@ -417,12 +417,8 @@ def run_mixed(args):
         return
 
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        pg = dist
+    from gpudbmetalcodegen_b200 import replicas
+    pg = replicas.init("nccl", 300)
 
     t0 = time.perf_counter()
     tables = B.MixTables(rows=args.mix_rows, zipf_s=W.MIX_ZIPF_S, nranks=W.MIX_NRANKS,
@@ -466,7 +462,7 @@ def run_mixed(args):
         res, rep = learned.run(queries)
     stream = torch.cuda.current_stream()
     if pg:
-        pg.barrier()
+        replicas.barrier(pg)
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -484,10 +480,8 @@ def run_mixed(args):
         wall_ms = (time.perf_counter() - w0) * 1e3 / args.steps
     step_ms = ev0.elapsed_time(ev1) / args.steps
     if pg:
-        tt = torch.tensor([step_ms, wall_ms], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        step_ms, wall_ms = float(tt[0].item()), float(tt[1].item())
-        pg.barrier()
+        step_ms, wall_ms = replicas.max_over_ranks(pg, [step_ms, wall_ms], "cuda")
+        replicas.barrier(pg)
     verified = all(B.same_result(a, b) for a, b in zip(res, plain_res)) and \
         all(B.same_result(a, b) for a, b in zip(exact_res, plain_res))
 
@@ -552,7 +546,7 @@ def run_mixed(args):
     sizer.close()
     ctx.close()
     if pg:
-        pg.destroy_process_group()
+        replicas.shutdown(pg)
 
 
 def run_serve(args):
@@ -744,12 +738,8 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    from gpudbmetalcodegen_b200 import replicas
+    pg = replicas.init("nccl", 120)
 
     from gpudbmetalcodegen_b200 import Context, _lib
 
@@ -793,7 +783,7 @@ def main():
     ctx.sync()
     phase_acc, names = {}, []
     if pg:
-        pg.barrier()
+        replicas.barrier(pg)
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -814,10 +804,8 @@ def main():
         for i, ms in enumerate(t.phase_ms):
             phase_acc[i] = phase_acc.get(i, 0.0) + ms
     if pg:
-        tt = torch.tensor([step_ms], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        step_ms = float(tt.item())
-        pg.barrier()
+        step_ms = replicas.max_over_ranks(pg, [step_ms], "cuda")[0]
+        replicas.barrier(pg)
     rows_total = w.rows() * world
     value = rows_total / (step_ms / 1e3)
 
@@ -877,9 +865,7 @@ def main():
         if verified is not None:
             verified = verified and w.matches(r)
         if pg:
-            tt = torch.tensor([e_ms], device="cuda")
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            e_ms = float(tt.item())
+            e_ms = replicas.max_over_ranks(pg, [e_ms], "cuda")[0]
         d2h = sum(len(row) for row in r.rows) * 16 + 8
         in_place_bytes = late_bytes * ab.get("rows_reaching_aggregation", 0)
         e2e = {"value": rows_total / (e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": host_bytes + in_place_bytes,
@@ -914,7 +900,7 @@ def main():
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:
-        pg.destroy_process_group()
+        replicas.shutdown(pg)
 
 
 if __name__ == "__main__":
