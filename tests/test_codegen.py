@@ -73,6 +73,22 @@ def test_split_join_sizes_its_group_table_on_the_device():
         assert "gpudb_device_log2cap((unsigned long long)(min(__ldg(jm_n), __ldg(jb_distinct))), jg_log2max)" in body
 
 
+def test_top_k_over_a_slot_list_is_warp_cooperative():
+    src = engine.Query("template=join_topk", "split=1").source
+    topk = src.split("// === Phase 4: JT_topk ===")[1]
+    assert "gpudb_topk_warp_offer<10>(" in topk and "_tk_v[" not in topk  # no per-thread k-lists
+    assert "jt_top_floor" in topk  # block floors prune the grid merge
+
+
+def test_hash_join_counts_matches_and_multiplies():
+    q = engine.Query("template=hashjoin")
+    phases = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
+    assert phases == ["HJ_build", "HJ_probe_count", "HJ_sum"]
+    probe = q.source.split("// === Phase 1: HJ_probe_count ===")[1].split("// === Phase 2")[0]
+    assert "hj_payload" not in probe  # the probe reads no payload
+    assert "hj_sum[_ak0] = (long long)((long long)hj_payload[s] * (long long)hj_count[s]);" in q.source
+
+
 def test_packed_layout_is_for_group_by_tables():
     q = engine.Query("template=groupby", "layout=packed")
     assert "packed" in q.plan and "zg_slots" in q.source and "gpudb_htp_insert64(" in q.source
