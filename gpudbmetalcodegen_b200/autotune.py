@@ -37,6 +37,7 @@ SCAN_SPACE = {
 HASH_SPACE = {
     "layout": ["linear", "bucket8", "packed"],
     "smem": ["10", "0", "8", "12"],
+    "sprobe": ["0", "4", "2"],
     "warp": ["1", "0"],
 }
 SPACES = {
@@ -45,7 +46,7 @@ SPACES = {
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["0", "1"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
-                 "smem": ["10", "0", "8"], "warp": ["1", "0"]},
+                 "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"]},
 }
 # Joint moves coordinate descent cannot make one parameter at a time (a
 # shallower TMA ring frees the shared memory that a higher occupancy needs):
@@ -56,7 +57,8 @@ SEEDS = {
     "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
                   {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"},
-                {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "layout": "packed"}],
+                {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "layout": "packed"},
+                {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "sprobe": "4"}],
     "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"}],
 }
 BATCH_SPACE = {

@@ -898,7 +898,8 @@ void CudaAtomicAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
             }, " else {");
             cg.increaseIndent();
             if (L > 0) {
-                cg.addLine("const int _as = gpudb_smem_ht_slot64(_ac_k, " + S(L) + ", (unsigned long long)_ab, 16);");
+                cg.addLine("const int _as = gpudb_smem_ht_slot64(_ac_k, " + S(L) + ", (unsigned long long)_ab, " +
+                           S(smemProbe_) + ");");
                 cg.addBlock("if (_as >= 0)", [&]() {
                     for (int j = 0; j < na; j++)
                         cg.addLine("atomicAdd(_ac_v + " + S(j * slots) + " + _as, (unsigned long long)_av" + S(j) + ");");
@@ -1271,7 +1272,8 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
         }
         auto update = [&]() {
             if (smem) {
-                cg.addLine("const int _gss = gpudb_smem_ht_slot64(_gs_k, " + S(L) + ", (unsigned long long)_gk, 8);");
+                cg.addLine("const int _gss = gpudb_smem_ht_slot64(_gs_k, " + S(L) + ", (unsigned long long)_gk, " +
+                           S(smemProbe_) + ");");
                 cg.addBlock("if (_gss >= 0)", [&]() {
                     for (int j = 0; j < na; j++)
                         cg.addLine("atomicAdd(_gs_v + " + S(j) + " * " + S(1 << L) + " + _gss, (unsigned long long)_gv" +

@@ -319,7 +319,14 @@ public:
     // and the shared-memory cache), e.g. a count beside a sum.
     void addAggregate(const std::string& arrayName, const std::string& valueExpr);
     void setWarpAggregate(bool on) { warpAgg_ = on; }
-    void setSharedCache(int log2Slots) { smemLog2_ = log2Slots; }
+    // `probe` = shared slots tried before a row goes to the global array
+    // (0 = 2). Once the cache is full every cold row pays that many, and
+    // hot keys settle near their home slot while it fills: on the Zipf hash
+    // join, 2 probes took 1.81 ms against 2.39 ms for 16.
+    void setSharedCache(int log2Slots, int probe = 0) {
+        smemLog2_ = log2Slots;
+        smemProbe_ = probe > 0 ? probe : 2;
+    }
     void setZeroInit(bool on) { zeroInit_ = on; }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
@@ -329,6 +336,7 @@ private:
     std::vector<std::pair<std::string, std::string>> extra_;
     bool warpAgg_ = false;
     int smemLog2_ = 0;
+    int smemProbe_ = 2;
     bool zeroInit_ = true;
 };
 
@@ -435,7 +443,11 @@ public:
                     HashLayout layout = HashLayout::Linear, int maxProbe = 128);
     void addAggregate(const std::string& name, const std::string& valueExpr);  // "1" = count
     void setWarpAggregate(bool on) { warpAgg_ = on; }
-    void setSharedPreAgg(int log2Slots) { smemLog2_ = log2Slots; }
+    // `probe` as for CudaAtomicAgg::setSharedCache (0 = 8)
+    void setSharedPreAgg(int log2Slots, int probe = 0) {
+        smemLog2_ = log2Slots;
+        smemProbe_ = probe > 0 ? probe : 8;
+    }
     // Record every slot when its group is created in <table>_slotlist
     // (count in <table>_nslots): later phases visit only used slots.
     void setSlotList(bool on) { slotList_ = on; }
@@ -459,6 +471,7 @@ private:
     std::vector<Agg> aggs_;
     bool warpAgg_ = true;
     int smemLog2_ = 0;
+    int smemProbe_ = 8;
     bool slotList_ = false;
     std::string devGroups_, devBound_;
     std::vector<std::string> devCounters_;

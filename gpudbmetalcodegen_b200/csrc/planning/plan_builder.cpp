@@ -100,7 +100,7 @@ std::string TuneConfig::toString() const {
       << ";smem=" << smemPreAggLog2
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
-      << ";split=" << (splitJoin ? 1 : 0) << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
+      << ";split=" << (splitJoin ? 1 : 0) << ";sprobe=" << smemProbe << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
       << ";bvec=" << buildVectorRows;
     return o.str();
 }
@@ -138,6 +138,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "l2pf") t.scan.l2Prefetch = std::stoi(v);
         else if (k == "split") t.splitJoin = std::stoi(v) != 0;
         else if (k == "carve") t.smemCarveout = std::stoi(v);
+        else if (k == "sprobe") t.smemProbe = std::stoi(v);
         else if (k == "bbs") t.buildBlockSize = std::stoi(v);
         else if (k == "bvec") t.buildVectorRows = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
@@ -379,7 +380,7 @@ CudaQueryPlan buildGroupBy(Spec& s, const TuneConfig& tune) {
     gb->addAggregate("count", "1");
     gb->addAggregate("sum", "z_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
-    gb->setSharedPreAgg(tune.smemPreAggLog2);
+    gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
     appendPhase(plan, "GB_aggregate", std::move(gb), tune);
     return plan;
 }
@@ -411,7 +412,7 @@ CudaQueryPlan buildHashJoin(Spec& s, const TuneConfig& tune) {
                                                   tune.hashLayout, tune.maxProbe);
         auto ag = std::make_unique<CudaAtomicAgg>(std::move(pr), "hj_count", "_slot", "1ll", slots);
         ag->setWarpAggregate(tune.warpAggregate);
-        ag->setSharedCache(tune.smemPreAggLog2);
+        ag->setSharedCache(tune.smemPreAggLog2, tune.smemProbe);
         auto& ph = appendPhase(plan, "HJ_probe_count", std::move(ag), tune);
         ph.extraBuffers.push_back({"hj_keys", "unsigned long long", true, false});
     }
@@ -519,7 +520,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
     gb->addAggregate("count", "1");
     gb->addAggregate("sum", "m_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
-    gb->setSharedPreAgg(tune.smemPreAggLog2);
+    gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
     gb->setSlotList(tmpl == "mix_topk");
     appendPhase(plan, "MIXG_group", std::move(gb), tune);
     if (tmpl == "mix_topk") {

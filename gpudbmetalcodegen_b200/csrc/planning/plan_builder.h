@@ -100,6 +100,7 @@ struct TuneConfig {
     ScanConfig scan;
     HashLayout hashLayout = HashLayout::Linear;
     int smemPreAggLog2 = 10;    // hash group-by shared-memory table (0 = off)
+    int smemProbe = 0;          // slots tried in that table per row (0 = the operator's default)
     int minBlocksPerSM = 1;     // __launch_bounds__ occupancy hint (caps registers)
     bool warpAggregate = true;  // match_any pre-aggregation in hash / atomic aggregation
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)

@@ -240,7 +240,8 @@ def test_join_topk_full_size(ctx):
 # skewed group-by and hash join
 # ---------------------------------------------------------------------------
 GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0",
-            "vec=4", "vec=2;smem=0", "layout=packed", "layout=packed;smem=8;warp=0", "layout=packed;smem=0;warp=1"]
+            "vec=4", "vec=2;smem=0", "layout=packed", "layout=packed;smem=8;warp=0", "layout=packed;smem=0;warp=1",
+            "smem=8;sprobe=4;warp=0", "sprobe=1"]
 
 
 @pytest.fixture(scope="module")
@@ -262,7 +263,7 @@ def test_groupby_parity(ctx, zipf_small, tune):
     assert np.array_equal(np.array(res.column("sum")), s)
 
 
-@pytest.mark.parametrize("tune", ["", "layout=bucket8", "smem=11", "warp=0"])
+@pytest.mark.parametrize("tune", ["", "layout=bucket8", "smem=11", "warp=0", "smem=8;sprobe=1", "sprobe=16"])
 def test_hashjoin_parity(ctx, zipf_small, tune):
     zb, zp, _ = zipf_small
     ctx.upload_table("zbuild", zb)
