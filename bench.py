@@ -182,13 +182,14 @@ class JoinTopK(Workload):
         return self._exp
 
     def kernel_for(self, tune):
-        # with split=1 the probe only lists matched rows; JT_group aggregates them
-        return "JT_probe" if "split=1" in tune else "JT_probe_group"
+        # the split plan (the default) only lists matched rows in the probe;
+        # JT_group aggregates them. split=0 probes and groups in one kernel
+        return "JT_probe_group" if "split=0" in tune else "JT_probe"
 
     def algorithmic_bytes(self, tune):
         # eager columns (fk, ship_day) for every probe row + the late
         # price/discount (8 B each) for rows reaching the aggregation; with
-        # split=1 the dominant kernel (JT_probe) reads the eager columns only
+        # in the split plan the dominant kernel (JT_probe) reads the eager columns only
         import numpy as np
         dim, probe = self.tables["dim"], self.tables["probe"]
         qual = np.zeros(self.build_rows + 2, dtype=bool)
@@ -199,7 +200,7 @@ class JoinTopK(Workload):
         self.bitmap_lookups = int(np.count_nonzero(passing))
         late = "late=0" not in tune
         alg = self.probe_rows * 8 + matched * 16 if late else self.probe_rows * 24
-        if "split=1" in tune:
+        if "split=0" not in tune:
             alg = self.probe_rows * 8
         return {"algorithmic_bytes": alg, "rows_reaching_aggregation": matched,
                 "all_columns_bytes": self.probe_rows * 24,
@@ -211,7 +212,7 @@ class JoinTopK(Workload):
         """The split probe's bound: each row passing the ship-day filter
         looks up a random word of a bitmap far larger than L1, one L2 sector
         request, at about one request per SM clock."""
-        if "split=1" not in tune or not kernel_ms or not sm_mhz:
+        if "split=0" in tune or not kernel_ms or not sm_mhz:
             return {}
         floor_ms = self.bitmap_lookups / (148 * sm_mhz * 1e6) * 1e3
         return {"limiter": "l1_miss_requests", "bitmap_lookups": self.bitmap_lookups,

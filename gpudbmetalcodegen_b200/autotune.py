@@ -43,7 +43,7 @@ HASH_SPACE = {
 SPACES = {
     "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4"]},
     "q6": SCAN_SPACE,
-    "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["0", "1"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
+    "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["1", "0"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
                  "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"]},
@@ -54,7 +54,7 @@ SPACES = {
 SEEDS = {
     "q1": [{"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
-    "join_topk": [{"stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
+    "join_topk": [{"split": "0", "stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
                   {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"},
                 {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "layout": "packed"},

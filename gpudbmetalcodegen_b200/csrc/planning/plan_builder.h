@@ -106,7 +106,10 @@ struct TuneConfig {
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
     int maxProbe = 128;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
-    bool splitJoin = false;       // join_topk: probe materialises matched rows, a second phase aggregates
+    // join_topk: the probe lists matched rows and later phases aggregate
+    // them, sized on the device (split=0: probe and group-by in one kernel,
+    // sized by a host read of the build's distinct count)
+    bool splitJoin = true;
     // Preferred shared-memory carveout (percent of the SM's maximum) of
     // phases that use dynamic shared memory; -1 leaves it to the driver,
     // which may then fit fewer staged-ring blocks per SM.

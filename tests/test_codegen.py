@@ -55,15 +55,15 @@ def test_tma_scan_is_default_and_direct_mode_has_no_bulk_copies():
 
 
 def test_join_topk_three_phases_and_sizing_step():
-    plan = engine.Query("template=join_topk").plan
+    plan = engine.Query("template=join_topk", "split=0").plan
     assert "JT_build" in plan and "JT_probe_group" in plan and "JT_topk" in plan
     assert "sizing jt_groups after phase 1 from counter jb_distinct" in plan
-    given = engine.Query("template=join_topk;groups=1000").plan
+    given = engine.Query("template=join_topk;groups=1000", "split=0").plan
     assert "from '1000'" in given
 
 
 def test_split_join_sizes_its_group_table_on_the_device():
-    q = engine.Query("template=join_topk", "split=1")
+    q = engine.Query("template=join_topk")  # the split plan is the default
     phases = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
     assert phases == ["JT_build", "JT_probe", "JT_init", "JT_group", "JT_topk"]
     assert "sizing jt_groups" not in q.plan  # no host round trip between the phases

@@ -103,15 +103,16 @@ def load_join(ctx, nd, npr, seed=3):
     return d, p
 
 
-@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "warp=0", "late=0", "bs=1024;tile=2048;stages=3",
-                                  "vec=4", "vec=4;pf=4", "vec=8;late=0", "pf=4", "split=1", "split=1;stages=2;warp=0"])
+@pytest.mark.parametrize("tune", ["", "scan=direct", "bs=256", "split=0", "split=0;warp=0", "split=0;late=0",
+                                  "split=0;bs=1024;tile=2048;stages=3", "split=0;vec=4;pf=4", "split=0;vec=8;late=0",
+                                  "vec=4", "pf=4", "stages=2;warp=0;occ=4", "bvec=4;bbs=256"])
 def test_join_topk_parity(ctx, tune):
     d, p = load_join(ctx, 200_000, 800_000)
     top, groups, distinct = O.join_topk(d, p, k=10)
     res, t = ctx.run("template=join_topk", tune)
     assert t.device_error == 0
     assert res.rows == top
-    if "split=1" in tune:
+    if "split=0" not in tune:
         # sized on the device from min(matched rows, qualifying build keys):
         # no host sizing symbol; the table holds exactly the joined groups
         assert int(ctx.read_buffer("jg_nslots", np.uint64, 1)[0]) == groups
@@ -156,7 +157,7 @@ def test_join_topk_ties_break_by_key(ctx):
 def test_join_topk_learned_size_overflow_is_reported(ctx):
     load_join(ctx, 200_000, 800_000)
     with pytest.raises(GpudbError) as e:
-        ctx.run("template=join_topk;groups=4")
+        ctx.run("template=join_topk;groups=4", "split=0")
     assert e.value.status == -7
     assert e.value.timing.device_error & DEVERR_HASH_OVERFLOW
 
@@ -169,14 +170,14 @@ def test_enqueue_pipelines_runs_and_reports_errors_at_sync(ctx):
     top = O.join_topk(d, p, k=10)[0]
     ctx.set_use_graphs(True)
     try:
-        for tune in ("split=1", "split=1;stages=2;occ=3", ""):
+        for tune in ("", "split=1;stages=2;occ=3", "split=0"):
             q = ctx.prepare("template=join_topk", tune)
             for _ in range(5):
                 ctx.enqueue(q)
             ctx.sync()
             res, t = ctx.run(q)
             assert res.rows == top and t.device_error == 0
-        bad = ctx.prepare("template=join_topk;groups=4")
+        bad = ctx.prepare("template=join_topk;groups=4", "split=0")
         ok = ctx.prepare("template=join_topk", "split=1")
         ctx.enqueue(bad)
         ctx.enqueue(ok)
@@ -232,6 +233,10 @@ def test_join_topk_full_size(ctx):
     d, p = load_join(ctx, W.DIM_ROWS, W.PROBE_ROWS, seed=W.SEED)
     top, groups, distinct = O.join_topk(d, p, k=10)
     res, _ = ctx.run("template=join_topk")
+    assert res.rows == top
+    assert int(ctx.read_buffer("jg_nslots", np.uint64, 1)[0]) == groups
+    assert int(ctx.read_buffer("jb_distinct", np.uint64, 1)[0]) == distinct
+    res, _ = ctx.run("template=join_topk", "split=0")
     assert res.rows == top
     assert ctx.get_symbol("jt_groups") == distinct
 
