@@ -367,6 +367,36 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
     return plan;
 }
 
+// ---- join_rows: the Q3 semi-join with its matching probe rows
+// materialised (row id, key, revenue) instead of aggregated — the
+// reference's Materialize operator (metal_operators.cpp:618-643) on the
+// join of metal_plan_builder.cpp:1170-1239. Rows come out in no order, as
+// the reference's atomic output positions do; the capacity is the probe
+// table (every row may match).
+CudaQueryPlan buildJoinRows(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "JOIN_ROWS";
+    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
+    {
+        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
+                                                                      " && b_order_day[i] < " + std::to_string(odLt));
+        auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "jb_bitmap", "b_key[i]", "max_b_key / 32 + 1");
+        appendPhase(plan, "JR_build", std::move(bm), tune);
+    }
+    {
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune, true, {"p_price", "p_discount"});
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
+        auto mt = std::make_unique<CudaMaterialize>(std::move(pr), "jr_n", "n_probe");
+        mt->addColumn("jr_row", "long long", "_row", "row");
+        mt->addColumn("jr_key", "int", "p_fk[i]", "key");
+        mt->addColumn("jr_revenue", "long long", "p_price[i] * (100ll - p_discount[i])", "revenue");
+        appendPhase(plan, "JR_probe", std::move(mt), tune);
+    }
+    return plan;
+}
+
 // ---- groupby: high-cardinality hash group-by, count + sum (reference
 // Q18 shape metal_plan_builder.cpp:1529-1545, which aggregates into a
 // direct-address array; here an open-addressing table keyed by int64).
@@ -539,7 +569,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
 }  // namespace
 
 std::vector<std::string> planTemplates() {
-    return {"q1", "q6", "join_topk", "groupby", "hashjoin", "colmax", "distinct",
+    return {"q1", "q6", "join_topk", "join_rows", "groupby", "hashjoin", "colmax", "distinct",
             "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
 }
 
@@ -550,6 +580,7 @@ CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) 
     if (tmpl == "q1" || tmpl == "scan_filter_groupagg") plan = buildQ1(s, tune);
     else if (tmpl == "q6" || tmpl == "scan_filter_sum") plan = buildQ6(s, tune);
     else if (tmpl == "join_topk") plan = buildJoinTopK(s, tune);
+    else if (tmpl == "join_rows") plan = buildJoinRows(s, tune);
     else if (tmpl == "groupby") plan = buildGroupBy(s, tune);
     else if (tmpl == "hashjoin") plan = buildHashJoin(s, tune);
     else if (tmpl == "colmax") plan = buildColMax(s, tune);

@@ -104,6 +104,26 @@ def join_topk(dim, probe, seg=1, od_lt=1170, ship_gt=1170, k=10, threads: int = 
     return [(int(keys[i]), int(vals[i])) for i in range(cnt)], groups.value, distinct.value
 
 
+def join_rows(dim, probe, seg=1, od_lt=1170, ship_gt=1170) -> List[tuple]:
+    """The rows of the Q3-shape semi-join, materialised instead of
+    aggregated: (probe row, key, price * (100 - discount)) for every probe
+    row with ship_day > ship_gt whose key is a build key with segment == seg
+    and order_day < od_lt (reference: MetalMaterialize,
+    metal_operators.cpp:618-643, over the join of
+    metal_plan_builder.cpp:1170-1239). Sorted by row: the engine's output
+    order is unspecified, as the reference's atomic positions are. numpy,
+    exact int64."""
+    keep = (dim["b_segment"] == seg) & (dim["b_order_day"] < od_lt)
+    top = int(max(int(dim["b_key"].max(initial=0)), int(probe["p_fk"].max(initial=0)))) + 1
+    qual = np.zeros(top + 1, dtype=bool)
+    qual[dim["b_key"][keep]] = True
+    fk = probe["p_fk"]
+    ok = (probe["p_ship_day"] > ship_gt) & (fk >= 0) & qual[np.clip(fk, 0, top)]
+    rows = np.nonzero(ok)[0]
+    rev = probe["p_price"][rows] * (100 - probe["p_discount"][rows])
+    return [(int(r), int(k), int(v)) for r, k, v in zip(rows, fk[rows], rev)]
+
+
 def groupby(key: np.ndarray, value: np.ndarray, cap: int, threads: int = 0):
     ok, oc, os_ = (np.zeros(cap, np.int64) for _ in range(3))
     g = lib().oracle_groupby(key.shape[0], _p(key), _p(value), cap, _p(ok), _p(oc), _p(os_), threads)

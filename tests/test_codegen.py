@@ -73,6 +73,14 @@ def test_split_join_sizes_its_group_table_on_the_device():
         assert "gpudb_device_log2cap((unsigned long long)(min(__ldg(jm_n), __ldg(jb_distinct))), jg_log2max)" in body
 
 
+def test_join_rows_materialises_the_matches():
+    q = engine.Query("template=join_rows;ship_gt=1000")
+    phases = [ln.split()[2].rstrip(":") for ln in q.plan.splitlines() if ln.strip().startswith("phase ")]
+    assert phases == ["JR_build", "JR_probe"]
+    assert "Materialize(3 columns)" in q.plan and "gpudb_warp_reserve(jr_n" in q.source
+    assert "p_ship_day[i] > 1000" in q.source
+
+
 def test_top_k_over_a_slot_list_is_warp_cooperative():
     src = engine.Query("template=join_topk", "split=1").source
     topk = src.split("// === Phase 4: JT_topk ===")[1]

@@ -141,6 +141,22 @@ def test_split_join_device_sizing_edges(ctx, ship_gt, od_lt):
         assert int(ctx.read_buffer("jg_nslots", np.uint64, 1)[0]) == groups
 
 
+@pytest.mark.parametrize("spec,tune", [("template=join_rows", ""), ("template=join_rows;ship_gt=2000", "scan=direct"),
+                                       ("template=join_rows;od_lt=0", ""), ("template=join_rows;seg=3;ship_gt=600", "bs=256")])
+def test_join_rows_parity(ctx, spec, tune):
+    """Materialised join output (row, key, revenue): the same multiset of
+    rows as the oracle, in any order; none when nothing matches."""
+    d, p = load_join(ctx, 100_000, 400_000, seed=13)
+    kv = dict(x.split("=") for x in spec.split(";")[1:])
+    exp = O.join_rows(d, p, seg=int(kv.get("seg", 1)), od_lt=int(kv.get("od_lt", 1170)),
+                      ship_gt=int(kv.get("ship_gt", 1170)))
+    for _ in range(2):  # twice through the same buffers
+        res, t = ctx.run(spec, tune)
+        assert t.device_error == 0
+        assert sorted(res.rows) == exp
+    assert res.columns == ["row", "key", "revenue"]
+
+
 def test_join_topk_ties_break_by_key(ctx):
     # every probe row carries the same revenue: ranking is decided by key
     d = W.gen_dim(5000, seed=4)

@@ -79,6 +79,25 @@ def test_join_topk_known_answer_with_ties():
     assert top2 == [(1, 10000), (3, 10000)]
 
 
+def test_join_rows_known_answer_agrees_with_join_topk():
+    dim = {"b_key": np.array([3, 1, 2, 5, 4], np.int32), "b_order_day": np.array([100, 100, 2000, 100, 100], np.int32),
+           "b_segment": np.array([1, 1, 1, 0, 1], np.uint8)}
+    probe = {"p_fk": np.array([3, 1, 1, 4, 2, 5, 3, 4], np.int32),
+             "p_ship_day": np.array([2000, 2000, 2000, 2000, 2000, 2000, 10, 2000], np.int32),
+             "p_price": np.array([100, 50, 50, 100, 999, 999, 999, 0], np.int64),
+             "p_discount": np.array([0, 0, 0, 0, 0, 0, 0, 10], np.int64)}
+    rows = O.join_rows(dim, probe)
+    # rows 4 (key 2) and 5 (key 5) have no qualifying build key; row 6 ships too early
+    assert rows == [(0, 3, 10000), (1, 1, 5000), (2, 1, 5000), (3, 4, 10000), (7, 4, 0)]
+    # grouping the materialised rows gives the aggregate pipeline's answer
+    sums = {}
+    for _, k, v in rows:
+        sums[k] = sums.get(k, 0) + v
+    top, _, _ = O.join_topk(dim, probe, k=10)
+    assert sorted(sums.items(), key=lambda kv: (-kv[1], kv[0])) == top
+    assert O.join_rows(dim, probe, od_lt=0) == []
+
+
 def test_groupby_and_hashjoin_known_answer():
     key = np.array([5, -3, 5, 9, -3, 5], np.int64)
     val = np.array([1, 2, 3, 4, 5, 6], np.int64)
