@@ -47,6 +47,18 @@ class Timing(C.Structure):
                 ("collect_ms", C.c_double)]
 
 
+class ColbinColumn(C.Structure):
+    _fields_ = [("column_index", C.c_int32), ("dtype", C.c_uint8), ("fixed_width", C.c_uint16),
+                ("offset", C.c_uint64), ("size_bytes", C.c_uint64)]
+
+
+class ColbinLoadSpec(C.Structure):
+    _fields_ = [("column_index", C.c_int32), ("column", C.c_char_p), ("transform", C.c_int32), ("scale", C.c_int32)]
+
+
+COLBIN_AS_IS, COLBIN_WIDEN, COLBIN_DECIMAL, COLBIN_DAYS = 0, 1, 2, 3
+
+
 # (name, restype, argtypes) for every exported entry point.
 _SIGNATURES = [
     # gpudb_rt.h
@@ -65,6 +77,9 @@ _SIGNATURES = [
     ("gpudb_upload_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
     ("gpudb_register_host_column", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64,
                                              C.c_int]),
+    ("gpudb_colbin_inspect", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                       C.POINTER(ColbinColumn), C.c_uint32]),
+    ("gpudb_colbin_load", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(ColbinLoadSpec), C.c_int]),
     ("gpudb_register_rows", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
     ("gpudb_register_buffer", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
     ("gpudb_register_symbol", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),

@@ -41,6 +41,7 @@ HOST_SOURCES = [
     "execution/query_engine.cpp",
     "capi/gpudb_capi.cpp",
     "datagen/datagen.cpp",
+    "io/colbin.cpp",
 ]
 CUDA_SOURCES: list[str] = [
     "kernels/noalloc_distinct.cu",

@@ -3,13 +3,17 @@
 // context error text; nothing C++ crosses the boundary.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
+#include <vector>
 #include <memory>
 #include <string>
 
 #include "../../../include/gpudb_engine.h"
 #include "../../../include/gpudb_rt.h"
 #include "../execution/query_engine.h"
+#include "../io/colbin.h"
+#include "../planning/plan_builder.h"
 
 struct gpudb_ctx {
     std::unique_ptr<gpudb::QueryContext> qc;
@@ -205,6 +209,97 @@ int gpudb_register_host_column(gpudb_ctx* ctx, const char* table, const char* co
     if (!ctx || !table || !column || (!host && rows) || elem_bytes <= 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
     try {
         ctx->qc->ex.registerHostColumn(column, table, host, rows, (size_t)elem_bytes);
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, GPUDB_E_INVALID, e.what());
+    }
+}
+
+int gpudb_colbin_inspect(const char* path, uint64_t* rows, uint32_t* ncols, gpudb_colbin_column* cols, uint32_t cap) {
+    if (!path) return fail(nullptr, GPUDB_E_INVALID, "bad argument");
+    try {
+        gpudb::ColbinFile f(path);
+        if (rows) *rows = f.rows();
+        if (ncols) *ncols = (uint32_t)f.columns().size();
+        for (uint32_t i = 0; cols && i < cap && i < (uint32_t)f.columns().size(); i++) {
+            const auto& d = f.columns()[i];
+            cols[i] = {d.columnIndex, d.dtype, d.fixedWidth, d.offset, d.sizeBytes};
+        }
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(nullptr, GPUDB_E_INVALID, e.what());
+    }
+}
+
+int gpudb_colbin_load(gpudb_ctx* ctx, const char* path, const char* table, const gpudb_colbin_load_spec* specs,
+                      int n) {
+    if (!ctx || !path || !table || (!specs && n) || n < 0) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    try {
+        cudaSetDevice(ctx->qc->ex.device());
+        gpudb::ColbinFile f(path);
+        const gpudb::TableDef& td = gpudb::catalogTable(table);
+        const uint64_t rows = f.rows();
+        for (int k = 0; k < n; k++) {
+            const auto& s = specs[k];
+            if (!s.column) return fail(ctx, GPUDB_E_INVALID, "colbin: a load spec names no column");
+            const gpudb::ColbinDesc& d = f.find(s.column_index);
+            const size_t want = gpudb::cudaTypeBytes(td.col(s.column).cudaType);
+            const std::string what = std::string("colbin: column ") + std::to_string(s.column_index) + " -> " +
+                                     table + "." + s.column;
+            const unsigned char* src = f.payload(d);
+            std::vector<unsigned char> conv;
+            size_t width = gpudb::ColbinFile::width(d);
+            switch (s.transform) {
+                case GPUDB_COLBIN_AS_IS:
+                    if (d.dtype == 1 || d.dtype == 4 || width != want)
+                        return fail(ctx, GPUDB_E_INVALID, what + ": stored type does not match the column as is");
+                    break;
+                case GPUDB_COLBIN_WIDEN: {
+                    if ((d.dtype != 0 && d.dtype != 2) || want != 8)
+                        return fail(ctx, GPUDB_E_INVALID, what + ": widening needs an int32 source and an int64 column");
+                    conv.resize(rows * 8);
+                    for (uint64_t i = 0; i < rows; i++) {
+                        int32_t v;
+                        std::memcpy(&v, src + i * 4, 4);
+                        const int64_t w = v;
+                        std::memcpy(conv.data() + i * 8, &w, 8);
+                    }
+                    width = 8;
+                    break;
+                }
+                case GPUDB_COLBIN_DECIMAL: {
+                    if (d.dtype != 1 || want != 8 || s.scale <= 0)
+                        return fail(ctx, GPUDB_E_INVALID,
+                                    what + ": decimals need a float32 source, an int64 column and a positive scale");
+                    conv.resize(rows * 8);
+                    for (uint64_t i = 0; i < rows; i++) {
+                        float v;
+                        std::memcpy(&v, src + i * 4, 4);
+                        const int64_t w = std::llround((double)v * (double)s.scale);
+                        std::memcpy(conv.data() + i * 8, &w, 8);
+                    }
+                    width = 8;
+                    break;
+                }
+                case GPUDB_COLBIN_DAYS: {
+                    if (d.dtype != 2 || want != 4)
+                        return fail(ctx, GPUDB_E_INVALID, what + ": day numbers need a date source and an int32 column");
+                    conv.resize(rows * 4);
+                    for (uint64_t i = 0; i < rows; i++) {
+                        int32_t v;
+                        std::memcpy(&v, src + i * 4, 4);
+                        const int32_t w = gpudb::colbinDayNumber(v);
+                        std::memcpy(conv.data() + i * 4, &w, 4);
+                    }
+                    break;
+                }
+                default: return fail(ctx, GPUDB_E_INVALID, what + ": unknown transform");
+            }
+            ctx->qc->ex.uploadColumn(s.column, table, conv.empty() ? (const void*)src : conv.data(), rows, width);
+            // the source (mapped file or converted copy) must outlive the copy
+            const cudaError_t e = cudaStreamSynchronize(ctx->qc->ex.stream());
+            if (e != cudaSuccess) return fail(ctx, GPUDB_E_CUDA, cudaGetErrorString(e));
+        }
         return GPUDB_OK;
     } catch (const std::exception& e) {
         return fail(ctx, GPUDB_E_INVALID, e.what());

@@ -205,6 +205,19 @@ class Context:
         self._keep.append(t)
         self.register_column(table, column, t.data_ptr(), t.numel(), t.element_size())
 
+    def load_colbin(self, path: str, table: str, specs) -> None:
+        """Upload columns of a .colbin v2 file into resident HBM as `table`'s
+        columns. `specs`: (source field index, engine column, transform,
+        scale) tuples, transform one of _lib.COLBIN_AS_IS / WIDEN / DECIMAL
+        / DAYS."""
+        arr = (_lib.ColbinLoadSpec * len(specs))()
+        names = [c.encode() for _, c, _, _ in specs]
+        for k, (idx, _, tr, sc) in enumerate(specs):
+            arr[k] = _lib.ColbinLoadSpec(idx, names[k], tr, sc)
+        check(self._lib.gpudb_colbin_load(self.handle, path.encode(), table.encode(), arr, len(specs)), self.handle)
+        rows = colbin_inspect(path)["rows"]
+        self._table_rows[table] = rows
+
     def register_host_column(self, table: str, column: str, host_ptr: int, rows: int, elem_bytes: int) -> None:
         """A pinned host column (gpudb_host_alloc) read in place by kernels
         that materialise it late; see gpudb_register_host_column."""
@@ -342,3 +355,14 @@ def compile_check(source: str) -> tuple:
 
 def templates() -> List[str]:
     return get_string(_lib.load().gpudb_list_templates).split(",")
+
+
+def colbin_inspect(path: str) -> dict:
+    """Header and column directory of a .colbin v2 file (no GPU needed)."""
+    lib = _lib.load()
+    rows, n = C.c_uint64(), C.c_uint32()
+    cols = (_lib.ColbinColumn * 256)()
+    check(lib.gpudb_colbin_inspect(path.encode(), C.byref(rows), C.byref(n), cols, 256))
+    return {"rows": rows.value, "columns": [{"index": c.column_index, "dtype": c.dtype, "fixed_width": c.fixed_width,
+                                               "offset": c.offset, "size_bytes": c.size_bytes}
+                                              for c in cols[:min(n.value, 256)]]}

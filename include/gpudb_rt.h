@@ -138,6 +138,41 @@ int gpudb_upload_column(gpudb_ctx* ctx, const char* table, const char* column, c
  * row fails (status < 0, message in gpudb_last_error) instead of streaming it. */
 int gpudb_register_host_column(gpudb_ctx* ctx, const char* table, const char* column, const void* host,
                                uint64_t rows, int elem_bytes);
+
+/* ---- .colbin v2 ingest (reference: colbin::loadColumnsFromBinary,
+ *      src/infra.h:583-670; format src/infra.h:512-560) ----------------
+ * A .colbin file: 48-byte header (magic "TPCHCB01", version 2, column
+ * count, row count), 32-byte column descriptors, 16 KiB-aligned payloads.
+ * The file is memory-mapped and checked the way the reference checks it
+ * (magic, version, directory and payloads inside the file, payload bytes =
+ * rows x type width). */
+typedef struct gpudb_colbin_column {
+    int32_t column_index; /* source .tbl field index */
+    uint8_t dtype;        /* 0 int32, 1 float32, 2 date YYYYMMDD (int32), 3 char, 4 fixed-width chars */
+    uint16_t fixed_width; /* bytes per value of dtype 4 */
+    uint64_t offset;      /* payload offset in the file */
+    uint64_t size_bytes;
+} gpudb_colbin_column;
+/* Header and column directory of a .colbin file; no GPU needed. Up to
+ * `cap` descriptors are copied; *ncols receives the file's count. */
+int gpudb_colbin_inspect(const char* path, uint64_t* rows, uint32_t* ncols, gpudb_colbin_column* cols, uint32_t cap);
+
+#define GPUDB_COLBIN_AS_IS 0   /* int32 / date / char stored at the engine column's width */
+#define GPUDB_COLBIN_WIDEN 1   /* int32 or date -> int64 */
+#define GPUDB_COLBIN_DECIMAL 2 /* float32 -> int64 round(x * scale): the engine's exact fixed point */
+#define GPUDB_COLBIN_DAYS 3    /* date YYYYMMDD -> int32 days since 1992-01-01 */
+typedef struct gpudb_colbin_load_spec {
+    int32_t column_index; /* source field index in the file */
+    const char* column;   /* engine column of `table` it becomes */
+    int32_t transform;    /* GPUDB_COLBIN_* */
+    int32_t scale;        /* GPUDB_COLBIN_DECIMAL: e.g. 100 for cents */
+} gpudb_colbin_load_spec;
+/* Upload the listed columns of a .colbin file into resident HBM as
+ * `table`'s columns (as gpudb_upload_column does), converting each to the
+ * engine column's type. The engine column's width must match the
+ * transform's result. Returns once the copies are complete. */
+int gpudb_colbin_load(gpudb_ctx* ctx, const char* path, const char* table, const gpudb_colbin_load_spec* specs,
+                      int n);
 /* registerTableRowCount. */
 int gpudb_register_rows(gpudb_ctx* ctx, const char* table, uint64_t rows);
 /* registerAllocatedBuffer: caller-owned device buffer (not freed). */
