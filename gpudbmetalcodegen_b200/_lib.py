@@ -80,6 +80,7 @@ _SIGNATURES = [
     ("gpudb_colbin_inspect", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                        C.POINTER(ColbinColumn), C.c_uint32]),
     ("gpudb_colbin_load", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(ColbinLoadSpec), C.c_int]),
+    ("gpudb_sql_to_spec", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t]),
     ("gpudb_register_rows", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),
     ("gpudb_register_buffer", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_int]),
     ("gpudb_register_symbol", C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64]),

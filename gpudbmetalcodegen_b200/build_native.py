@@ -42,6 +42,7 @@ HOST_SOURCES = [
     "capi/gpudb_capi.cpp",
     "datagen/datagen.cpp",
     "io/colbin.cpp",
+    "sql/sql_frontend.cpp",
 ]
 CUDA_SOURCES: list[str] = [
     "kernels/noalloc_distinct.cu",

@@ -13,6 +13,7 @@
 #include "../../../include/gpudb_rt.h"
 #include "../execution/query_engine.h"
 #include "../io/colbin.h"
+#include "../sql/sql_frontend.h"
 #include "../planning/plan_builder.h"
 
 struct gpudb_ctx {
@@ -212,6 +213,18 @@ int gpudb_register_host_column(gpudb_ctx* ctx, const char* table, const char* co
         return GPUDB_OK;
     } catch (const std::exception& e) {
         return fail(ctx, GPUDB_E_INVALID, e.what());
+    }
+}
+
+int gpudb_sql_to_spec(const char* sql, char* spec, size_t cap) {
+    if (!sql || (!spec && cap)) return fail(nullptr, GPUDB_E_INVALID, "bad argument");
+    try {
+        const std::string s = gpudb::sqlToSpec(sql);
+        if (s.size() + 1 > cap) return fail(nullptr, GPUDB_E_INVALID, "spec buffer too small");
+        std::memcpy(spec, s.c_str(), s.size() + 1);
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        return fail(nullptr, GPUDB_E_PLAN, e.what());
     }
 }
 

@@ -205,6 +205,10 @@ class Context:
         self._keep.append(t)
         self.register_column(table, column, t.data_ptr(), t.numel(), t.element_size())
 
+    def run_sql(self, sql: str, tune: str = "", collect: bool = True) -> tuple:
+        """Run a SELECT through the template its shape maps to (sql_to_spec)."""
+        return self.run(sql_to_spec(sql), tune, collect=collect)
+
     def load_colbin(self, path: str, table: str, specs) -> None:
         """Upload columns of a .colbin v2 file into resident HBM as `table`'s
         columns. `specs`: (source field index, engine column, transform,
@@ -366,3 +370,11 @@ def colbin_inspect(path: str) -> dict:
     return {"rows": rows.value, "columns": [{"index": c.column_index, "dtype": c.dtype, "fixed_width": c.fixed_width,
                                                "offset": c.offset, "size_bytes": c.size_bytes}
                                               for c in cols[:min(n.value, 256)]]}
+
+
+def sql_to_spec(sql: str) -> str:
+    """The pipeline-template spec of a SELECT over the engine's tables
+    (no GPU needed); raises GpudbError naming what does not map."""
+    buf = C.create_string_buffer(1024)
+    check(_lib.load().gpudb_sql_to_spec(sql.encode(), buf, 1024))
+    return buf.value.decode()

@@ -89,6 +89,17 @@ int gpudb_compare_canonical(const char* got, const char* expected, double abs_to
  * (column pointer, rows) like the reference's .maxkeys.json cache. */
 int gpudb_register_max_key(gpudb_ctx* ctx, const char* column, long long* max_out);
 
+/* SQL front end (reference: query_analyzer.cpp:640-727 over libpg_query,
+ * then buildMetalPlan by query shape). Maps a SELECT over the engine's
+ * tables to the spec string of the pipeline template that computes it
+ * (Q1 / Q6 shapes over fact, the dim-probe semi-join grouped with ORDER BY
+ * revenue DESC LIMIT k or as rows, the zprobe group-by, the zbuild-zprobe
+ * hash join); constants are integers in the columns' own units. No GPU
+ * needed. Copies the NUL-terminated spec into `spec` (up to `cap` bytes)
+ * and returns GPUDB_OK, or GPUDB_E_PLAN with the reason in
+ * gpudb_last_error(NULL, ...). */
+int gpudb_sql_to_spec(const char* sql, char* spec, size_t cap);
+
 /* Template names understood by gpudb_query_prepare, comma separated. */
 size_t gpudb_list_templates(char* buf, size_t cap);
 /* Library version / build string. */

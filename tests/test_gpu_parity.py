@@ -157,6 +157,20 @@ def test_join_rows_parity(ctx, spec, tune):
     assert res.columns == ["row", "key", "revenue"]
 
 
+def test_sql_runs_through_the_templates(ctx, fact_small):
+    """SELECTs over the engine's tables run through the template their
+    shape maps to and give the oracle's answers."""
+    d, p = load_join(ctx, 100_000, 400_000, seed=19)
+    res, _ = ctx.run_sql("SELECT p_fk, SUM(p_price * (100 - p_discount)) AS revenue FROM dim, probe "
+                         "WHERE b_key = p_fk AND b_segment = 2 AND b_order_day < 900 AND p_ship_day > 1000 "
+                         "GROUP BY p_fk ORDER BY revenue DESC, p_fk LIMIT 7")
+    assert res.rows == O.join_topk(d, p, seg=2, od_lt=900, ship_gt=1000, k=7)[0]
+    ctx.upload_table("fact", fact_small)
+    res, _ = ctx.run_sql("select sum(f_price * f_discount) from fact where f_ship_day >= 0 and f_ship_day < 3000 "
+                         "and f_discount between 0 and 10 and f_quantity < 51")
+    assert res.rows == [(O.q6(fact_small, 0, 3000, 0, 10, 51),)]
+
+
 def test_join_topk_ties_break_by_key(ctx):
     # every probe row carries the same revenue: ranking is decided by key
     d = W.gen_dim(5000, seed=4)
