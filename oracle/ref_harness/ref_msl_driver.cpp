@@ -114,6 +114,38 @@ MetalQueryPlan joinPlan() {
     return plan;
 }
 
+// The same join with its matching probe rows written out by the
+// reference's Materialize operator (metal_operators.cpp:618-643): row id,
+// key and revenue per match, at atomic output positions.
+MetalQueryPlan joinRowsPlan() {
+    MetalQueryPlan plan;
+    plan.name = "JOINROWS";
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("dim", "row", "i");
+        scan->addColumn("b_key", "int");
+        scan->addColumn("b_order_day", "int");
+        scan->addColumn("b_segment", "char");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "b_segment[i] == 1 && b_order_day[i] < 1170");
+        auto bm = std::make_unique<MetalBitmapBuild>(std::move(sel), "d_jb_bitmap", "b_key[i]", "(maxKey + 31) / 32");
+        plan.phases.push_back(makePhase("JOINROWS_build_bitmap", std::move(bm), 256));
+    }
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("probe", "row", "i");
+        scan->addColumn("p_fk", "int");
+        scan->addColumn("p_ship_day", "int");
+        scan->addColumn("p_price", "float");
+        scan->addColumn("p_discount", "float");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "p_ship_day[i] > 1170");
+        auto pr = std::make_unique<MetalBitmapProbe>(std::move(sel), "d_jb_bitmap", "p_fk[i]");
+        auto mt = std::make_unique<MetalMaterialize>(std::move(pr), "d_jr_n", "1");
+        mt->addColumn("d_jr_row", "uint", "(uint)i", "row", "n_probe");
+        mt->addColumn("d_jr_key", "int", "p_fk[i]", "key", "n_probe");
+        mt->addColumn("d_jr_rev", "float", "p_price[i] * (1.0f - p_discount[i])", "revenue", "n_probe");
+        plan.phases.push_back(makePhase("JOINROWS_probe_materialize", std::move(mt), 1024));
+    }
+    return plan;
+}
+
 MetalQueryPlan groupbyPlan() {
     MetalQueryPlan plan;
     plan.name = "GROUPBY";
@@ -262,8 +294,9 @@ int main(int argc, char** argv) {
     emitPlan(*q1, out, manifest, true);
     emitPlan(*q6, out, manifest, false);
     emitPlan(joinPlan(), out, manifest, false);
+    emitPlan(joinRowsPlan(), out, manifest, false);
     emitPlan(groupbyPlan(), out, manifest, false);
     manifest << "\n}\n";
-    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,GROUPBY}.cpp and manifest.json\n";
+    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,JOINROWS,GROUPBY}.cpp and manifest.json\n";
     return 0;
 }

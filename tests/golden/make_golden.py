@@ -62,6 +62,14 @@ def main():
                          "input_checksum": checksum(list(d.values()) + list(p.values())),
                          "ref": {"keys": [int(k) for k in keys], "revenue": [float(rev[k]) for k in keys]}})
 
+    b = rk.run("JOINROWS", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    cnt = int(b["d_jr_n"][0])
+    rows = sorted(zip(b["d_jr_row"][:cnt].tolist(), b["d_jr_key"][:cnt].tolist(), b["d_jr_rev"][:cnt].tolist()))
+    out["cases"].append({"plan": "JOINROWS", "dim_rows": nd, "probe_rows": npr, "seed": seed,
+                         "input_checksum": checksum(list(d.values()) + list(p.values())),
+                         "ref": {"row": [r for r, _, _ in rows], "key": [k for _, k, _ in rows],
+                                 "revenue": [float(v) for _, _, v in rows]}})
+
     n, seed, thr, card = 100_000, 5, 5000, 1000
     m = W.gen_mix(n, nranks=1 << 20, dim_rows=1000, seed=seed)
     cols = {"m_rank_u": m["m_rank_u"], "m_filter": m["m_filter"], "m_value": m["m_value"].astype(np.float32)}

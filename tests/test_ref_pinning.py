@@ -98,6 +98,26 @@ def test_oracle_matches_reference_join(case):
     check_join(case["ref"], d, p)
 
 
+def check_join_rows(ref, d, p):
+    """The reference's materialised join rows: the same (row, key) pairs as
+    the oracle, its float revenue within the golden tolerance of the exact
+    one (1e-4 currency units)."""
+    exp = O.join_rows(d, p)
+    assert ref["row"] == [r for r, _, _ in exp]
+    assert ref["key"] == [k for _, k, _ in exp]
+    for a, (_, _, v) in zip(ref["revenue"], exp):
+        assert close(a, v / 1e4)
+
+
+@pytest.mark.parametrize("case", cases("JOINROWS"), ids=lambda c: f"p{c['probe_rows']}")
+def test_oracle_matches_reference_join_rows(case):
+    d = W.gen_dim(case["dim_rows"], seed=case["seed"])
+    p = W.gen_probe(case["probe_rows"], dim_rows=case["dim_rows"], seed=case["seed"])
+    assert checksum(list(d.values()) + list(p.values())) == case["input_checksum"]
+    assert len(case["ref"]["row"]) > 100
+    check_join_rows(case["ref"], d, p)
+
+
 def check_groupby(ref, m, thr, card):
     k, c, s = O.mix_groupby(m, "m_rank_u", thr, card)
     assert list(k) == ref["keys"]
@@ -142,6 +162,11 @@ def test_live_reference_matches_oracle():
     b = rk.run("JOIN", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
     keys = np.nonzero(b["d_revenue"] > 0)[0]
     check_join({"keys": [int(k) for k in keys], "revenue": [float(b["d_revenue"][k]) for k in keys]}, d, p)
+    b = rk.run("JOINROWS", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    n = int(b["d_jr_n"][0])
+    rows = sorted(zip(b["d_jr_row"][:n].tolist(), b["d_jr_key"][:n].tolist(), b["d_jr_rev"][:n].tolist()))
+    check_join_rows({"row": [r for r, _, _ in rows], "key": [k for _, k, _ in rows],
+                     "revenue": [float(v) for _, _, v in rows]}, d, p)
     m = W.gen_mix(40_000, nranks=1 << 20, dim_rows=1000, seed=404)
     cols = {"m_rank_u": m["m_rank_u"], "m_filter": m["m_filter"], "m_value": m["m_value"].astype(np.float32)}
     b = rk.run("GROUPBY", cols, {"mix": 40_000}, {"card": 500}, scalars={"thr": 7000, "card": 500})
