@@ -665,7 +665,7 @@ def run_aggmodes(args):
     world, rank, local = dist_info()
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "a measurement of this build's strategies only"}))
+            print(json.dumps({"impl": "reference", "unavailable": "a measurement of the engine's own aggregation strategies only"}))
         return
     torch.cuda.set_device(local)
     rows = args.zprobe_rows // 2

@@ -11,7 +11,7 @@ from .engine import Context, Query, Result, Timing, compare_canonical, compile_c
 # Plans compiled ahead of time into the in-tree cubin cache by prewarm().
 STANDARD_PLANS = [
     ("template=q1", ""), ("template=q1", "scan=direct"), ("template=q6", ""), ("template=q6", "scan=direct"),
-    ("template=join_topk", ""), ("template=join_topk", "scan=direct"),
+    ("template=join_topk", ""), ("template=join_topk", "scan=direct"), ("template=join_rows", ""),
     ("template=groupby", ""), ("template=groupby", "smem=11"), ("template=groupby", "layout=bucket8"),
     ("template=hashjoin", ""), ("template=hashjoin", "smem=11"),
     ("template=colmax;table=dim;col=b_key", "bs=512;scan=direct"),
