@@ -68,7 +68,7 @@ std::vector<Tok> tokenize(const std::string& s) {
 
 // ---- expressions --------------------------------------------------------
 struct Expr {
-    enum Kind { Col, Num, Str, Bin, Func } kind;
+    enum Kind { Col, Num, Str, Bin, Func } kind = Col;
     std::string name;  // column / function name, operator
     long long num = 0;
     bool star = false;  // count(*)
@@ -91,6 +91,13 @@ struct Expr {
     }
 };
 using P = std::shared_ptr<Expr>;
+
+P node(Expr::Kind k, const std::string& name) {
+    auto e = std::make_shared<Expr>();
+    e->kind = k;
+    e->name = name;
+    return e;
+}
 
 struct Pred {
     P lhs, rhs;
@@ -221,13 +228,13 @@ private:
         const Tok& t = t_[p_];
         if (t.kind == Tok::Number) {
             ++p_;
-            auto e = std::make_shared<Expr>(Expr{Expr::Num, ""});
+            auto e = node(Expr::Num, "");
             e->num = t.num;
             return e;
         }
         if (t.kind == Tok::String) {
             ++p_;
-            return std::make_shared<Expr>(Expr{Expr::Str, t.text});
+            return node(Expr::Str, t.text);
         }
         if (sym("-")) {
             P f = factor();
@@ -242,7 +249,7 @@ private:
         }
         const std::string name = ident();
         if (sym("(")) {
-            auto e = std::make_shared<Expr>(Expr{Expr::Func, name});
+            auto e = node(Expr::Func, name);
             if (sym("*")) {
                 e->star = true;
             } else {
@@ -252,10 +259,10 @@ private:
             if (!sym(")")) throw std::runtime_error("sql: expected ')' after the arguments of " + name);
             return e;
         }
-        return std::make_shared<Expr>(Expr{Expr::Col, name});
+        return node(Expr::Col, name);
     }
     static P bin(const std::string& op, P l, P r) {
-        auto e = std::make_shared<Expr>(Expr{Expr::Bin, op});
+        auto e = node(Expr::Bin, op);
         e->args = {std::move(l), std::move(r)};
         return e;
     }
