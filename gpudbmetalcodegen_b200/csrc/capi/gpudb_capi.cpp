@@ -250,7 +250,7 @@ int gpudb_colbin_load(gpudb_ctx* ctx, const char* path, const char* table, const
     try {
         cudaSetDevice(ctx->qc->ex.device());
         gpudb::ColbinFile f(path);
-        const gpudb::TableDef& td = gpudb::catalogTable(table);
+        const gpudb::TableDef td = gpudb::catalogTable(table);  // a copy: no reference tied to the name temporary
         const uint64_t rows = f.rows();
         for (int k = 0; k < n; k++) {
             const auto& s = specs[k];
