@@ -44,3 +44,21 @@ def test_seeds_reach_joint_moves():
     assert best == {"a": 0, "b": 0}
     best, bt, t0 = A.coordinate_descent(space, measure, seeds=[{"a": 1, "b": 1}, {"zzz": 3}])
     assert best == {"a": 1, "b": 1} and bt == 5.0 and t0 == 10.0
+
+
+def test_every_tuning_the_tuner_can_try_is_a_valid_plan():
+    """Each value of each searched parameter, and each seed, parses and
+    plans and compiles for its template (no GPU needed)."""
+    from gpudbmetalcodegen_b200 import autotune as A
+    from gpudbmetalcodegen_b200 import engine
+    specs = {"q1": "template=q1", "q6": "template=q6", "join_topk": "template=join_topk",
+             "groupby": "template=groupby", "hashjoin": "template=hashjoin"}
+    for tpl, space in A.SPACES.items():
+        tunes = [f"{k}={v}" for k, vals in space.items() for v in vals]
+        tunes += [";".join(f"{k}={v}" for k, v in seed.items()) for seed in A.SEEDS.get(tpl, [])]
+        for t in tunes:
+            if "layout=bucket8" in t and tpl == "join_topk":
+                continue
+            q = engine.Query(specs[tpl], t)
+            assert "phase 0" in q.plan, (tpl, t)
+            q.close()
