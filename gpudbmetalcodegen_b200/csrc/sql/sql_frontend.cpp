@@ -55,7 +55,7 @@ std::vector<Tok> tokenize(const std::string& s) {
             std::string sym(1, c);
             for (const char* t : two)
                 if (s.compare(i, 2, t) == 0) sym = t;
-            if (sym.size() == 1 && std::string("=<>*+-/(),;").find(c) == std::string::npos)
+            if (sym.size() == 1 && std::string("=<>*+-/%(),;").find(c) == std::string::npos)
                 throw std::runtime_error(std::string("sql: unexpected character '") + c + "'");
             if (sym == "!=") sym = "<>";
             out.push_back({Tok::Symbol, sym});
@@ -218,7 +218,7 @@ private:
     }
     P term() {
         P l = factor();
-        while (t_[p_].kind == Tok::Symbol && (t_[p_].text == "*" || t_[p_].text == "/")) {
+        while (t_[p_].kind == Tok::Symbol && (t_[p_].text == "*" || t_[p_].text == "/" || t_[p_].text == "%")) {
             const std::string op = t_[p_++].text;
             l = bin(op, l, factor());
         }
@@ -313,6 +313,8 @@ public:
         if (from == std::set<std::string>{"dim", "probe"}) return semiJoin();
         if (from == std::set<std::string>{"zprobe"}) return groupBy();
         if (from == std::set<std::string>{"zbuild", "zprobe"}) return hashJoin();
+        if (from == std::set<std::string>{"mix"}) return mix();
+        if (from == std::set<std::string>{"mix", "mixdim"}) return mixJoin();
         throw std::runtime_error("sql: no plan template reads the tables of this query");
     }
 
@@ -459,6 +461,53 @@ private:
         itemsIn({"z_key", "zb_key", "count(*)", "sum(zb_payload)"}, "hash join");
         orderedBy({"z_key", "zb_key"}, "hash join");
         return "template=hashjoin";
+    }
+
+    // The mixed-workload templates over `mix` (the batch path's query
+    // shapes): filtered count + sum, grouped by key % card, top-k of it.
+    std::string mix() {
+        if (!joins_.empty()) throw std::runtime_error("sql: mix takes no join predicate");
+        const long long thr = need("m_filter", "<", "mix query");
+        noneLeft("mix query");
+        const std::string t = ";thr=" + std::to_string(thr);
+        if (q_.groupBy.empty()) {
+            itemsIn({"count(*)", "sum(m_value)"}, "filtered aggregate");
+            orderedBy({}, "filtered aggregate");
+            return "template=mix_agg" + t;
+        }
+        // GROUP BY <key column> % <card>
+        const P g = q_.groupBy.size() == 1 ? q_.groupBy[0] : nullptr;
+        if (!g || g->kind != Expr::Bin || g->name != "%" || g->args[0]->kind != Expr::Col ||
+            g->args[1]->kind != Expr::Num || g->args[1]->num < 1 ||
+            (g->args[0]->name != "m_rank_u" && g->args[0]->name != "m_rank_z"))
+            throw std::runtime_error("sql: mix is grouped by m_rank_u % <card> or m_rank_z % <card>");
+        const std::string key = g->args[0]->name, gk = g->canon();
+        const long long card = g->args[1]->num;
+        itemsIn({gk, "count(*)", "sum(m_value)"}, "mix group-by");
+        const std::string base = ";key=" + key + ";card=" + std::to_string(card) + t + ";groups=" + std::to_string(card);
+        if (q_.limit < 0) {
+            orderedBy({}, "mix group-by");
+            return "template=mix_groupby" + base;
+        }
+        if (q_.limit < 1 || q_.limit > 32) throw std::runtime_error("sql: the mix top-k needs LIMIT 1..32");
+        if (q_.orderBy.empty() || q_.orderBy[0].first->canon() != "sum(m_value)" || !q_.orderBy[0].second)
+            throw std::runtime_error("sql: the mix top-k orders by sum(m_value) descending");
+        for (size_t i = 1; i < q_.orderBy.size(); i++)
+            if (q_.orderBy[i].first->canon() != gk || q_.orderBy[i].second)
+                throw std::runtime_error("sql: ties of the mix top-k are broken by the group key ascending");
+        return "template=mix_topk" + base + ";k=" + std::to_string(q_.limit);
+    }
+
+    std::string mixJoin() {
+        if (!joined("m_fk", "md_key") || joins_.size() != 1)
+            throw std::runtime_error("sql: mix and mixdim join on m_fk = md_key");
+        const long long thr = need("m_filter", "<", "mix join");
+        const long long attr = need("md_attr", "<", "mix join");
+        noneLeft("mix join");
+        if (!q_.groupBy.empty()) throw std::runtime_error("sql: the mix join is not grouped");
+        itemsIn({"count(*)", "sum(m_value)"}, "mix join");
+        orderedBy({}, "mix join");
+        return "template=mix_join;thr=" + std::to_string(thr) + ";attr_lt=" + std::to_string(attr);
     }
 
     Select q_;

@@ -14,7 +14,10 @@
 // numbers). The analyser matches the statement to a template (Q1 and Q6
 // shapes over `fact`, the semi-join of `dim` and `probe` as a grouped
 // top-k or as materialised rows, the group-by over `zprobe`, the hash join
-// of `zbuild` and `zprobe`) and returns that template's spec string.
+// of `zbuild` and `zprobe`, and the mixed-workload shapes over `mix`:
+// filtered count + sum, the same through the `mixdim` semi-join, grouped by
+// a key modulo a cardinality, and its top-k) and returns that template's
+// spec string.
 // ===================================================================
 
 #include <string>

@@ -38,6 +38,13 @@ Q3 = """SELECT p_fk, SUM(p_price * (100 - p_discount)) AS revenue
     ("select z_key, count(*), sum(z_value) from zprobe group by z_key", "template=groupby"),
     ("select z_key, count(*), sum(zb_payload) from zbuild, zprobe where zb_key = z_key group by z_key order by z_key",
      "template=hashjoin"),
+    ("select count(*), sum(m_value) from mix where m_filter < 5000", "template=mix_agg;thr=5000"),
+    ("select m_rank_z % 1000, count(*), sum(m_value) from mix where m_filter < 5000 group by m_rank_z % 1000",
+     "template=mix_groupby;key=m_rank_z;card=1000;thr=5000;groups=1000"),
+    ("select m_rank_u % 64, sum(m_value) from mix where m_filter < 900 group by m_rank_u % 64 "
+     "order by sum(m_value) desc, m_rank_u % 64 limit 5", "template=mix_topk;key=m_rank_u;card=64;thr=900;groups=64;k=5"),
+    ("select count(*), sum(m_value) from mix, mixdim where m_fk = md_key and md_attr < 300 and m_filter < 7000",
+     "template=mix_join;thr=7000;attr_lt=300"),
 ])
 def test_benchmark_queries_map_to_their_templates(sql, spec):
     assert sql_to_spec(sql) == spec
@@ -56,6 +63,10 @@ def test_benchmark_queries_map_to_their_templates(sql, spec):
     ("select * from lineitem", "expected a name"),
     ("select x from nowhere", "no plan template reads"),
     ("select z_key from zprobe where", "expected a name"),
+    ("select m_value % 10, count(*) from mix where m_filter < 5 group by m_value % 10", "grouped by m_rank_u %"),
+    ("select count(*), sum(m_value) from mix", "m_filter < <constant>"),
+    ("select m_rank_u % 8, sum(m_value) from mix where m_filter < 9 group by m_rank_u % 8 order by sum(m_value) limit 3",
+     "sum(m_value) descending"),
 ])
 def test_unmapped_queries_are_refused_with_the_reason(sql, why):
     with pytest.raises(GpudbError) as e:
