@@ -104,10 +104,16 @@ class TuneCache:
     def put(self, template: str, rows: int, tune: str, ms: float, default_ms: float) -> None:
         self.data[self.key(template, rows)] = {"tune": tune, "ms": ms, "default_ms": default_ms,
                                                "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
-        self.path.parent.mkdir(parents=True, exist_ok=True)
-        tmp = self.path.with_suffix(".tmp")
-        tmp.write_text(json.dumps(self.data, indent=1, sort_keys=True))
-        tmp.replace(self.path)
+        # replicas of a multi-GPU run tune at the same time: each writes its
+        # own temporary file and renames it over the cache (last one wins);
+        # a cache that cannot be written only costs a re-tune later
+        try:
+            self.path.parent.mkdir(parents=True, exist_ok=True)
+            tmp = self.path.with_suffix(f".{os.getpid()}.tmp")
+            tmp.write_text(json.dumps(self.data, indent=1, sort_keys=True))
+            tmp.replace(self.path)
+        except OSError:
+            pass
 
 
 def _tune_string(cfg: Dict[str, str]) -> str:

@@ -62,3 +62,28 @@ def test_every_tuning_the_tuner_can_try_is_a_valid_plan():
             q = engine.Query(specs[tpl], t)
             assert "phase 0" in q.plan, (tpl, t)
             q.close()
+
+
+def _writer(path, i):
+    from gpudbmetalcodegen_b200 import autotune as A
+    c = A.TuneCache(path)
+    for j in range(100):
+        c.put("q1", 1000, f"bs={32 * (i + 1)}", float(j), 2.0)
+
+
+def test_replicas_writing_the_cache_at_once_leave_a_valid_file(tmp_path):
+    """Ranks of a multi-GPU run tune concurrently and all write the same
+    per-device cache: none may fail, and the file stays readable."""
+    import json
+    import multiprocessing as mp
+    from gpudbmetalcodegen_b200 import autotune as A
+    path = tmp_path / "dev.json"
+    ps = [mp.get_context("spawn").Process(target=_writer, args=(path, i)) for i in range(4)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(timeout=120)
+    assert [p.exitcode for p in ps] == [0, 0, 0, 0]
+    data = json.loads(path.read_text())
+    assert data[A.TuneCache.key("q1", 1000)]["tune"] in {f"bs={32 * (i + 1)}" for i in range(4)}
+    assert not list(tmp_path.glob("*.tmp"))
