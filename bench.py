@@ -5,8 +5,10 @@ Default workload (the join configuration of the benchmark set): build side
 probe side 60M rows (fk, ship_day, price, discount); build filter segment==1
 AND order_day<1170, probe filter ship_day>1170, group by build key summing
 price*(100-discount) exactly in int64, top 10 by (sum desc, key asc).
-One step = one full query: bitmap semi-join build, exact group-count sizing
-(host read of the distinct counter), probe + hash group-by, top-k.
+One step = one full query of five kernels with no host round trip: bitmap
+semi-join build; probe listing the matched rows and popcounting the bitmap's
+keys; initialisation of the group table sized on the device from those two
+counters; gather + hash group-by of the listed rows; top-k.
 Seeded synthetic data of the configuration's shapes; inputs exceed the
 126 MB L2, so no flush is needed between steps.
 

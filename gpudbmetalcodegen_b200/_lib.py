@@ -149,6 +149,8 @@ _SIGNATURES = [
     ("gpudb_sizer_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float,
                                     C.c_uint64, C.POINTER(C.c_float)]),
     ("gpudb_sizer_predict", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    ("gpudb_column_minmax", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64), C.c_void_p]),
     ("gpudb_batch_create", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("gpudb_batch_free", None, [C.c_void_p]),
     ("gpudb_batch_set_queries", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

@@ -104,16 +104,36 @@ class TuneCache:
     def put(self, template: str, rows: int, tune: str, ms: float, default_ms: float) -> None:
         self.data[self.key(template, rows)] = {"tune": tune, "ms": ms, "default_ms": default_ms,
                                                "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
-        # replicas of a multi-GPU run tune at the same time: each writes its
-        # own temporary file and renames it over the cache (last one wins);
-        # a cache that cannot be written only costs a re-tune later
+        # replicas of a multi-GPU run tune at the same time: under an
+        # exclusive lock each re-reads the file, merges its own entry into
+        # it and renames its own temporary copy over it, so no replica's
+        # entry is lost; a cache that cannot be written only costs a
+        # re-tune later
+        tmp = self.path.with_suffix(f".{os.getpid()}.tmp")
         try:
             self.path.parent.mkdir(parents=True, exist_ok=True)
-            tmp = self.path.with_suffix(f".{os.getpid()}.tmp")
-            tmp.write_text(json.dumps(self.data, indent=1, sort_keys=True))
-            tmp.replace(self.path)
+            with open(self.path.with_suffix(".lock"), "a") as lk:
+                try:
+                    import fcntl
+                    fcntl.flock(lk.fileno(), fcntl.LOCK_EX)
+                except (ImportError, OSError):
+                    pass
+                try:
+                    merged = json.loads(self.path.read_text()) if self.path.exists() else {}
+                    if not isinstance(merged, dict):
+                        merged = {}
+                except (OSError, ValueError):
+                    merged = {}
+                merged[self.key(template, rows)] = self.data[self.key(template, rows)]
+                for k, v in merged.items():
+                    self.data.setdefault(k, v)
+                tmp.write_text(json.dumps(merged, indent=1, sort_keys=True))
+                tmp.replace(self.path)
         except OSError:
-            pass
+            try:
+                tmp.unlink()
+            except OSError:
+                pass
 
 
 def _tune_string(cfg: Dict[str, str]) -> str:

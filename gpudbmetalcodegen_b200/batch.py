@@ -142,6 +142,18 @@ def describe_difference(a, b) -> str:
 # ---------------------------------------------------------------------------
 # resident tables
 # ---------------------------------------------------------------------------
+def column_minmax(col, stream=None) -> Tuple[int, int]:
+    """(min, max) of a resident int32 / int64 device column, by the
+    library's own zone-map kernel (gpudb_column_minmax); (0, 0) when empty."""
+    lib = _lib.load()
+    lo, hi = C.c_int64(), C.c_int64()
+    st = lib.gpudb_column_minmax(C.c_void_p(col.data_ptr()), col.numel(), col.element_size(), C.byref(lo),
+                                 C.byref(hi), C.c_void_p(stream) if stream else None)
+    if st != 0:
+        raise RuntimeError(f"column_minmax failed: {_lib.last_error(None)}")
+    return int(lo.value), int(hi.value)
+
+
 class MixTables:
     """Resident mixed-workload tables: several mix tables (one Zipf exponent
     each for m_rank_z; m_rank_u is uniform) and one mixdim table, as
@@ -169,7 +181,7 @@ class MixTables:
                                           *(cols[c].data_ptr() for c in W.MIX_COLUMNS), stream)
             if st != 0:
                 raise RuntimeError(f"device generator failed: {_lib.last_error(None)}")
-            self.stats.append({c: (int(v.min()), int(v.max())) if rows else (0, 0) for c, v in cols.items()})
+            self.stats.append({c: column_minmax(v, stream) for c, v in cols.items()})
             self.tables.append(cols)
             if host:
                 self.host.append({c: v.cpu().numpy() for c, v in cols.items()})

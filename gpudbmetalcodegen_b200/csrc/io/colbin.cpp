@@ -74,7 +74,13 @@ ColbinFile::ColbinFile(const std::string& path) {
             if (d.offset > size_ || d.sizeBytes > size_ - d.offset)
                 throw std::runtime_error("colbin: payload of column " + std::to_string(d.columnIndex) +
                                          " beyond the end of " + path);
-            if (d.sizeBytes != rows_ * width(d))
+            // rows x width must not wrap: a huge row count with a tiny
+            // payload would otherwise pass the size check below
+            const uint64_t w = width(d);
+            if ((w == 0 && rows_ != 0) || (w != 0 && rows_ > (uint64_t)size_ / w))
+                throw std::runtime_error("colbin: " + std::to_string(rows_) + " rows of column " +
+                                         std::to_string(d.columnIndex) + " cannot fit in " + path);
+            if (d.sizeBytes != rows_ * w)
                 throw std::runtime_error("colbin: column " + std::to_string(d.columnIndex) + " holds " +
                                          std::to_string(d.sizeBytes) + " bytes, not rows x width");
             descs_.push_back(d);

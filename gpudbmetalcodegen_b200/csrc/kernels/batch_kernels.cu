@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -947,6 +948,31 @@ float elapsed(gpudb_batch* b) {
     return t;
 }
 
+// Zone-map statistics of a resident column: min and max of n int32 or
+// int64 values (the sizer's column features). One grid-stride pass, warp
+// shuffle reduction, one signed 64-bit atomicMin / atomicMax per warp.
+template <typename T>
+__global__ void __launch_bounds__(256) kColumnMinMax(const T* __restrict__ v, unsigned long long n,
+                                                     long long* __restrict__ out) {
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const long long x = (long long)__ldcs(v + i);
+        lo = x < lo ? x : lo;
+        hi = x > hi ? x : hi;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long a = __shfl_xor_sync(0xffffffffu, lo, o), b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31u) == 0u) {
+        atomicMin(out, lo);
+        atomicMax(out + 1, hi);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1316,6 +1342,46 @@ int gpudb_batch_stage_ms(gpudb_batch* b, double* ms) {
         return GPUDB_E_INVALID;
     }
     for (int i = 0; i < GPUDB_BATCH_STAGES; i++) ms[i] = b->stageMs[i];
+    return GPUDB_OK;
+}
+
+int gpudb_column_minmax(const void* column, uint64_t n, int elem_bytes, int64_t* min_out, int64_t* max_out,
+                        void* stream) {
+    if (!min_out || !max_out || (n && !column) || (elem_bytes != 4 && elem_bytes != 8)) {
+        gpudb::setThreadError("column_minmax: needs int32 / int64 elements and output pointers");
+        return GPUDB_E_INVALID;
+    }
+    if (n == 0) {
+        *min_out = 0;
+        *max_out = 0;
+        return GPUDB_OK;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int dev = 0, sms = 0;
+    B_CHECK(cudaGetDevice(&dev), GPUDB_E_NOGPU);
+    B_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), GPUDB_E_CUDA);
+    long long* d = nullptr;
+    B_CHECK(cudaMallocAsync((void**)&d, 2 * sizeof(long long), st), GPUDB_E_ALLOC);
+    const long long init[2] = {LLONG_MAX, LLONG_MIN};
+    long long host[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(d, init, sizeof init, cudaMemcpyHostToDevice, st);
+    const unsigned long long want = (n + 255) / 256;
+    const int blocks = (int)std::min<unsigned long long>(want, (unsigned long long)sms * 8);
+    if (e == cudaSuccess) {
+        if (elem_bytes == 4) kColumnMinMax<int><<<blocks, 256, 0, st>>>(static_cast<const int*>(column), n, d);
+        else kColumnMinMax<long long><<<blocks, 256, 0, st>>>(static_cast<const long long*>(column), n, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, sizeof host, cudaMemcpyDeviceToHost, st);
+    const cudaError_t f = cudaFreeAsync(d, st);
+    if (e == cudaSuccess) e = f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        gpudb::setThreadError(std::string("column_minmax: ") + cudaGetErrorString(e));
+        return GPUDB_E_CUDA;
+    }
+    *min_out = host[0];
+    *max_out = host[1];
     return GPUDB_OK;
 }
 

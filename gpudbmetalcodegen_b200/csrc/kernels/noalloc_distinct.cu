@@ -27,7 +27,10 @@
 //     race on it and produce wrong counts.
 //   * the first call on a device looks up the scratch array's device
 //     address (cudaGetSymbolAddress) with that device current; make that
-//     first call before starting any stream capture.
+//     first call before starting any stream capture. The address is kept
+//     until the process exits: a device reset (cudaDeviceReset, or a
+//     destroyed primary context) leaves it stale, so after one this entry
+//     point must not be called on that device again.
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -49,6 +49,14 @@ int gpudb_sizer_train(gpudb_sizer* s, const float* X, const float* Y, int n, int
                       uint64_t seed, float* final_loss);
 int gpudb_sizer_predict(gpudb_sizer* s, const float* X, int n, float* Y_out);
 
+/* ---- column statistics -------------------------------------------------- */
+/* Zone-map min / max of a device column of n int32 (elem_bytes 4) or int64
+ * (elem_bytes 8) values, on `stream` (NULL = legacy default); returns after
+ * the stream has finished. n = 0 gives (0, 0). These are the sizer's column
+ * features (the key / filter domain of a resident table). */
+int gpudb_column_minmax(const void* column, uint64_t n, int elem_bytes, int64_t* min_out, int64_t* max_out,
+                        void* stream);
+
 /* ---- batched mixed queries --------------------------------------------- */
 typedef struct gpudb_batch gpudb_batch;
 

@@ -207,16 +207,20 @@ void gpudb_host_free(void* p);
 /* No counterpart in the reference: an entry point for callers that cannot
  * allocate device memory on the call path (inside CUDA-graph capture, or
  * hosts whose allocator owns all device memory). Counts the distinct values
- * of key[i] % card over rows with filter[i] < thr — the result of the
- * "distinct" pipeline — and writes it to *out_count (device pointer), all
+ * of key[i] % card over rows with filter[i] < thr and writes the count to
+ * *out_count (device pointer). For non-negative keys that is the result of
+ * the "distinct" pipeline; a negative key is skipped here, where that
+ * pipeline reports a bounds error instead. All work runs
  * on `stream` (a cudaStream_t; NULL = legacy default stream). Inputs and
  * the output are the caller's device buffers; the scratch bitmap is a
  * static device array sized for card <= 2^22 (512 KiB, held by every GPU
  * that loads the library). card outside [1, 2^22] -> GPUDB_E_INVALID.
- * Negative keys are skipped. Calls share the scratch: calls that overlap on
- * the GPU race. The first call on a device resolves the scratch address and
- * should come before any stream capture. Asynchronous: read *out_count
- * after the stream has completed. */
+ * n = 0 writes 0. Calls share the scratch: calls that overlap on the GPU
+ * race. The first call on a device resolves the scratch address and should
+ * come before any stream capture; that address is kept for the life of the
+ * process, so a device reset (cudaDeviceReset, or destroying the primary
+ * context) invalidates this entry point for that device. Asynchronous:
+ * read *out_count after the stream has completed. */
 int gpudb_distinct_count_noalloc(const int32_t* key, const int32_t* filter, uint64_t n, int32_t thr, int64_t card,
                                  uint64_t* out_count, void* stream);
 

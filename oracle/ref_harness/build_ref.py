@@ -8,18 +8,21 @@
 3. Compiles those kernels as C++ against msl_cpu_shim.h into
    oracle/_ref/libref_kernels.so, loaded by oracle/ref_harness/ref_run.py.
 
-Needs the reference tree at /root/reference (present in the build container,
-not on GPU hosts); oracle/_ref/ is git-ignored.
+Needs the reference source tree: the directory named by the environment
+variable GPUDB_REFERENCE_ROOT, by default /root/reference (present in the
+build container, not on GPU hosts); oracle/_ref/ is git-ignored.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref"
-REF = Path("/root/reference")
+REF = Path(os.environ.get("GPUDB_REFERENCE_ROOT", "/root/reference"))
+
 REF_SOURCES = [
     "codegen/planning/metal_plan_builder.cpp",
     "codegen/operators/metal_operators.cpp",
@@ -28,6 +31,11 @@ REF_SOURCES = [
 ]
 REF_INCLUDES = ["codegen/planning", "codegen/operators", "codegen/core"]
 PLANS = ["Q1", "Q6", "JOIN", "JOINROWS", "GROUPBY"]
+
+
+def available() -> bool:
+    """True when the reference source tree is present on this host."""
+    return all((REF / s).is_file() for s in REF_SOURCES)
 
 
 def _run(cmd):
@@ -39,8 +47,8 @@ def _run(cmd):
 
 
 def build(force: bool = False) -> Path:
-    if not REF.exists():
-        raise RuntimeError("the reference tree is not available on this host")
+    if not available():
+        raise RuntimeError(f"the reference tree is not available on this host ({REF}; set GPUDB_REFERENCE_ROOT)")
     OUT.mkdir(exist_ok=True)
     lib = OUT / "libref_kernels.so"
     inputs = [HERE / "ref_msl_driver.cpp", HERE / "msl_cpu_shim.h", Path(__file__)] + [REF / s for s in REF_SOURCES]

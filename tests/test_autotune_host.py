@@ -69,6 +69,7 @@ def _writer(path, i):
     c = A.TuneCache(path)
     for j in range(100):
         c.put("q1", 1000, f"bs={32 * (i + 1)}", float(j), 2.0)
+        c.put(f"own{i}", 1000, f"bs={32 * (i + 1)}", float(j), 2.0)
 
 
 def test_replicas_writing_the_cache_at_once_leave_a_valid_file(tmp_path):
@@ -86,4 +87,7 @@ def test_replicas_writing_the_cache_at_once_leave_a_valid_file(tmp_path):
     assert [p.exitcode for p in ps] == [0, 0, 0, 0]
     data = json.loads(path.read_text())
     assert data[A.TuneCache.key("q1", 1000)]["tune"] in {f"bs={32 * (i + 1)}" for i in range(4)}
+    # each writer's own entry survives the others' writes (merged, not overwritten)
+    for i in range(4):
+        assert data[A.TuneCache.key(f"own{i}", 1000)]["tune"] == f"bs={32 * (i + 1)}"
     assert not list(tmp_path.glob("*.tmp"))

@@ -279,3 +279,16 @@ def test_query_array_equals_structs(tables):
         for name, _ in B.BatchQueryStruct._fields_:
             a, s = arr[i][name], getattr(st, name)
             assert int(a) == int(s or 0), (i, name, a, s)
+
+
+def test_column_minmax_kernel_matches_numpy():
+    """The zone-map kernel behind the sizer's column features (int32 and
+    int64, ragged lengths, negative values, empty)."""
+    import torch
+    from gpudbmetalcodegen_b200.batch import column_minmax
+    rng = np.random.default_rng(5)
+    for n, dt in ((1, np.int32), (1025, np.int32), (300_001, np.int64), (7, np.int64)):
+        a = rng.integers(-(1 << 40) if dt == np.int64 else -(1 << 30), 1 << 30, n).astype(dt)
+        t = torch.from_numpy(a).cuda()
+        assert column_minmax(t) == (int(a.min()), int(a.max()))
+    assert column_minmax(torch.empty(0, dtype=torch.int32, device="cuda")) == (0, 0)

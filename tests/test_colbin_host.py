@@ -60,3 +60,13 @@ def test_truncated_payload_and_size_mismatch_are_errors(tmp_path):
     assert "not rows x width" in e.value.message
     with pytest.raises(GpudbError):
         engine.colbin_inspect(str(tmp_path / "missing.colbin"))
+
+
+def test_row_count_that_overflows_rows_times_width_is_rejected(tmp_path):
+    # 2^62 int32 rows: rows x 4 wraps to 0 in 64 bits, matching a zero-byte
+    # payload unless the reader checks the product before comparing it
+    p = tmp_path / "wrap.colbin"
+    write_colbin(p, [(4, INT, np.zeros(0, np.int32), 0)], 1 << 62)
+    with pytest.raises(GpudbError) as e:
+        engine.colbin_inspect(str(p))
+    assert "cannot fit" in e.value.message

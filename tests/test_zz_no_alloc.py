@@ -47,6 +47,16 @@ def test_noalloc_distinct_matches_the_allocating_pipeline():
                 ctx.synchronize()
                 assert int(out.item()) == expect
 
+        # no rows: the count is 0 (the scratch still holds the last call's bits)
+        out.fill_(-1)
+        torch.cuda.synchronize()
+        st = lib.gpudb_distinct_count_noalloc(C.c_void_p(cols["m_rank_u"].data_ptr()),
+                                              C.c_void_p(cols["m_filter"].data_ptr()), 0, 5000, 1000,
+                                              C.c_void_p(out.data_ptr()), C.c_void_p(ctx.stream_ptr))
+        assert st == 0, _lib.last_error(None)
+        ctx.synchronize()
+        assert int(out.item()) == 0
+
         st = lib.gpudb_distinct_count_noalloc(C.c_void_p(cols["m_rank_u"].data_ptr()),
                                               C.c_void_p(cols["m_filter"].data_ptr()), n, 5000, (1 << 22) + 1,
                                               C.c_void_p(out.data_ptr()), C.c_void_p(ctx.stream_ptr))
