@@ -218,6 +218,16 @@ void CudaGridStrideScan::produce(CudaCodegen& cg, ConsumerFn consume) {
                         });
                     }
                 });
+                // Exit rule: the CTA must not exit while a bulk copy it issued
+                // is still writing its shared memory. Normally the consumers
+                // waited for every stage; after a timed-out wait (producer or
+                // consumer side) the producer itself waits, again bounded, for
+                // the last copy issued into each stage (tiles _sb_j - stages ..
+                // _sb_j - 1) before the block may leave the ring.
+                cg.addBlock("for (long long _dj = _sb_j > " + ST + " ? _sb_j - " + ST + " : 0; _dj < _sb_j; ++_dj)", [&]() {
+                    cg.addLine("if (!gpudb_mbar_wait(_sb_full + (int)(_dj % " + ST + "), (unsigned)((_dj / " + ST +
+                               ") & 1), gpudb_err)) { _sb_ok = false; break; }");
+                });
             });
         }, " else {");
         cg.increaseIndent();
@@ -793,6 +803,50 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
                 cg.addLine("default: break;");
             });
         });
+    } else if (st == Strategy::SharedPrivate) {
+        const int bs = cg.currentThreadgroupSize();
+        const int nacc = nb * na;
+        const std::string BS = S(bs);
+        // allocated before the scan below sizes its ring from what is left
+        const int poff = cg.allocDynamicSmem(nacc * bs * 8);
+        cg.addComment("keyed aggregation: thread-private accumulators in shared memory (" + S(nb) + " buckets x " +
+                      S(na) + " aggregates per thread, slot (bucket * " + S(na) + " + aggregate) * " + BS +
+                      " + thread: a warp's lanes hit consecutive words)");
+        cg.addLine("if (blockDim.x > " + BS + "u) { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); return; }");
+        cg.addLine("unsigned long long* const _kp_all = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(poff) +
+                   ");");
+        cg.addLine("unsigned long long* const _kp = _kp_all + threadIdx.x;");
+        cg.addLine("#pragma unroll");
+        cg.addLine("for (int _a = 0; _a < " + S(nacc) + "; ++_a) _kp[_a * " + BS + "] = 0ull;");
+        child_->produce(cg, [&]() {
+            emitValues();
+            cg.addBlock("if ((unsigned)_bucket < " + S(nb) + "u)", [&]() {
+                cg.addLine("unsigned long long* const _kq = _kp + _bucket * " + S(na * bs) + ";");
+                for (int j = 0; j < na; j++)
+                    cg.addLine("_kq[" + S(j * bs) + "] += (unsigned long long)_kv" + S(j) + ";");
+            }, " else { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); }");
+            consume();
+        });
+        cg.addComment("each warp sums whole slots over the block's threads, then one RED per non-zero slot");
+        cg.addLine("__syncthreads();");
+        cg.addBlock("for (int _a = (int)(threadIdx.x >> 5); _a < " + S(nacc) + "; _a += (int)(blockDim.x >> 5))", [&]() {
+            cg.addLine("unsigned long long _t = 0ull;");
+            cg.addLine("for (int _u = (int)(threadIdx.x & 31u); _u < (int)blockDim.x; _u += 32) _t += _kp_all[_a * " +
+                       BS + " + _u];");
+            cg.addLine("#pragma unroll");
+            cg.addLine("for (int _o = 16; _o > 0; _o >>= 1) _t += __shfl_xor_sync(0xffffffffu, _t, _o);");
+            cg.addLine("if ((threadIdx.x & 31u) != 0u || _t == 0ull) continue;");
+            cg.addLine("const long long _tot = (long long)_t;");
+            cg.addLine("const int _b = _a / " + S(na) + ", _j = _a % " + S(na) + ";");
+            cg.addBlock("switch (_j)", [&]() {
+                for (int j = 0; j < na; j++) {
+                    const auto& ag = aggregates_[j];
+                    cg.addLine("case " + S(j) + ": " + (ag.isWide ? "gpudb_acc128_add(" : "gpudb_acc64_add(") + out +
+                               " + _b * " + S(vpb) + " + " + S(ag.offset) + ", _tot); break;");
+                }
+                cg.addLine("default: break;");
+            });
+        });
     } else if (st == Strategy::Shared) {
         const int words = nb * vpb;
         const int soff = cg.allocDynamicSmem(words * 8);
@@ -845,7 +899,7 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
 }
 
 std::string CudaKeyedAgg::describe() const {
-    static const char* names[] = {"auto", "registers", "shared", "global", "registers-switch"};
+    static const char* names[] = {"auto", "registers", "shared", "global", "registers-switch", "shared-private"};
     return "KeyedAgg(" + outputArrayName_ + ", " + S(numBuckets_) + " buckets, " + S((long long)aggregates_.size()) +
            " aggs, " + names[(int)chosenStrategy()] + ") <- " + describeChain();
 }

@@ -284,8 +284,13 @@ public:
         int scaleDown = 0;
     };
     // Registers: predicated update of every bucket's accumulators per row;
-    // RegistersSwitch: a switch on the bucket, each row updates only its own.
-    enum class Strategy { Auto, Registers, Shared, Global, RegistersSwitch };
+    // RegistersSwitch: a switch on the bucket, each row updates only its own;
+    // SharedPrivate: the reference's thread-local arrays (metal_operators.cpp:
+    // 402-405) kept in shared memory instead of registers — every thread owns
+    // buckets x aggregates 64-bit slots, a row adds into its own bucket's
+    // slots by address (no switch, no divergence, few registers), and the
+    // block sums each slot over its threads at the end.
+    enum class Strategy { Auto, Registers, Shared, Global, RegistersSwitch, SharedPrivate };
     CudaKeyedAgg(std::unique_ptr<CudaOperator> child, const std::string& outputArrayName,
                  const std::string& bucketExpr, int numBuckets, int valuesPerBucket,
                  const std::string& sizeExpr = "");

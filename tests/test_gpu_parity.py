@@ -13,7 +13,9 @@ pytestmark = pytest.mark.gpu
 REL = 1e-12
 
 Q1_TUNES = ["", "scan=direct", "bs=256;tile=1024;stages=2", "bs=1024;tile=2048;stages=3", "bs=128;tile=512;stages=8",
-            "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3", "vec=4", "vec=2;bs=256", "vec=8;tile=2048"]
+            "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3", "vec=4", "vec=2;bs=256", "vec=8;tile=2048",
+            "keyed=5;bs=256;tile=512;stages=2;occ=2", "keyed=5;scan=direct", "keyed=5;bs=128;tile=256;occ=3",
+            "keyed=5;vec=2;bs=256;tile=512;stages=2", "keyed=5;bs=1024;tile=1024;stages=2"]
 
 
 def assert_q1_equal(res, expect):
@@ -77,15 +79,16 @@ def test_q1_misaligned_columns_fall_back_to_direct_loads(ctx):
         ctx.register_column("fact", name, t.data_ptr() + arr.itemsize, arr.shape[0] - 1, arr.itemsize)
     torch.cuda.synchronize()
     sub = {k: v[1:] for k, v in f.items()}
-    res, _ = ctx.run("template=q1")
-    assert_q1_equal(res, O.q1(sub))
+    for tune in ("", "keyed=5", "keyed=4"):
+        res, _ = ctx.run("template=q1", tune)
+        assert_q1_equal(res, O.q1(sub))
     del keep
 
 
 def test_q1_full_size(ctx):
     f = W.gen_fact(W.FACT_ROWS)
     ctx.upload_table("fact", f)
-    for tune in ("", "scan=direct"):
+    for tune in ("", "scan=direct", "keyed=5;bs=256;tile=512;stages=2;occ=2", "keyed=4;bs=256;stages=2;occ=2"):
         res, _ = ctx.run("template=q1", tune)
         assert_q1_equal(res, O.q1(f))
     res, _ = ctx.run("template=q6")
