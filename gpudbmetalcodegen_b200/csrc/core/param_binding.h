@@ -96,7 +96,7 @@ private:
 // Result schema: what a plan produces and how to decode it.
 // ===================================================================
 struct CudaResultSchema {
-    enum Kind { NONE, MATERIALIZE, SCALAR_AGG, KEYED_AGG, HASH_AGG, TOPK };
+    enum Kind { NONE, MATERIALIZE, SCALAR_AGG, KEYED_AGG, HASH_AGG, TOPK, DIRECT_AGG };
     Kind kind = NONE;
 
     // MATERIALIZE (reference: counter + output columns)
@@ -144,6 +144,7 @@ struct CudaResultSchema {
         std::vector<KeyedAggSlot> slots;
         std::vector<DerivedColumn> derived;
         std::vector<BucketKey> keys;
+        std::string bucketName = "bucket";  // the bucket column's name when no keys decode it
     };
     KeyedAggInfo keyedAgg;
 
@@ -171,8 +172,28 @@ struct CudaResultSchema {
         std::string keyName = "key";
         std::string valueName = "value";
         int k = 0;
+        // further columns of the k rows, gathered on the device into
+        // buffers of k elements (e.g. attributes of the top keys)
+        struct Extra {
+            std::string name, buffer, elementType;
+        };
+        std::vector<Extra> extra;
     };
     TopKInfo topk;
+
+    // DIRECT_AGG: direct-address arrays of equal length (AtomicAgg /
+    // AtomicCount outputs), one row (index, values...) per index where any
+    // value is non-zero, in index order (reference: the host read-back of
+    // direct-address aggregates, codegen_main.cpp:1105-1721).
+    struct DirectAggInfo {
+        std::string sizeExpr;
+        std::string keyName = "bucket";
+        struct Agg {
+            std::string name, buffer;
+        };
+        std::vector<Agg> aggs;
+    };
+    DirectAggInfo directAgg;
 };
 
 }  // namespace gpudb

@@ -166,6 +166,7 @@ GenericResult CudaResultCollector::collect(const CudaResultSchema& s, const Buff
         case CudaResultSchema::HASH_AGG: return collectHashAgg(s, read, size);
         case CudaResultSchema::TOPK: return collectTopK(s, read);
         case CudaResultSchema::MATERIALIZE: return collectMaterialize(s, read, size);
+        case CudaResultSchema::DIRECT_AGG: return collectDirectAgg(s, read, size);
         default: return {};
     }
 }
@@ -189,7 +190,7 @@ GenericResult CudaResultCollector::collectKeyedAgg(const CudaResultSchema& s, co
     std::vector<uint64_t> data((size_t)k.numBuckets * k.valuesPerBucket);
     if (!read(k.bufferName, data.data(), data.size() * 8))
         throw std::runtime_error("collector: missing buffer " + k.bufferName);
-    if (k.keys.empty()) r.columns.push_back({"bucket", "int"});
+    if (k.keys.empty()) r.columns.push_back({k.bucketName, "int"});
     for (const auto& bk : k.keys) r.columns.push_back({bk.name, "string"});
     for (const auto& sl : k.slots) r.columns.push_back({sl.name, "int"});
     for (const auto& d : k.derived) r.columns.push_back({d.name, "double"});
@@ -286,7 +287,49 @@ GenericResult CudaResultCollector::collectTopK(const CudaResultSchema& s, const 
     if (!read(t.keyBuffer, k.data(), 8 * (size_t)t.k) || !read(t.valueBuffer, v.data(), 8 * (size_t)t.k))
         throw std::runtime_error("collector: missing top-k output");
     r.columns = {{t.keyName, "int"}, {t.valueName, "int"}};
-    for (uint64_t i = 0; i < cnt && i < (uint64_t)t.k; i++) r.rows.push_back({(int128)k[i], (int128)v[i]});
+    std::vector<std::vector<int64_t>> extra;
+    for (const auto& e : t.extra) {
+        const size_t w = cudaTypeBytes(e.elementType);
+        std::vector<char> raw((size_t)t.k * w);
+        if (!read(e.buffer, raw.data(), raw.size())) throw std::runtime_error("collector: missing " + e.buffer);
+        std::vector<int64_t> col(t.k);
+        for (int i = 0; i < t.k; i++) {
+            const char* p = raw.data() + (size_t)i * w;
+            if (w == 8) col[i] = *(const int64_t*)p;
+            else if (w == 4) col[i] = *(const int32_t*)p;
+            else col[i] = *(const uint8_t*)p;
+        }
+        extra.push_back(std::move(col));
+        r.columns.push_back({e.name, "int"});
+    }
+    for (uint64_t i = 0; i < cnt && i < (uint64_t)t.k; i++) {
+        GenericResult::Row row{(int128)k[i], (int128)v[i]};
+        for (const auto& col : extra) row.push_back((int128)col[i]);
+        r.rows.push_back(std::move(row));
+    }
+    return r;
+}
+
+GenericResult CudaResultCollector::collectDirectAgg(const CudaResultSchema& s, const BufferReader& read,
+                                                    const SizeEval& size) {
+    GenericResult r;
+    const auto& d = s.directAgg;
+    const uint64_t n = size(d.sizeExpr);
+    std::vector<std::vector<int64_t>> cols;
+    r.columns.push_back({d.keyName, "int"});
+    for (const auto& a : d.aggs) {
+        cols.emplace_back(n);
+        if (n && !read(a.buffer, cols.back().data(), n * 8)) throw std::runtime_error("collector: missing " + a.buffer);
+        r.columns.push_back({a.name, "int"});
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        bool any = false;
+        for (const auto& c : cols) any |= (c[i] != 0);
+        if (!any) continue;  // empty bins are omitted, as for keyed aggregates
+        GenericResult::Row row{(int128)i};
+        for (const auto& c : cols) row.push_back((int128)c[i]);
+        r.rows.push_back(std::move(row));
+    }
     return r;
 }
 

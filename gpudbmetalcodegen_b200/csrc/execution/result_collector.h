@@ -67,6 +67,7 @@ private:
     static GenericResult collectHashAgg(const CudaResultSchema& s, const BufferReader& read, const SizeEval& size);
     static GenericResult collectTopK(const CudaResultSchema& s, const BufferReader& read);
     static GenericResult collectMaterialize(const CudaResultSchema& s, const BufferReader& read, const SizeEval& size);
+    static GenericResult collectDirectAgg(const CudaResultSchema& s, const BufferReader& read, const SizeEval& size);
 };
 
 }  // namespace gpudb

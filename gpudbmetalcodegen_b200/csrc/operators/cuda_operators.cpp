@@ -468,12 +468,105 @@ CudaSelection::CudaSelection(std::unique_ptr<CudaOperator> child, const std::str
     : CudaUnaryOperator(std::move(child)), predicate_(predicate) {}
 
 void CudaSelection::produce(CudaCodegen& cg, ConsumerFn consume) {
+    if (!bitmapOut_.empty()) {
+        // one bit per row of the scanned table, zero-filled before the run
+        cg.addBufferParam(bitmapOut_, "unsigned", "(" + bitmapRows_ + ") / 32 + 1", true, 0);
+        cg.addBufferLengthParam("len_" + bitmapOut_, bitmapOut_);
+    }
     cg.pushScanHint({CudaCodegen::ScanHint::Guard, predicate_, ""});
-    child_->produce(cg, [&]() { cg.addIf(predicate_, [&]() { consume(); }); });
+    child_->produce(cg, [&]() {
+        if (bitmapOut_.empty()) {
+            cg.addIf(predicate_, [&]() { consume(); });
+            return;
+        }
+        const std::string p = cg.fresh("_sp"), w = cg.fresh("_sw"), g = cg.fresh("_sg"), b = cg.fresh("_sb");
+        cg.addLine("const bool " + p + " = (" + predicate_ + ");");
+        cg.addBlock("", [&]() {
+            cg.addComment("selection bitmap: lanes sharing a 32-row word OR their bits, one atomic per word");
+            cg.addLine("const long long " + w + " = _row >> 5;");
+            cg.addLine("const unsigned " + g + " = __match_any_sync(__activemask(), (unsigned long long)" + w + ");");
+            cg.addLine("const unsigned " + b + " = __reduce_or_sync(" + g + ", " + p + " ? 1u << (unsigned)(_row & 31) : 0u);");
+            cg.addBlock("if (" + b + " != 0u && (int)(threadIdx.x & 31u) == __ffs(" + g + ") - 1)", [&]() {
+                cg.addLine("if ((unsigned long long)" + w + " < (unsigned long long)len_" + bitmapOut_ + ") atomicOr(" +
+                           bitmapOut_ + " + " + w + ", " + b + "); else gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+            });
+        });
+        cg.addIf(p, [&]() { consume(); });
+    });
     cg.popScanHint();
 }
 
-std::string CudaSelection::describe() const { return "Selection(" + predicate_ + ")"; }
+std::string CudaSelection::describe() const {
+    return "Selection(" + predicate_ + (bitmapOut_.empty() ? "" : " -> bitmap " + bitmapOut_) + ")";
+}
+
+// ===================================================================
+// CudaSelectionScan
+// ===================================================================
+CudaSelectionScan::CudaSelectionScan(const std::string& table, const std::string& bitmapName, const std::string& idxVar)
+    : table_(table), bitmap_(bitmapName), idxVar_(idxVar) {}
+
+void CudaSelectionScan::addColumn(const std::string& paramName, const std::string& cudaType) {
+    columns_.push_back({paramName, cudaType});
+}
+
+void CudaSelectionScan::produce(CudaCodegen& cg, ConsumerFn consume) {
+    for (const auto& c : columns_) cg.addColumnParam(c.first, c.second, table_, true);
+    cg.addTableSizeParam(table_);
+    cg.addReadBufferParam(bitmap_, "unsigned");
+    cg.addBufferLengthParam("len_" + bitmap_, bitmap_);
+    const std::string n = tableSizeName(table_);
+    const std::string& i = idxVar_;
+    cg.addComment("rows of " + table_ + " selected in " + bitmap_ + ": whole 32-row words per thread");
+    cg.addLine("const long long _ss_words = min((long long)len_" + bitmap_ + ", (" + n + " + 31) / 32);");
+    cg.addBlock("for (long long _ssw = tid; _ssw < _ss_words; _ssw += tpg)", [&]() {
+        cg.addLine("unsigned _ssb = __ldcs(" + bitmap_ + " + _ssw);");
+        cg.addBlock("while (_ssb)", [&]() {
+            cg.addLine("const long long " + i + " = _ssw * 32 + (__ffs(_ssb) - 1);");
+            cg.addLine("_ssb &= _ssb - 1u;");
+            cg.addLine("if (" + i + " >= " + n + ") break;");
+            cg.addLine("const long long _row = " + i + "; (void)_row;");
+            consume();
+        });
+    });
+}
+
+std::string CudaSelectionScan::describe() const { return "SelectionScan(" + table_ + " where " + bitmap_ + ")"; }
+
+// ===================================================================
+// CudaIndexGather
+// ===================================================================
+CudaIndexGather::CudaIndexGather(const std::string& indexBuffer, const std::string& countBuffer, int k)
+    : index_(indexBuffer), count_(countBuffer), k_(k) {}
+
+void CudaIndexGather::addColumn(const std::string& sourceArray, const std::string& type, const std::string& outBuffer,
+                                const std::string& displayName) {
+    cols_.push_back({sourceArray, type, outBuffer, displayName});
+}
+
+void CudaIndexGather::produce(CudaCodegen& cg, ConsumerFn consume) {
+    (void)consume;
+    cg.addReadBufferParam(index_, "long long");
+    cg.addReadBufferParam(count_, "unsigned long long");
+    for (const auto& c : cols_) {
+        cg.addReadBufferParam(c.src, c.type);
+        cg.addBufferLengthParam("len_" + c.src, c.src);
+        cg.addBufferParam(c.out, c.type, S(k_), true, 0);
+    }
+    cg.addLine("const long long _ig_n = min((long long)__ldcg(" + count_ + "), " + S(k_) + "ll);");
+    cg.addBlock("for (long long _j = tid; _j < _ig_n; _j += tpg)", [&]() {
+        cg.addLine("const long long _ix = __ldcg(" + index_ + " + _j);");
+        for (const auto& c : cols_)
+            cg.addLine("if ((unsigned long long)_ix < (unsigned long long)len_" + c.src + ") " + c.out + "[_j] = " + c.src +
+                       "[_ix]; else gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS);");
+    });
+    auto& rs = cg.resultSchema();
+    for (const auto& c : cols_) rs.topk.extra.push_back({c.name, c.out, c.type});
+}
+
+std::string CudaIndexGather::describe() const {
+    return "IndexGather(" + S((long long)cols_.size()) + " columns at " + index_ + "[0.." + count_ + "))";
+}
 
 CudaComputeExpr::CudaComputeExpr(std::unique_ptr<CudaOperator> child, const std::string& varName,
                                  const std::string& varType, const std::string& expression)

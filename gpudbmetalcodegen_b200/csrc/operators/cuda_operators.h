@@ -139,14 +139,67 @@ private:
 };
 
 // Selection: if (predicate) consume(). Reference: metal_operators.cpp:63-69.
+// With setBitmapOut, the predicate is also written out as a selection
+// bitmap of the scanned table (bit r = row r passed), built per warp: the
+// lanes that share a 32-row word (__match_any_sync on row >> 5) OR their
+// bits together (__reduce_or_sync, i.e. a warp ballot when the lanes hold
+// consecutive rows) and one lane sets the word with one atomicOr. A later
+// phase reads it back with CudaSelectionScan.
 class CudaSelection : public CudaUnaryOperator {
 public:
     CudaSelection(std::unique_ptr<CudaOperator> child, const std::string& predicate);
+    void setBitmapOut(const std::string& bitmapName, const std::string& rowsExpr) {
+        bitmapOut_ = bitmapName;
+        bitmapRows_ = rowsExpr;
+    }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
 private:
     std::string predicate_;
+    std::string bitmapOut_, bitmapRows_;
+};
+
+// Leaf: visits the rows of `table` whose bit is set in a selection bitmap
+// written by an earlier phase (CudaSelection::setBitmapOut). Each thread
+// takes whole 32-row words (grid-stride); zero words cost one load and no
+// row. The columns registered with addColumn are read at the selected rows
+// through their global pointers (a gather), so columns needed only by
+// selected rows are never streamed.
+class CudaSelectionScan : public CudaOperator {
+public:
+    CudaSelectionScan(const std::string& table, const std::string& bitmapName, const std::string& idxVar = "i");
+    void addColumn(const std::string& paramName, const std::string& cudaType);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string table_, bitmap_, idxVar_;
+    std::vector<std::pair<std::string, std::string>> columns_;
+};
+
+// A small phase after a top-k: for each of the (at most k) entries of the
+// index buffer `indexBuffer` (long long, count in `countBuffer`), gathers
+// source[index] of each registered direct-address array into an output
+// buffer of k elements — e.g. the build-side attributes of the top keys,
+// which the reference's host post-processing reads from its order maps
+// (codegen_main.cpp:1211-1248). Indices outside a source raise
+// GPUDB_ERR_BOUNDS.
+class CudaIndexGather : public CudaOperator {
+public:
+    CudaIndexGather(const std::string& indexBuffer, const std::string& countBuffer, int k);
+    void addColumn(const std::string& sourceArray, const std::string& type, const std::string& outBuffer,
+                   const std::string& displayName);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string index_, count_;
+    int k_;
+    struct Col {
+        std::string src, type, out, name;
+    };
+    std::vector<Col> cols_;
 };
 
 // ComputeExpr: T var = expr; consume(). Reference: metal_operators.cpp:86-91.

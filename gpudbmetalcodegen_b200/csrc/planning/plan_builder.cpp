@@ -397,6 +397,159 @@ CudaQueryPlan buildJoinRows(Spec& s, const TuneConfig& tune) {
     return plan;
 }
 
+// ---- join_direct: the reference's Q3 operator chain on the join tables
+// (metal_plan_builder.cpp:1170-1239): the qualifying build rows fill two
+// direct-address maps indexed by key (ArrayStore x2, sentinel -1), the
+// probe looks its key up in the first (ArrayLookup) and adds its revenue
+// into a dense per-key array (AtomicAgg); the reference's host post-step
+// (top 10 of the dense array with the maps' attributes, codegen_main.cpp:
+// 1211-1248) runs on the GPU: a top-k over the non-zero entries, then a
+// gather of the top keys' map values.
+CudaQueryPlan buildJoinDirect(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "JOIN_DIRECT";
+    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
+    const long long k = s.num("k", 10);
+    const std::string keys = "max_b_key + 1";
+    {
+        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
+                                                                      " && b_order_day[i] < " + std::to_string(odLt));
+        auto day = std::make_unique<CudaArrayStore>(std::move(f), "jd_day", "b_key[i]", "b_order_day[i]", "int", keys);
+        auto sg = std::make_unique<CudaArrayStore>(std::move(day), "jd_seg", "b_key[i]", "(int)b_segment[i]", "int", keys);
+        appendPhase(plan, "JD_build", std::move(sg), tune);
+    }
+    {
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune, true, {"p_price", "p_discount"});
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto lk = std::make_unique<CudaArrayLookup>(std::move(f), "jd_day", "p_fk[i]", "_oday", "int", -1);
+        auto ag = std::make_unique<CudaAtomicAgg>(std::move(lk), "jd_rev", "p_fk[i]",
+                                                  "p_price[i] * (100ll - p_discount[i])", keys);
+        appendPhase(plan, "JD_probe", std::move(ag), tune);
+    }
+    {
+        auto sc = std::make_unique<CudaBufferScan>("n_jd", keys, "i");
+        auto nz = std::make_unique<CudaSelection>(std::move(sc), "jd_rev[i] != 0ull");
+        auto tk = std::make_unique<CudaTopK>(std::move(nz), "jd_top", "i", "(long long)jd_rev[i]", (int)k);
+        auto& ph = appendPhase(plan, "JD_topk", std::move(tk), tune);
+        ph.minBlocksPerSM = 1;  // the register-resident top-k lists must not be capped by an occupancy hint
+        ph.extraBuffers.push_back({"jd_rev", "unsigned long long", true, false});
+    }
+    {
+        auto g = std::make_unique<CudaIndexGather>("jd_top_keys", "jd_top_count", (int)k);
+        g->addColumn("jd_day", "int", "jd_top_day", "order_day");
+        g->addColumn("jd_seg", "int", "jd_top_seg", "segment");
+        auto& ph = appendPhase(plan, "JD_attrs", std::move(g), tune);
+        ph.threadgroupSize = 32;
+        ph.minBlocksPerSM = 1;
+    }
+    plan.decorate.push_back([](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::TOPK;
+        rs.topk.keyName = "key";
+        rs.topk.valueName = "revenue";
+    });
+    plan.cpuSort = CudaQueryPlan::CpuSort{{{"revenue", true}, {"key", false}}, (int)k};
+    return plan;
+}
+
+// ---- anti_join: the reference's Q22 operator chain (metal_plan_builder.cpp:
+// 1304-1357) on the join tables: a bitmap of the qualifying build keys, then
+// the probe rows whose key is NOT in it (AntiBitmapProbe), binned by a
+// computed expression (ComputeExpr: the discount) and aggregated per bin by
+// AtomicCount (rows) and AtomicAgg (sum of price).
+CudaQueryPlan buildAntiJoin(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "ANTI_JOIN";
+    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
+    const std::string bins = "11";  // discount 0..10 (hundredths)
+    {
+        auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
+                                                                      " && b_order_day[i] < " + std::to_string(odLt));
+        auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "aj_bitmap", "b_key[i]", "max_b_key / 32 + 1");
+        appendPhase(plan, "AJ_build", std::move(bm), tune);
+    }
+    {
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day", "p_discount"}, tune, true, {"p_price"});
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto anti = std::make_unique<CudaAntiBitmapProbe>(std::move(f), "aj_bitmap", "p_fk[i]");
+        auto bin = std::make_unique<CudaComputeExpr>(std::move(anti), "_bin", "int", "(int)p_discount[i]");
+        auto cnt = std::make_unique<CudaAtomicCount>(std::move(bin), "aj_count", "_bin", bins);
+        auto sum = std::make_unique<CudaAtomicAgg>(std::move(cnt), "aj_sum", "_bin", "p_price[i]", bins);
+        sum->setWarpAggregate(true);
+        sum->setSharedCache(4, 4);
+        appendPhase(plan, "AJ_probe", std::move(sum), tune);
+    }
+    plan.decorate.push_back([bins](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::DIRECT_AGG;
+        rs.directAgg.sizeExpr = bins;
+        rs.directAgg.keyName = "discount";
+        rs.directAgg.aggs = {{"count", "aj_count"}, {"sum_price", "aj_sum"}};
+    });
+    return plan;
+}
+
+// ---- histogram: the reference's Q13 operator chain (metal_plan_builder.cpp:
+// 1244-1299): AtomicCount of the filtered probe rows per build key, then
+// for every build row an ArrayLookup of its key's count and an AtomicCount
+// histogram over those counts (bin = rows per key, value = keys).
+CudaQueryPlan buildHistogram(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "HISTOGRAM";
+    const long long shipGt = s.num("ship_gt", 1170);
+    const long long bins = s.num("bins", 256);
+    if (bins < 1 || bins > 8192) throw std::runtime_error("histogram: bins must be in [1, 8192]");
+    {
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto cnt = std::make_unique<CudaAtomicCount>(std::move(f), "h_count", "p_fk[i]", "max_b_key + 1");
+        appendPhase(plan, "H_count", std::move(cnt), tune);
+    }
+    {
+        auto scan = makeScan(plan, "dim", {"b_key"}, tune);
+        auto lk = std::make_unique<CudaArrayLookup>(std::move(scan), "h_count", "b_key[i]", "_cnt", "long long", -1);
+        auto hist = std::make_unique<CudaAtomicCount>(std::move(lk), "h_hist", "_cnt", std::to_string(bins));
+        appendPhase(plan, "H_hist", std::move(hist), tune);
+    }
+    plan.decorate.push_back([bins](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::DIRECT_AGG;
+        rs.directAgg.sizeExpr = std::to_string(bins);
+        rs.directAgg.keyName = "rows_per_key";
+        rs.directAgg.aggs = {{"keys", "h_hist"}};
+    });
+    return plan;
+}
+
+// ---- q6_selvec: the predicate variant in two phases over a selection
+// bitmap: the first evaluates the predicate on its three columns and
+// writes one bit per row (warp-ORed words); the second visits only the set
+// bits and gathers price and discount of those rows for the sum.
+CudaQueryPlan buildQ6SelVec(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "Q6_SELVEC";
+    const long long ge = s.num("ship_ge", 365), lt = s.num("ship_lt", 730);
+    const long long dlo = s.num("disc_lo", 5), dhi = s.num("disc_hi", 7), qlt = s.num("qty_lt", 24);
+    {
+        auto scan = makeScan(plan, "fact", {"f_ship_day", "f_quantity", "f_discount"}, tune);
+        const std::string pred = "(f_ship_day[i] >= " + std::to_string(ge) + " && f_ship_day[i] < " + std::to_string(lt) +
+                                 ") && (f_discount[i] >= " + L(dlo) + " && f_discount[i] <= " + L(dhi) +
+                                 ") && (f_quantity[i] < " + L(qlt) + ")";
+        auto sel = std::make_unique<CudaSelection>(std::move(scan), pred);
+        sel->setBitmapOut("q6_sel", "n_fact");
+        appendPhase(plan, "Q6S_select", std::move(sel), tune);
+    }
+    {
+        auto ss = std::make_unique<CudaSelectionScan>("fact", "q6_sel");
+        ss->addColumn("f_price", "long long");
+        ss->addColumn("f_discount", "long long");
+        auto reduce = std::make_unique<CudaTGReduce>(std::move(ss), "d_q6s");
+        reduce->addAccumulator("revenue", "f_price[i] * f_discount[i]", "wide");
+        reduce->setResultAlias("revenue", 0);
+        appendPhase(plan, "Q6S_sum", std::move(reduce), tune);
+    }
+    return plan;
+}
+
 // ---- groupby: high-cardinality hash group-by, count + sum (reference
 // Q18 shape metal_plan_builder.cpp:1529-1545, which aggregates into a
 // direct-address array; here an open-addressing table keyed by int64).
@@ -569,8 +722,8 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
 }  // namespace
 
 std::vector<std::string> planTemplates() {
-    return {"q1", "q6", "join_topk", "join_rows", "groupby", "hashjoin", "colmax", "distinct",
-            "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
+    return {"q1", "q6", "q6_selvec", "join_topk", "join_rows", "join_direct", "anti_join", "histogram", "groupby",
+            "hashjoin", "colmax", "distinct", "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
 }
 
 CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) {
@@ -581,6 +734,10 @@ CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) 
     else if (tmpl == "q6" || tmpl == "scan_filter_sum") plan = buildQ6(s, tune);
     else if (tmpl == "join_topk") plan = buildJoinTopK(s, tune);
     else if (tmpl == "join_rows") plan = buildJoinRows(s, tune);
+    else if (tmpl == "join_direct") plan = buildJoinDirect(s, tune);
+    else if (tmpl == "anti_join") plan = buildAntiJoin(s, tune);
+    else if (tmpl == "histogram") plan = buildHistogram(s, tune);
+    else if (tmpl == "q6_selvec") plan = buildQ6SelVec(s, tune);
     else if (tmpl == "groupby") plan = buildGroupBy(s, tune);
     else if (tmpl == "hashjoin") plan = buildHashJoin(s, tune);
     else if (tmpl == "colmax") plan = buildColMax(s, tune);

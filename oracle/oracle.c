@@ -394,3 +394,114 @@ int64_t oracle_max_i32(uint64_t n, const int32_t* v, int threads) {
         if (v[i] > m) m = v[i];
     return m;
 }
+
+/* ---- anti_join: Q22 operator chain, metal_plan_builder.cpp:1304-1357 —
+ * BitmapBuild over the qualifying build keys, AntiBitmapProbe
+ * (metal_operators.cpp:157-165) of the probe rows passing ship_day >
+ * ship_gt, bin = discount (ComputeExpr, :86-91), AtomicCount (:550-594)
+ * and AtomicAgg of price (:525-533) per bin. A key outside the bitmap is
+ * absent, so such a probe row passes the anti-probe. Returns 0, or -1 if a
+ * bin falls outside [0, nbins) (the engine's bounds error). */
+int oracle_anti_join(uint64_t nb, const int32_t* b_key, const int32_t* b_order_day, const uint8_t* b_segment,
+                     uint64_t np, const int32_t* p_fk, const int32_t* p_ship_day, const int64_t* p_price,
+                     const int64_t* p_discount, int32_t seg, int32_t od_lt, int32_t ship_gt, int nbins,
+                     int64_t* out_counts, oracle_i128* out_sums, int threads) {
+    const int T = nthreads(threads);
+    int64_t maxk = 0;
+    for (uint64_t i = 0; i < nb; i++)
+        if (b_key[i] > maxk) maxk = b_key[i];
+    const uint64_t words = (uint64_t)maxk / 32 + 1;
+    uint32_t* bm = calloc(words, 4);
+    if (!bm || nbins < 1 || nbins > 4096) {
+        free(bm);
+        return -1;
+    }
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int64_t i = 0; i < (int64_t)nb; i++) {
+        if (b_segment[i] == seg && b_order_day[i] < od_lt && b_key[i] >= 0)
+            __atomic_fetch_or(&bm[b_key[i] >> 5], 1u << (b_key[i] & 31), __ATOMIC_RELAXED);
+    }
+    int64_t cnt[4096];
+    i128 sum[4096];
+    memset(cnt, 0, sizeof(int64_t) * (size_t)nbins);
+    memset(sum, 0, sizeof(i128) * (size_t)nbins);
+    int bad = 0;
+#pragma omp parallel num_threads(T)
+    {
+        int64_t lc[4096];
+        i128 ls[4096];
+        memset(lc, 0, sizeof(int64_t) * (size_t)nbins);
+        memset(ls, 0, sizeof(i128) * (size_t)nbins);
+        int lbad = 0;
+#pragma omp for schedule(static)
+        for (int64_t i = 0; i < (int64_t)np; i++) {
+            if (p_ship_day[i] <= ship_gt) continue;
+            const int64_t k = p_fk[i];
+            const int in = k >= 0 && (uint64_t)(k >> 5) < words && ((bm[k >> 5] >> (k & 31)) & 1u);
+            if (in) continue;
+            const int64_t b = p_discount[i];
+            if (b < 0 || b >= nbins) {
+                lbad = 1;
+                continue;
+            }
+            lc[b] += 1;
+            ls[b] += p_price[i];
+        }
+#pragma omp critical
+        {
+            for (int b = 0; b < nbins; b++) {
+                cnt[b] += lc[b];
+                sum[b] += ls[b];
+            }
+            bad |= lbad;
+        }
+    }
+    free(bm);
+    for (int b = 0; b < nbins; b++) {
+        out_counts[b] = cnt[b];
+        out_sums[b] = to_pair(sum[b]);
+    }
+    return bad ? -1 : 0;
+}
+
+/* ---- histogram: Q13 operator chain, metal_plan_builder.cpp:1244-1299 —
+ * AtomicCount of the probe rows passing ship_day > ship_gt per key (an
+ * array indexed by key, sized by the largest build key), then for every
+ * build row an ArrayLookup of its key's count (metal_operators.cpp:213-225)
+ * and an AtomicCount histogram over the counts. out_hist[c] = build rows
+ * whose key has c such probe rows. Returns 0, or -1 if a probe key lies
+ * beyond the largest build key or a count reaches nbins (the engine's
+ * bounds errors). */
+int oracle_histogram(uint64_t nb, const int32_t* b_key, uint64_t np, const int32_t* p_fk, const int32_t* p_ship_day,
+                     int32_t ship_gt, int nbins, int64_t* out_hist, int threads) {
+    const int T = nthreads(threads);
+    int64_t maxk = 0;
+    for (uint64_t i = 0; i < nb; i++)
+        if (b_key[i] > maxk) maxk = b_key[i];
+    uint32_t* cnt = calloc((size_t)maxk + 1, 4);
+    if (!cnt) return -1;
+    int bad = 0;
+#pragma omp parallel for num_threads(T) schedule(static) reduction(| : bad)
+    for (int64_t i = 0; i < (int64_t)np; i++) {
+        if (p_ship_day[i] <= ship_gt) continue;
+        const int64_t k = p_fk[i];
+        if (k < 0 || k > maxk) {
+            bad = 1;
+            continue;
+        }
+        __atomic_fetch_add(&cnt[k], 1u, __ATOMIC_RELAXED);
+    }
+    memset(out_hist, 0, sizeof(int64_t) * (size_t)nbins);
+    for (uint64_t i = 0; i < nb; i++) {
+        const int64_t k = b_key[i];
+        if (k < 0 || k > maxk) continue;
+        const uint32_t c = cnt[k];
+        if (c >= (uint32_t)nbins) {
+            bad = 1;
+            continue;
+        }
+        out_hist[c] += 1;
+    }
+    free(cnt);
+    return bad ? -1 : 0;
+}

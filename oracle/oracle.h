@@ -86,6 +86,21 @@ int oracle_topk(uint64_t n, const int64_t* keys, const int64_t* vals, int k, int
 /* Exact max of an int32 / int64 column (max_key_symbols.cpp:188-235). */
 int64_t oracle_max_i32(uint64_t n, const int32_t* v, int threads);
 
+/* Anti-join (Q22 operator chain): probe rows with ship_day > ship_gt whose
+ * key is not a qualifying build key (segment == seg, order_day < od_lt),
+ * per discount bin: row count and exact sum of price. 0, or -1 on a bin
+ * outside [0, nbins). */
+int oracle_anti_join(uint64_t nb, const int32_t* b_key, const int32_t* b_order_day, const uint8_t* b_segment,
+                     uint64_t np, const int32_t* p_fk, const int32_t* p_ship_day, const int64_t* p_price,
+                     const int64_t* p_discount, int32_t seg, int32_t od_lt, int32_t ship_gt, int nbins,
+                     int64_t* out_counts, oracle_i128* out_sums, int threads);
+
+/* Histogram (Q13 operator chain): probe rows with ship_day > ship_gt counted
+ * per key, then out_hist[c] = build rows whose key has c of them. 0, or -1
+ * on a probe key beyond the largest build key or a count >= nbins. */
+int oracle_histogram(uint64_t nb, const int32_t* b_key, uint64_t np, const int32_t* p_fk, const int32_t* p_ship_day,
+                     int32_t ship_gt, int nbins, int64_t* out_hist, int threads);
+
 #ifdef __cplusplus
 }
 #endif

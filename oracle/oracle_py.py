@@ -45,6 +45,9 @@ def lib() -> C.CDLL:
                                           C.c_int]),
             "oracle_topk": (C.c_int, [C.c_uint64, P, P, C.c_int, P, P]),
             "oracle_max_i32": (C.c_int64, [C.c_uint64, P, C.c_int]),
+            "oracle_anti_join": (C.c_int, [C.c_uint64, P, P, P, C.c_uint64, P, P, P, P, C.c_int32, C.c_int32,
+                                           C.c_int32, C.c_int, P, P, C.c_int]),
+            "oracle_histogram": (C.c_int, [C.c_uint64, P, C.c_uint64, P, P, C.c_int32, C.c_int, P, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -177,3 +180,40 @@ def topk(keys: np.ndarray, vals: np.ndarray, k: int) -> List[tuple]:
 
 def max_i32(v: np.ndarray, threads: int = 0) -> int:
     return int(lib().oracle_max_i32(v.shape[0], _p(v), threads))
+
+
+def join_direct(dim, probe, seg=1, od_lt=1170, ship_gt=1170, k=10, threads: int = 0) -> List[tuple]:
+    """The Q3 operator chain's answer (metal_plan_builder.cpp:1170-1239 with
+    the host top-k of codegen_main.cpp:1211-1248, ties by key): the join's
+    top k (key, revenue) with the matched build row's order_day and
+    segment, read from the build table as the reference reads its maps."""
+    top, _, _ = join_topk(dim, probe, seg, od_lt, ship_gt, k, threads)
+    if not top:
+        return []
+    keys = dim["b_key"]
+    order = np.argsort(keys, kind="stable")
+    pos = order[np.searchsorted(keys[order], [t[0] for t in top])]
+    return [(key, rev, int(dim["b_order_day"][p]), int(dim["b_segment"][p])) for (key, rev), p in zip(top, pos)]
+
+
+def anti_join(dim, probe, seg=1, od_lt=1170, ship_gt=1170, nbins=11, threads: int = 0) -> List[tuple]:
+    """Rows (discount, count, sum_price) of non-empty bins, in bin order."""
+    cnt = np.zeros(nbins, np.int64)
+    sums = (I128 * nbins)()
+    st = lib().oracle_anti_join(dim["b_key"].shape[0], _p(dim["b_key"]), _p(dim["b_order_day"]),
+                                _p(dim["b_segment"]), probe["p_fk"].shape[0], _p(probe["p_fk"]),
+                                _p(probe["p_ship_day"]), _p(probe["p_price"]), _p(probe["p_discount"]), seg, od_lt,
+                                ship_gt, nbins, _p(cnt), sums, threads)
+    if st != 0:
+        raise ValueError("anti_join: a bin lies outside [0, nbins)")
+    return [(b, int(cnt[b]), sums[b].value()) for b in range(nbins) if cnt[b] or sums[b].value()]
+
+
+def histogram(dim, probe, ship_gt=1170, nbins=256, threads: int = 0) -> List[tuple]:
+    """Rows (rows_per_key, keys) of non-empty bins, in bin order."""
+    hist = np.zeros(nbins, np.int64)
+    st = lib().oracle_histogram(dim["b_key"].shape[0], _p(dim["b_key"]), probe["p_fk"].shape[0], _p(probe["p_fk"]),
+                                _p(probe["p_ship_day"]), ship_gt, nbins, _p(hist), threads)
+    if st != 0:
+        raise ValueError("histogram: a probe key beyond the build keys, or a count beyond the bins")
+    return [(c, int(hist[c])) for c in range(nbins) if hist[c]]

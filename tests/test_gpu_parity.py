@@ -15,7 +15,7 @@ REL = 1e-12
 Q1_TUNES = ["", "scan=direct", "bs=256;tile=1024;stages=2", "bs=1024;tile=2048;stages=3", "bs=128;tile=512;stages=8",
             "keyed=1", "keyed=2", "keyed=3", "keyed=4;occ=2", "bs=256;occ=3", "vec=4", "vec=2;bs=256", "vec=8;tile=2048",
             "keyed=5;bs=256;tile=512;stages=2;occ=2", "keyed=5;scan=direct", "keyed=5;bs=128;tile=256;occ=3",
-            "keyed=5;vec=2;bs=256;tile=512;stages=2", "keyed=5;bs=1024;tile=1024;stages=2"]
+            "keyed=5;vec=2;bs=256;tile=512;stages=2", "keyed=5;vec=4;bs=256;tile=512;stages=2", "keyed=5;bs=512;tile=512;stages=2"]
 
 
 def assert_q1_equal(res, expect):

@@ -98,6 +98,66 @@ def test_join_rows_known_answer_agrees_with_join_topk():
     assert O.join_rows(dim, probe, od_lt=0) == []
 
 
+def _tiny_join():
+    dim = {"b_key": np.array([3, 1, 2, 5, 4], np.int32), "b_order_day": np.array([100, 100, 2000, 100, 100], np.int32),
+           "b_segment": np.array([1, 1, 1, 0, 1], np.uint8)}
+    probe = {"p_fk": np.array([3, 1, 1, 4, 2, 5, 3, 4, 9], np.int32),
+             "p_ship_day": np.array([2000, 2000, 2000, 2000, 2000, 2000, 10, 2000, 2000], np.int32),
+             "p_price": np.array([100, 50, 50, 100, 999, 998, 997, 0, 7], np.int64),
+             "p_discount": np.array([0, 0, 0, 0, 3, 3, 0, 10, 3], np.int64)}
+    return dim, probe
+
+
+def test_join_direct_known_answer_carries_the_build_attributes():
+    dim, probe = _tiny_join()
+    dim["b_order_day"] = np.array([100, 101, 2000, 100, 104], np.int32)
+    # the join's top k with the matched build row's order_day and segment
+    assert O.join_direct(dim, probe, k=10) == [(1, 10000, 101, 1), (3, 10000, 100, 1), (4, 10000, 104, 1)]
+    assert O.join_direct(dim, probe, od_lt=0) == []
+
+
+def test_anti_join_known_answer():
+    dim, probe = _tiny_join()
+    # qualifying keys 3, 1, 4; anti-probe keeps rows with keys 2, 5 and 9
+    # (9 lies beyond every build key, so it is absent from the bitmap);
+    # row 6 ships too early
+    assert O.anti_join(dim, probe) == [(3, 3, 999 + 998 + 7)]
+    # with no qualifying key every shipped row passes
+    assert O.anti_join(dim, probe, od_lt=0) == [(0, 4, 100 + 50 + 50 + 100), (3, 3, 999 + 998 + 7), (10, 1, 0)]
+    bad = dict(probe, p_discount=np.array([0, 0, 0, 0, 11, 3, 0, 10, 3], np.int64))
+    with pytest.raises(ValueError):
+        O.anti_join(dim, bad)
+
+
+def test_histogram_known_answer():
+    dim, probe = _tiny_join()
+    probe = {k: v[:8] for k, v in probe.items()}  # drop the key beyond the build keys
+    # shipped rows per key: 1 -> 2, 2 -> 1, 3 -> 1 (one row ships too early), 4 -> 2, 5 -> 1
+    assert O.histogram(dim, probe) == [(1, 3), (2, 2)]
+    assert O.histogram(dim, probe, ship_gt=5000) == [(0, 5)]
+    with pytest.raises(ValueError):
+        O.histogram(dim, probe, nbins=2)  # a count of 2 needs three bins
+    with pytest.raises(ValueError):
+        O.histogram(dim, _tiny_join()[1])  # key 9 has no slot
+
+
+def test_new_chains_agree_with_numpy_restatements():
+    """The C oracle of the anti-join and histogram chains against plain
+    numpy restatements on seeded tables."""
+    d = W.gen_dim(5000, seed=8)
+    p = W.gen_probe(40000, dim_rows=5000, seed=8)
+    keep = (d["b_segment"] == 1) & (d["b_order_day"] < 1170)
+    qual = np.zeros(5002, bool)
+    qual[d["b_key"][keep]] = True
+    ok = (p["p_ship_day"] > 1170) & ~qual[p["p_fk"]]
+    cnt = np.bincount(p["p_discount"][ok], minlength=11)
+    sm = np.bincount(p["p_discount"][ok], weights=p["p_price"][ok].astype(np.float64), minlength=11)
+    assert O.anti_join(d, p) == [(b, int(cnt[b]), int(sm[b])) for b in range(11) if cnt[b]]
+    per_key = np.bincount(p["p_fk"][p["p_ship_day"] > 1170], minlength=5001)
+    h = np.bincount(per_key[d["b_key"]], minlength=256)
+    assert O.histogram(d, p) == [(c, int(h[c])) for c in range(256) if h[c]]
+
+
 def test_groupby_and_hashjoin_known_answer():
     key = np.array([5, -3, 5, 9, -3, 5], np.int64)
     val = np.array([1, 2, 3, 4, 5, 6], np.int64)
