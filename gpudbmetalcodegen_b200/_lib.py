@@ -98,6 +98,32 @@ _SIGNATURES = [
     ("gpudb_host_free", None, [C.c_void_p]),
     ("gpudb_distinct_count_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_int64,
                                                C.c_void_p, C.c_void_p]),
+    # gpudb_engine.h: analyzed queries
+    ("gpudb_aq_create", C.c_int, [C.POINTER(C.c_void_p)]),
+    ("gpudb_aq_free", None, [C.c_void_p]),
+    ("gpudb_aq_col", C.c_void_p, [C.c_void_p, C.c_char_p, C.c_char_p]),
+    ("gpudb_aq_lit_int", C.c_void_p, [C.c_void_p, C.c_int64]),
+    ("gpudb_aq_lit_decimal", C.c_void_p, [C.c_void_p, C.c_double]),
+    ("gpudb_aq_lit_str", C.c_void_p, [C.c_void_p, C.c_char_p]),
+    ("gpudb_aq_binary", C.c_void_p, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_cmp", C.c_void_p, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_between", C.c_void_p, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_in_list", C.c_void_p, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p), C.c_int]),
+    ("gpudb_aq_and", C.c_void_p, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]),
+    ("gpudb_aq_or", C.c_void_p, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]),
+    ("gpudb_aq_not", C.c_void_p, [C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_add_table", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("gpudb_aq_add_join", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    ("gpudb_aq_add_filter", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_add_target", C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p]),
+    ("gpudb_aq_add_agg", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_char_p]),
+    ("gpudb_aq_add_group_by", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gpudb_aq_add_order_by", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_aq_set_limit", C.c_int, [C.c_void_p, C.c_int]),
+    ("gpudb_aq_lower_expr", C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_int)]),
+    ("gpudb_aq_lower_pred", C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("gpudb_query_prepare_analyzed", C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p, C.c_char_p,
+                                               C.POINTER(C.c_void_p)]),
     # gpudb_engine.h
     ("gpudb_query_prepare", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     ("gpudb_query_free", None, [C.c_void_p]),

@@ -41,7 +41,7 @@ HASH_SPACE = {
     "warp": ["1", "0"],
 }
 SPACES = {
-    "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4"]},
+    "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4", "5"], "vec": ["0", "2", "4"]},
     "q6": SCAN_SPACE,
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["1", "0"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
@@ -52,7 +52,11 @@ SPACES = {
 # shallower TMA ring frees the shared memory that a higher occupancy needs):
 # measured alongside the default before the descent starts from the best.
 SEEDS = {
-    "q1": [{"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
+    # thread-private shared-memory accumulators need a small ring next to
+    # their slots for two CTAs per SM: 512-row tiles, two stages
+    "q1": [{"keyed": "5", "bs": "256", "tile": "512", "stages": "2", "occ": "2", "vec": "2"},
+           {"keyed": "5", "bs": "256", "tile": "448", "stages": "2", "occ": "2", "vec": "2"},
+           {"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
     "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
     "join_topk": [{"split": "0", "stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
                   {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],

@@ -34,6 +34,7 @@ HOST_SOURCES = [
     "core/cuda_codegen.cpp",
     "operators/cuda_operators.cpp",
     "planning/plan_builder.cpp",
+    "planning/query_ir.cpp",
     "execution/cuda_api.cpp",
     "execution/runtime_compiler.cpp",
     "execution/result_collector.cpp",

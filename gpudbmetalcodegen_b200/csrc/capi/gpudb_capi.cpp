@@ -3,6 +3,7 @@
 // context error text; nothing C++ crosses the boundary.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -15,6 +16,7 @@
 #include "../io/colbin.h"
 #include "../sql/sql_frontend.h"
 #include "../planning/plan_builder.h"
+#include "../planning/query_ir.h"
 
 struct gpudb_ctx {
     std::unique_ptr<gpudb::QueryContext> qc;
@@ -28,6 +30,37 @@ struct gpudb_query {
 };
 struct gpudb_result {
     gpudb::GenericResult r;
+};
+// An analyzed query under construction: its nodes are owned here and handed
+// out as opaque pointers (checked against this pool before use).
+struct gpudb_expr {
+    gpudb::ir::ExprPtr e;
+};
+struct gpudb_pred {
+    gpudb::ir::PredPtr p;
+};
+struct gpudb_aq {
+    gpudb::ir::AnalyzedQuery q;
+    std::vector<std::unique_ptr<gpudb_expr>> exprs;
+    std::vector<std::unique_ptr<gpudb_pred>> preds;
+    bool owns(const gpudb_expr* e) const {
+        for (const auto& x : exprs)
+            if (x.get() == e) return true;
+        return false;
+    }
+    bool owns(const gpudb_pred* p) const {
+        for (const auto& x : preds)
+            if (x.get() == p) return true;
+        return false;
+    }
+    gpudb_expr* add(gpudb::ir::ExprPtr e) {
+        exprs.push_back(std::make_unique<gpudb_expr>(gpudb_expr{std::move(e)}));
+        return exprs.back().get();
+    }
+    gpudb_pred* add(gpudb::ir::PredPtr p) {
+        preds.push_back(std::make_unique<gpudb_pred>(gpudb_pred{std::move(p)}));
+        return preds.back().get();
+    }
 };
 
 namespace {
@@ -623,5 +656,165 @@ size_t gpudb_list_templates(char* buf, size_t cap) {
 }
 
 const char* gpudb_version(void) { return "gpudb-b200 0.1 (sm_100a, NVRTC)"; }
+
+}  // extern "C"
+
+// ===================================================================
+// analyzed queries
+// ===================================================================
+namespace {
+using namespace gpudb::ir;
+bool okExpr(const gpudb_aq* aq, const gpudb_expr* e) { return aq && e && aq->owns(e); }
+bool okPred(const gpudb_aq* aq, const gpudb_pred* p) { return aq && p && aq->owns(p); }
+}  // namespace
+
+extern "C" {
+
+int gpudb_aq_create(gpudb_aq** out) {
+    if (!out) return GPUDB_E_INVALID;
+    *out = new gpudb_aq();
+    return GPUDB_OK;
+}
+
+void gpudb_aq_free(gpudb_aq* aq) { delete aq; }
+
+gpudb_expr* gpudb_aq_col(gpudb_aq* aq, const char* table, const char* column) {
+    if (!aq || !column) return nullptr;
+    return aq->add(Expr::col(table ? table : "", column));
+}
+gpudb_expr* gpudb_aq_lit_int(gpudb_aq* aq, int64_t v) { return aq ? aq->add(Expr::lit((long long)v)) : nullptr; }
+gpudb_expr* gpudb_aq_lit_decimal(gpudb_aq* aq, double v) { return aq ? aq->add(Expr::litf(v)) : nullptr; }
+gpudb_expr* gpudb_aq_lit_str(gpudb_aq* aq, const char* v) { return aq && v ? aq->add(Expr::lits(v)) : nullptr; }
+gpudb_expr* gpudb_aq_binary(gpudb_aq* aq, int op, gpudb_expr* l, gpudb_expr* r) {
+    if (!okExpr(aq, l) || !okExpr(aq, r) || op < GPUDB_EXPR_ADD || op > GPUDB_EXPR_DIV) return nullptr;
+    return aq->add(Expr::binary((ExprOp)op, l->e, r->e));
+}
+gpudb_pred* gpudb_aq_cmp(gpudb_aq* aq, int op, gpudb_expr* l, gpudb_expr* r) {
+    if (!okExpr(aq, l) || !okExpr(aq, r) || op < GPUDB_CMP_EQ || op > GPUDB_CMP_GE) return nullptr;
+    return aq->add(Predicate::cmp((CmpOp)op, l->e, r->e));
+}
+gpudb_pred* gpudb_aq_between(gpudb_aq* aq, gpudb_expr* e, gpudb_expr* lo, gpudb_expr* hi) {
+    if (!okExpr(aq, e) || !okExpr(aq, lo) || !okExpr(aq, hi)) return nullptr;
+    return aq->add(Predicate::between(e->e, lo->e, hi->e));
+}
+gpudb_pred* gpudb_aq_in_list(gpudb_aq* aq, gpudb_expr* e, gpudb_expr* const* values, int n) {
+    if (!okExpr(aq, e) || n < 0 || (n && !values)) return nullptr;
+    std::vector<ExprPtr> v;
+    for (int i = 0; i < n; i++) {
+        if (!okExpr(aq, values[i])) return nullptr;
+        v.push_back(values[i]->e);
+    }
+    return aq->add(Predicate::inList(e->e, std::move(v)));
+}
+static gpudb_pred* logical(gpudb_aq* aq, gpudb_pred* const* ch, int n, bool isAnd) {
+    if (!aq || n < 0 || (n && !ch)) return nullptr;
+    std::vector<PredPtr> v;
+    for (int i = 0; i < n; i++) {
+        if (!okPred(aq, ch[i])) return nullptr;
+        v.push_back(ch[i]->p);
+    }
+    return aq->add(isAnd ? Predicate::logAnd(std::move(v)) : Predicate::logOr(std::move(v)));
+}
+gpudb_pred* gpudb_aq_and(gpudb_aq* aq, gpudb_pred* const* children, int n) { return logical(aq, children, n, true); }
+gpudb_pred* gpudb_aq_or(gpudb_aq* aq, gpudb_pred* const* children, int n) { return logical(aq, children, n, false); }
+gpudb_pred* gpudb_aq_not(gpudb_aq* aq, gpudb_pred* child) {
+    return okPred(aq, child) ? aq->add(Predicate::logNot(child->p)) : nullptr;
+}
+
+int gpudb_aq_add_table(gpudb_aq* aq, const char* table) {
+    if (!aq || !table) return GPUDB_E_INVALID;
+    aq->q.tables.push_back(table);
+    return GPUDB_OK;
+}
+int gpudb_aq_add_join(gpudb_aq* aq, const char* lt, const char* lc, const char* rt, const char* rc) {
+    if (!aq || !lt || !lc || !rt || !rc) return GPUDB_E_INVALID;
+    aq->q.joins.push_back({lt, rt, lc, rc});
+    return GPUDB_OK;
+}
+int gpudb_aq_add_filter(gpudb_aq* aq, gpudb_pred* p) {
+    if (!okPred(aq, p)) return GPUDB_E_INVALID;
+    aq->q.filters.push_back(p->p);
+    return GPUDB_OK;
+}
+int gpudb_aq_add_target(gpudb_aq* aq, gpudb_expr* e, const char* alias) {
+    if (!okExpr(aq, e)) return GPUDB_E_INVALID;
+    SelectTarget t;
+    t.expr = e->e;
+    t.alias = alias ? alias : "";
+    aq->q.targets.push_back(t);
+    return GPUDB_OK;
+}
+int gpudb_aq_add_agg(gpudb_aq* aq, int func, gpudb_expr* e, const char* alias) {
+    if (!aq || func < GPUDB_AGGF_SUM || func > GPUDB_AGGF_MAX || (e && !aq->owns(e))) return GPUDB_E_INVALID;
+    if (!e && func != GPUDB_AGGF_COUNT) return GPUDB_E_INVALID;
+    SelectTarget t;
+    t.isAgg = true;
+    t.alias = alias ? alias : "";
+    AggTarget a;
+    a.func = (AggFunc)func;
+    a.innerExpr = e ? e->e : nullptr;
+    a.alias = t.alias;
+    a.isStar = e == nullptr;
+    t.agg = a;
+    t.expr = a.innerExpr;
+    aq->q.targets.push_back(t);
+    return GPUDB_OK;
+}
+int gpudb_aq_add_group_by(gpudb_aq* aq, gpudb_expr* e) {
+    if (!okExpr(aq, e)) return GPUDB_E_INVALID;
+    aq->q.groupBy.push_back(e->e);
+    return GPUDB_OK;
+}
+int gpudb_aq_add_order_by(gpudb_aq* aq, gpudb_expr* e, int descending) {
+    if (!okExpr(aq, e)) return GPUDB_E_INVALID;
+    aq->q.orderBy.push_back({e->e, descending != 0});
+    return GPUDB_OK;
+}
+int gpudb_aq_set_limit(gpudb_aq* aq, int limit) {
+    if (!aq || limit < -1) return GPUDB_E_INVALID;
+    aq->q.limit = limit;
+    return GPUDB_OK;
+}
+
+int gpudb_aq_lower_expr(gpudb_expr* e, char* code, size_t cap, int* scale) {
+    if (!e) return GPUDB_E_INVALID;
+    try {
+        const Lowered l = exprToCuda(e->e, "i");
+        copyOut(l.code, code, cap);
+        if (scale) *scale = l.scale;
+        return GPUDB_OK;
+    } catch (const std::exception& ex) {
+        return fail(nullptr, GPUDB_E_PLAN, ex.what());
+    }
+}
+
+int gpudb_aq_lower_pred(gpudb_pred* p, char* code, size_t cap) {
+    if (!p) return GPUDB_E_INVALID;
+    try {
+        copyOut(predToCuda(p->p, "i"), code, cap);
+        return GPUDB_OK;
+    } catch (const std::exception& ex) {
+        return fail(nullptr, GPUDB_E_PLAN, ex.what());
+    }
+}
+
+int gpudb_query_prepare_analyzed(gpudb_ctx* ctx, const gpudb_aq* aq, const char* name, const char* tune,
+                                 gpudb_query** out) {
+    if (!aq || !out) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    *out = nullptr;
+    try {
+        if (ctx) cudaSetDevice(ctx->qc->ex.device());
+        auto t0 = std::chrono::steady_clock::now();
+        const gpudb::TuneConfig tc = gpudb::TuneConfig::parse(tune ? tune : "");
+        gpudb::CudaQueryPlan plan = gpudb::buildCudaPlan(aq->q, name ? name : "", tc);
+        const double planMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        *out = new gpudb_query{gpudb::prepareFromPlan(std::move(plan), tc, planMs, true, ctx != nullptr)};
+        return GPUDB_OK;
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        const bool compile = m.find("NVRTC") != std::string::npos || m.find("cuModule") != std::string::npos;
+        return fail(ctx, compile ? GPUDB_E_COMPILE : GPUDB_E_PLAN, m);
+    }
+}
 
 }  // extern "C"

@@ -48,12 +48,19 @@ std::string describePlan(const PreparedQuery& q) {
 
 std::shared_ptr<PreparedQuery> prepareQuery(const std::string& spec, const std::string& tuneStr, bool compile,
                                             bool load) {
-    auto q = std::make_shared<PreparedQuery>();
     auto t0 = std::chrono::steady_clock::now();
-    q->tune = TuneConfig::parse(tuneStr);
-    q->plan = buildCudaPlan(spec, q->tune);
-    q->planMs = msSince(t0);
-    t0 = std::chrono::steady_clock::now();
+    const TuneConfig tune = TuneConfig::parse(tuneStr);
+    CudaQueryPlan plan = buildCudaPlan(spec, tune);
+    return prepareFromPlan(std::move(plan), tune, msSince(t0), compile, load);
+}
+
+std::shared_ptr<PreparedQuery> prepareFromPlan(CudaQueryPlan plan, const TuneConfig& tune, double planMs, bool compile,
+                                               bool load) {
+    auto q = std::make_shared<PreparedQuery>();
+    q->tune = tune;
+    q->plan = std::move(plan);
+    q->planMs = planMs;
+    auto t0 = std::chrono::steady_clock::now();
     q->cg = generateFromPlan(q->plan);
     q->source = q->cg.print();
     for (const auto& ph : q->cg.getPhases()) q->kernelNames.push_back(ph.name);

@@ -44,6 +44,10 @@ struct QueryContext {
 // Plan + generate (+ compile, + load when `load`). Throws std::runtime_error.
 std::shared_ptr<PreparedQuery> prepareQuery(const std::string& spec, const std::string& tune, bool compile, bool load);
 
+// The same from a plan already built (e.g. from an analyzed query).
+std::shared_ptr<PreparedQuery> prepareFromPlan(CudaQueryPlan plan, const TuneConfig& tune, double planMs, bool compile,
+                                               bool load);
+
 // Load a prepared-but-unloaded query into the current context.
 void loadQuery(PreparedQuery& q);
 

@@ -898,39 +898,66 @@ void CudaKeyedAgg::produce(CudaCodegen& cg, ConsumerFn consume) {
         });
     } else if (st == Strategy::SharedPrivate) {
         const int bs = cg.currentThreadgroupSize();
-        const int nacc = nb * na;
         const std::string BS = S(bs);
+        // a count ("1") never exceeds a thread's rows: its slots are 32-bit
+        // (one shared-memory wavefront per warp access instead of two)
+        std::vector<bool> narrow(na, false);
+        int nWide = 0, nNarrow = 0;
+        std::vector<int> pos(na, 0);
+        for (int j = 0; j < na; j++) {
+            const std::string& v = aggregates_[j].valueExpr;
+            narrow[j] = (v == "1" || v == "1ll" || v == "1u");
+            pos[j] = narrow[j] ? nNarrow++ : nWide++;
+        }
+        const int accW = nb * nWide, accN = nb * nNarrow;
         // allocated before the scan below sizes its ring from what is left
-        const int poff = cg.allocDynamicSmem(nacc * bs * 8);
+        const int poff = cg.allocDynamicSmem(accW * bs * 8);
+        const int noff = accN ? cg.allocDynamicSmem(accN * bs * 4) : 0;
         cg.addComment("keyed aggregation: thread-private accumulators in shared memory (" + S(nb) + " buckets x " +
-                      S(na) + " aggregates per thread, slot (bucket * " + S(na) + " + aggregate) * " + BS +
-                      " + thread: a warp's lanes hit consecutive words)");
+                      S(na) + " aggregates per thread; slot (bucket * aggregates + aggregate) * " + BS +
+                      " + thread, so a warp's lanes hit consecutive words; counts in 32-bit slots)");
         cg.addLine("if (blockDim.x > " + BS + "u) { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); return; }");
         cg.addLine("unsigned long long* const _kp_all = reinterpret_cast<unsigned long long*>(gpudb_smem + " + S(poff) +
                    ");");
         cg.addLine("unsigned long long* const _kp = _kp_all + threadIdx.x;");
         cg.addLine("#pragma unroll");
-        cg.addLine("for (int _a = 0; _a < " + S(nacc) + "; ++_a) _kp[_a * " + BS + "] = 0ull;");
+        cg.addLine("for (int _a = 0; _a < " + S(accW) + "; ++_a) _kp[_a * " + BS + "] = 0ull;");
+        if (accN) {
+            cg.addLine("unsigned* const _kn_all = reinterpret_cast<unsigned*>(gpudb_smem + " + S(noff) + ");");
+            cg.addLine("unsigned* const _kn = _kn_all + threadIdx.x;");
+            cg.addLine("#pragma unroll");
+            cg.addLine("for (int _a = 0; _a < " + S(accN) + "; ++_a) _kn[_a * " + BS + "] = 0u;");
+        }
         child_->produce(cg, [&]() {
             emitValues();
             cg.addBlock("if ((unsigned)_bucket < " + S(nb) + "u)", [&]() {
-                cg.addLine("unsigned long long* const _kq = _kp + _bucket * " + S(na * bs) + ";");
-                for (int j = 0; j < na; j++)
-                    cg.addLine("_kq[" + S(j * bs) + "] += (unsigned long long)_kv" + S(j) + ";");
+                if (nWide) cg.addLine("unsigned long long* const _kq = _kp + _bucket * " + S(nWide * bs) + ";");
+                if (nNarrow) cg.addLine("unsigned* const _kr = _kn + _bucket * " + S(nNarrow * bs) + ";");
+                for (int j = 0; j < na; j++) {
+                    if (narrow[j]) cg.addLine("_kr[" + S(pos[j] * bs) + "] += 1u;");
+                    else cg.addLine("_kq[" + S(pos[j] * bs) + "] += (unsigned long long)_kv" + S(j) + ";");
+                }
             }, " else { gpudb_set_error(gpudb_err, GPUDB_ERR_BOUNDS); }");
             consume();
         });
         cg.addComment("each warp sums whole slots over the block's threads, then one RED per non-zero slot");
         cg.addLine("__syncthreads();");
-        cg.addBlock("for (int _a = (int)(threadIdx.x >> 5); _a < " + S(nacc) + "; _a += (int)(blockDim.x >> 5))", [&]() {
+        cg.addBlock("for (int _a = (int)(threadIdx.x >> 5); _a < " + S(nb * na) + "; _a += (int)(blockDim.x >> 5))", [&]() {
+            cg.addLine("const int _b = _a / " + S(na) + ", _j = _a % " + S(na) + ";");
             cg.addLine("unsigned long long _t = 0ull;");
-            cg.addLine("for (int _u = (int)(threadIdx.x & 31u); _u < (int)blockDim.x; _u += 32) _t += _kp_all[_a * " +
-                       BS + " + _u];");
+            cg.addBlock("switch (_j)", [&]() {
+                for (int j = 0; j < na; j++) {
+                    const std::string src = narrow[j] ? "(unsigned long long)_kn_all[(_b * " + S(nNarrow) + " + " + S(pos[j]) + ") * " + BS
+                                                      : "_kp_all[(_b * " + S(nWide) + " + " + S(pos[j]) + ") * " + BS;
+                    cg.addLine("case " + S(j) + ": for (int _u = (int)(threadIdx.x & 31u); _u < (int)blockDim.x; _u += 32) _t += " +
+                               src + " + _u]; break;");
+                }
+                cg.addLine("default: break;");
+            });
             cg.addLine("#pragma unroll");
             cg.addLine("for (int _o = 16; _o > 0; _o >>= 1) _t += __shfl_xor_sync(0xffffffffu, _t, _o);");
             cg.addLine("if ((threadIdx.x & 31u) != 0u || _t == 0ull) continue;");
             cg.addLine("const long long _tot = (long long)_t;");
-            cg.addLine("const int _b = _a / " + S(na) + ", _j = _a % " + S(na) + ";");
             cg.addBlock("switch (_j)", [&]() {
                 for (int j = 0; j < na; j++) {
                     const auto& ag = aggregates_[j];

@@ -1,5 +1,9 @@
 #include "plan_builder.h"
 
+#include "query_ir.h"
+
+#include <algorithm>
+#include <cctype>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -17,15 +21,15 @@ std::vector<TableDef> buildCatalog() {
         {"fact",
          {{"f_ship_day", "int"},
           {"f_quantity", "long long"},
-          {"f_price", "long long"},
-          {"f_discount", "long long"},
-          {"f_tax", "long long"},
-          {"f_flag_a", "unsigned char"},
-          {"f_flag_b", "unsigned char"}}},
+          {"f_price", "long long", 2},
+          {"f_discount", "long long", 2},
+          {"f_tax", "long long", 2},
+          {"f_flag_a", "unsigned char", 0, "ANR"},
+          {"f_flag_b", "unsigned char", 0, "FO"}}},
         // Build side (orders role): unique int keys.
         {"dim", {{"b_key", "int"}, {"b_order_day", "int"}, {"b_segment", "unsigned char"}}},
         // Probe side (lineitem role for the join).
-        {"probe", {{"p_fk", "int"}, {"p_ship_day", "int"}, {"p_price", "long long"}, {"p_discount", "long long"}}},
+        {"probe", {{"p_fk", "int"}, {"p_ship_day", "int"}, {"p_price", "long long", 2}, {"p_discount", "long long", 2}}},
         // Skewed-key probe / group-by input.
         {"zprobe", {{"z_key", "long long"}, {"z_value", "long long"}}},
         // Skewed-key build side: every distinct key once.
@@ -266,44 +270,61 @@ CudaQueryPlan buildQ6(Spec& s, const TuneConfig& tune) {
     return plan;
 }
 
-// ---- join_topk: bitmap semi-join build -> probe + hash group-by ->
-// top-k (reference Q3 shape: metal_plan_builder.cpp:1170-1239 + host top-k
-// codegen_main.cpp:1211-1248). The build's distinct counter is the exact
-// sizing pass for the group table; `groups=N` supplies it instead.
-CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
+// ---- semi-join + group-by (+ top-k): the join's parts as kernel source over the dim / probe columns: the
+// build-side and probe-side filters, the summed expression, the group
+// count when the caller supplies it (groups < 0: sized on the device, or
+// by the build's distinct count in the unsplit plan), and k (0 = every
+// group, no top-k).
+struct JoinAggParts {
+    std::string buildPred, probePred, revenue;
+    long long k = 10;
+    long long groups = -1;
+};
+
+CudaQueryPlan buildJoinAgg(const JoinAggParts& jp, const TuneConfig& tune) {
     CudaQueryPlan plan;
-    plan.name = "JOIN_TOPK";
-    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
-    const long long k = s.num("k", 10);
-    const bool given = s.has("groups");
-    const long long groups = s.num("groups", 0);
+    plan.name = jp.k > 0 ? "JOIN_TOPK" : "JOIN_GROUPS";
+    const long long k = jp.k;
+    const bool given = jp.groups >= 0;
+    const long long groups = jp.groups;
+    auto filtered = [](std::unique_ptr<CudaOperator> in, const std::string& pred) -> std::unique_ptr<CudaOperator> {
+        if (pred.empty()) return in;
+        return std::make_unique<CudaSelection>(std::move(in), pred);
+    };
+    const TuneConfig splitTune = [&] {
+        TuneConfig t = tune;
+        // every group: the host-sized plan, whose table is filled whole, so
+        // the collector can read every slot (the device-sized table only
+        // initialises the slots it uses)
+        if (k <= 0) t.splitJoin = false;
+        return t;
+    }();
     {
-        const TuneConfig bt = tune.forBuild();
+        const TuneConfig bt = splitTune.forBuild();
         auto scan = makeScan(plan, "dim", {"b_key", "b_order_day", "b_segment"}, bt);
-        auto f = std::make_unique<CudaSelection>(std::move(scan), "b_segment[i] == " + std::to_string(seg) +
-                                                                      " && b_order_day[i] < " + std::to_string(odLt));
+        auto f = filtered(std::move(scan), jp.buildPred);
         auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "jb_bitmap", "b_key[i]", "max_b_key / 32 + 1");
         // the split plan counts the bitmap's keys after the build (in its
         // probe), so the build sets bits without waiting on their old values
-        if (!tune.splitJoin) bm->setDistinctCounter("jb_distinct");
+        if (!splitTune.splitJoin) bm->setDistinctCounter("jb_distinct");
         appendPhase(plan, "JT_build", std::move(bm), bt);
     }
     const std::string cap = "2 * max(jt_groups, 1)";
-    if (tune.splitJoin) {
+    if (splitTune.splitJoin) {
         // The probe only lists the matched rows; a second phase gathers
         // their price / discount and aggregates. A matched row's slow work
         // (gathers, hash insert) then never holds a staged tile, and the
         // group table is sized by min(qualifying build keys, matched rows).
         {
-            auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune);
-            auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+            auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, splitTune);
+            auto f = filtered(std::move(scan), jp.probePred);
             auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
             pr->setPopcountInto("jb_distinct");
             auto mt = std::make_unique<CudaMaterialize>(std::move(pr), "jm_n", "n_probe");
             mt->addColumn("jm_rows", "unsigned", "(unsigned)_row");
             mt->addColumn("jm_fk", "int", "p_fk[i]");  // the group key rides along: no gather of it later
             mt->setIntermediate(true);
-            appendPhase(plan, "JT_probe", std::move(mt), tune);
+            appendPhase(plan, "JT_probe", std::move(mt), splitTune);
         }
         // No host round trip sizes the group table: it is allocated for
         // min(probe rows, build keys) groups and JT_init / JT_group derive
@@ -316,42 +337,42 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         appendPhase(plan, "JT_init",
                     std::make_unique<CudaHashInit>("jg", "int", HashLayout::Linear, std::vector<std::string>{"revenue"},
                                                    devGroups, bound, counters),
-                    tune);
+                    splitTune);
         {
             auto ls = std::make_unique<CudaSlotListScan>("jm_rows", "jm_n");
             ls->addListColumn("jm_fk", "int", "_jm_fk");
             ls->addGatherColumn("p_price", "long long", "probe");
             ls->addGatherColumn("p_discount", "long long", "probe");
             auto gb = std::make_unique<CudaHashGroupBy>(std::move(ls), "jg", "_jm_fk", "int", cap, HashLayout::Linear,
-                                                        tune.maxProbe);
-            gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
-            gb->setWarpAggregate(tune.warpAggregate);
+                                                        splitTune.maxProbe);
+            gb->addAggregate("revenue", jp.revenue);
+            gb->setWarpAggregate(splitTune.warpAggregate);
             gb->setSlotList(true);
             gb->setDeviceCapacity(devGroups, bound, counters);
-            appendPhase(plan, "JT_group", std::move(gb), tune);
+            appendPhase(plan, "JT_group", std::move(gb), splitTune);
         }
     } else {
-        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, tune, true, {"p_price", "p_discount"});
-        auto f = std::make_unique<CudaSelection>(std::move(scan), "p_ship_day[i] > " + std::to_string(shipGt));
+        auto scan = makeScan(plan, "probe", {"p_fk", "p_ship_day"}, splitTune, true, {"p_price", "p_discount"});
+        auto f = filtered(std::move(scan), jp.probePred);
         auto pr = std::make_unique<CudaBitmapProbe>(std::move(f), "jb_bitmap", "p_fk[i]");
         auto gb = std::make_unique<CudaHashGroupBy>(std::move(pr), "jg", "p_fk[i]", "int", cap, HashLayout::Linear,
-                                                    tune.maxProbe);
-        gb->addAggregate("revenue", "p_price[i] * (100ll - p_discount[i])");
-        gb->setWarpAggregate(tune.warpAggregate);
+                                                    splitTune.maxProbe);
+        gb->addAggregate("revenue", jp.revenue);
+        gb->setWarpAggregate(splitTune.warpAggregate);
         gb->setSlotList(true);
-        appendPhase(plan, "JT_probe_group", std::move(gb), tune);
+        appendPhase(plan, "JT_probe_group", std::move(gb), splitTune);
     }
-    {
+    if (k > 0) {
         // only the slots whose groups were created (the probe's slot list)
         auto lscan = std::make_unique<CudaSlotListScan>("jg_slotlist", "jg_nslots");
         auto tk = std::make_unique<CudaTopK>(std::move(lscan), "jt_top", "(long long)(int)jg_keys[i]",
                                              "(long long)jg_revenue[i]", (int)k);
-        auto& ph = appendPhase(plan, "JT_topk", std::move(tk), tune);
+        auto& ph = appendPhase(plan, "JT_topk", std::move(tk), splitTune);
         ph.minBlocksPerSM = 1;  // the register-resident top-k lists must not be capped by an occupancy hint
         ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});
         ph.extraBuffers.push_back({"jg_revenue", "unsigned long long", true, false});
     }
-    if (!tune.splitJoin) {
+    if (!splitTune.splitJoin) {
         CudaQueryPlan::SizingStep st;
         st.symbol = "jt_groups";
         st.afterPhase = 1;
@@ -359,12 +380,32 @@ CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
         else st.counterBuffer = "jb_distinct";
         plan.sizing.push_back(st);
     }
-    plan.decorate.push_back([](CudaResultSchema& rs) {
-        rs.topk.keyName = "key";
-        rs.topk.valueName = "revenue";
-    });
-    plan.cpuSort = CudaQueryPlan::CpuSort{{{"revenue", true}, {"key", false}}, (int)k};
+    if (k > 0) {
+        plan.decorate.push_back([](CudaResultSchema& rs) {
+            rs.topk.keyName = "key";
+            rs.topk.valueName = "revenue";
+        });
+        plan.cpuSort = CudaQueryPlan::CpuSort{{{"revenue", true}, {"key", false}}, (int)k};
+    } else {
+        plan.decorate.push_back([](CudaResultSchema& rs) { rs.hashAgg.keyName = "key"; });
+    }
     return plan;
+}
+
+// ---- join_topk: bitmap semi-join build -> probe + hash group-by ->
+// top-k (reference Q3 shape: metal_plan_builder.cpp:1170-1239 + host top-k
+// codegen_main.cpp:1211-1248). The build's distinct counter is the exact
+// sizing pass for the group table; `groups=N` supplies it instead.
+CudaQueryPlan buildJoinTopK(Spec& s, const TuneConfig& tune) {
+    const long long seg = s.num("seg", 1), odLt = s.num("od_lt", 1170), shipGt = s.num("ship_gt", 1170);
+    JoinAggParts jp;
+    jp.buildPred = "b_segment[i] == " + std::to_string(seg) + " && b_order_day[i] < " + std::to_string(odLt);
+    jp.probePred = "p_ship_day[i] > " + std::to_string(shipGt);
+    jp.revenue = "p_price[i] * (100ll - p_discount[i])";
+    jp.k = s.num("k", 10);
+    if (jp.k < 1) throw std::runtime_error("join_topk: k must be at least 1");
+    if (s.has("groups")) jp.groups = s.num("groups", 0);
+    return buildJoinAgg(jp, tune);
 }
 
 // ---- join_rows: the Q3 semi-join with its matching probe rows
@@ -747,6 +788,359 @@ CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) 
     else throw std::runtime_error("buildCudaPlan: unknown template '" + tmpl + "'");
     s.finish();
     plan.spec = canonicalSpec(s.m);
+    return plan;
+}
+
+// ===================================================================
+// Planning from an analyzed query
+// ===================================================================
+namespace {
+
+using namespace ir;
+
+struct TableSplit {
+    std::map<std::string, std::vector<PredPtr>> filters;  // engine table -> its filters
+};
+
+// The engine table a predicate's columns belong to ("" when it reads none).
+std::string predicateTable(const PredPtr& p) {
+    std::vector<ResolvedColumn> cols;
+    collectColumns(p, cols);
+    std::string t;
+    for (const auto& c : cols) {
+        if (!t.empty() && t != c.table)
+            throw std::runtime_error("analyzed plan: a filter reads two tables (" + t + ", " + c.table +
+                                     "); only equi-joins in the join clause connect tables");
+        t = c.table;
+    }
+    return t;
+}
+
+bool isAliasRef(const ExprPtr& e, const std::string& alias) {
+    if (!e || alias.empty()) return false;
+    if (auto* c = std::get_if<ColRef>(&e->node)) return c->table.empty() && c->column == alias;
+    return false;
+}
+
+std::optional<ResolvedColumn> plainColumn(const ExprPtr& e) {
+    if (!e) return std::nullopt;
+    if (auto* c = std::get_if<ColRef>(&e->node)) {
+        try {
+            return resolveColumn(c->table, c->column);
+        } catch (const std::exception&) {
+            return std::nullopt;
+        }
+    }
+    return std::nullopt;
+}
+
+std::string aggName(AggFunc f) {
+    switch (f) {
+        case AggFunc::SUM: return "SUM";
+        case AggFunc::COUNT: return "COUNT";
+        case AggFunc::AVG: return "AVG";
+        case AggFunc::MIN: return "MIN";
+        case AggFunc::MAX: return "MAX";
+        case AggFunc::COUNT_DISTINCT: return "COUNT(DISTINCT)";
+    }
+    return "?";
+}
+
+std::string aliasOf(const SelectTarget& t, size_t i) {
+    if (!t.alias.empty()) return t.alias;
+    if (t.agg && !t.agg->alias.empty()) return t.agg->alias;
+    return "agg" + std::to_string(i);
+}
+
+std::unique_ptr<CudaOperator> scanFor(CudaQueryPlan& plan, const std::string& table,
+                                      const std::vector<ResolvedColumn>& cols, const TuneConfig& tune) {
+    std::vector<std::string> names;
+    for (const auto& c : cols)
+        if (c.table == table && std::find(names.begin(), names.end(), c.column) == names.end()) names.push_back(c.column);
+    if (names.empty()) names.push_back(catalogTable(table).columns.front().name);  // COUNT(*) still scans
+    return makeScan(plan, table, names, tune);
+}
+
+std::unique_ptr<CudaOperator> selectIf(std::unique_ptr<CudaOperator> in, const std::string& pred) {
+    if (pred.empty()) return in;
+    return std::make_unique<CudaSelection>(std::move(in), pred);
+}
+
+// One table, aggregates, no GROUP BY (the Q6 shape).
+CudaQueryPlan planScalarAgg(const AnalyzedQuery& aq, const std::string& table, const std::string& name,
+                            const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = name.empty() ? "SCALAR_AGG" : name;
+    std::vector<ResolvedColumn> cols;
+    for (const auto& f : aq.filters) collectColumns(f, cols);
+    std::vector<std::tuple<std::string, std::string, std::string, int>> accs;  // alias, code, type, scale
+    for (size_t i = 0; i < aq.targets.size(); i++) {
+        const auto& t = aq.targets[i];
+        if (!t.isAgg || !t.agg) throw std::runtime_error("analyzed plan: a non-aggregate target without GROUP BY");
+        const auto& a = *t.agg;
+        if (a.func == AggFunc::SUM) {
+            collectColumns(a.innerExpr, cols);
+            const Lowered v = exprToCuda(a.innerExpr, "i");
+            accs.emplace_back(aliasOf(t, i), v.code, "wide", v.scale);
+        } else if (a.func == AggFunc::COUNT) {
+            accs.emplace_back(aliasOf(t, i), "1", "long", 0);
+        } else {
+            throw std::runtime_error("analyzed plan: " + aggName(a.func) + " in a scalar aggregate (SUM and COUNT "
+                                     "are computed exactly on the device)");
+        }
+    }
+    auto scan = scanFor(plan, table, cols, tune);
+    auto f = selectIf(std::move(scan), combineFilters(aq.filters, "i"));
+    auto r = std::make_unique<CudaTGReduce>(std::move(f), "d_ir");
+    for (const auto& [alias, code, type, scale] : accs) {
+        r->addAccumulator(alias, code, type);
+        r->setResultAlias(alias, scale);
+    }
+    appendPhase(plan, plan.name + "_reduce", std::move(r), tune);
+    plan.chunkable = true;
+    return plan;
+}
+
+// One table, GROUP BY columns with known value sets (the Q1 shape).
+CudaQueryPlan planKeyedAgg(const AnalyzedQuery& aq, const std::string& table, const std::vector<ResolvedColumn>& keys,
+                           const std::vector<std::string>& keyNames, const std::string& name, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = name.empty() ? "KEYED_AGG" : name;
+    int nb = 1;
+    std::vector<std::string> domains;
+    for (const auto& k : keys) {
+        domains.push_back(catalogTable(k.table).col(k.column).domain);
+        nb *= (int)domains.back().size();
+    }
+    if (nb > 64) throw std::runtime_error("analyzed plan: more than 64 groups for a keyed aggregate");
+    // bucket = mixed radix over the keys in GROUP BY order, each key's index
+    // in its value set (the reference's order: metal_plan_builder.cpp:335);
+    // a value outside the set lands beyond the buckets: a bounds error
+    std::string bucket;
+    int radix = nb;
+    for (size_t j = 0; j < keys.size(); j++) {
+        radix /= (int)domains[j].size();
+        std::string idx = std::to_string(nb);
+        for (int v = (int)domains[j].size() - 1; v >= 0; --v)
+            idx = "(" + keys[j].column + "[i] == '" + std::string(1, domains[j][v]) + "' ? " + std::to_string(v) +
+                  " : " + idx + ")";
+        bucket += (bucket.empty() ? "" : " + ") + std::string("(") + idx + ") * " + std::to_string(radix);
+    }
+    std::vector<ResolvedColumn> cols(keys.begin(), keys.end());
+    for (const auto& f : aq.filters) collectColumns(f, cols);
+    struct Slot {
+        std::string name, code;
+        bool wide;
+        int scale;
+    };
+    std::vector<Slot> slots;
+    std::vector<CudaResultSchema::DerivedColumn> derived;
+    int countIdx = -1;
+    auto needCount = [&]() {
+        if (countIdx < 0) {
+            countIdx = (int)slots.size();
+            slots.push_back({"_count", "1", false, 0});
+        }
+        return slots[countIdx].name;
+    };
+    std::vector<std::string> outCols;
+    for (size_t i = 0; i < aq.targets.size(); i++) {
+        const auto& t = aq.targets[i];
+        if (!t.isAgg || !t.agg) {
+            auto c = plainColumn(t.expr);
+            bool isKey = false;
+            for (const auto& k : keys) isKey |= c && c->column == k.column && c->table == k.table;
+            if (!isKey) throw std::runtime_error("analyzed plan: a non-aggregate target that is not a GROUP BY column");
+            continue;
+        }
+        const auto& a = *t.agg;
+        const std::string alias = aliasOf(t, i);
+        if (a.func == AggFunc::SUM || a.func == AggFunc::AVG) {
+            collectColumns(a.innerExpr, cols);
+            const Lowered v = exprToCuda(a.innerExpr, "i");
+            slots.push_back({a.func == AggFunc::SUM ? alias : "_sum_" + alias, v.code, true, v.scale});
+            if (a.func == AggFunc::AVG) derived.push_back({alias, slots.back().name, needCount()});
+        } else if (a.func == AggFunc::COUNT) {
+            if (countIdx >= 0 && slots[countIdx].name == "_count") slots[countIdx].name = alias;
+            else if (countIdx < 0) {
+                countIdx = (int)slots.size();
+                slots.push_back({alias, "1", false, 0});
+            } else {
+                slots.push_back({alias, "1", false, 0});
+            }
+        } else {
+            throw std::runtime_error("analyzed plan: " + aggName(a.func) + " in a keyed aggregate");
+        }
+    }
+    // derived columns named the count slot before a COUNT target may have renamed it
+    for (auto& d : derived)
+        if (d.denominator == "_count" && countIdx >= 0) d.denominator = slots[countIdx].name;
+    int vpb = 0;
+    std::vector<int> offs;
+    for (const auto& sl : slots) {
+        offs.push_back(vpb);
+        vpb += sl.wide ? 2 : 1;
+    }
+    auto scan = scanFor(plan, table, cols, tune);
+    auto f = selectIf(std::move(scan), combineFilters(aq.filters, "i"));
+    auto agg = std::make_unique<CudaKeyedAgg>(std::move(f), "d_ir_keyed", bucket, nb, vpb);
+    for (size_t j = 0; j < slots.size(); j++) agg->addAggregate(slots[j].name, offs[j], slots[j].code, "add", slots[j].wide, slots[j].scale);
+    if (tune.keyedStrategy) agg->setStrategy((CudaKeyedAgg::Strategy)tune.keyedStrategy);
+    appendPhase(plan, plan.name + "_reduce", std::move(agg), tune);
+    plan.chunkable = true;
+    plan.decorate.push_back([keyNames, domains, nb, derived](CudaResultSchema& rs) {
+        int radix = nb;
+        rs.keyedAgg.keys.clear();
+        for (size_t j = 0; j < keyNames.size(); j++) {
+            radix /= (int)domains[j].size();
+            std::vector<std::string> labels;
+            for (char ch : domains[j]) labels.push_back(std::string(1, ch));
+            rs.keyedAgg.keys.push_back({keyNames[j], radix, (int)domains[j].size(), labels});
+        }
+        rs.keyedAgg.derived = derived;
+    });
+    return plan;
+}
+
+// One table, GROUP BY one integer column (the Q18 shape).
+CudaQueryPlan planHashGroupBy(const AnalyzedQuery& aq, const std::string& table, const ResolvedColumn& key,
+                              const std::string& keyName, const std::string& name, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = name.empty() ? "HASH_GROUPBY" : name;
+    std::vector<ResolvedColumn> cols{key};
+    for (const auto& f : aq.filters) collectColumns(f, cols);
+    std::vector<std::pair<std::string, std::string>> aggs;
+    for (size_t i = 0; i < aq.targets.size(); i++) {
+        const auto& t = aq.targets[i];
+        if (!t.isAgg || !t.agg) {
+            auto c = plainColumn(t.expr);
+            if (!c || c->column != key.column) throw std::runtime_error("analyzed plan: a non-aggregate target that is not the GROUP BY column");
+            continue;
+        }
+        const auto& a = *t.agg;
+        if (a.func == AggFunc::SUM) {
+            collectColumns(a.innerExpr, cols);
+            aggs.emplace_back(aliasOf(t, i), exprToCuda(a.innerExpr, "i").code);
+        } else if (a.func == AggFunc::COUNT) {
+            aggs.emplace_back(aliasOf(t, i), "1");
+        } else {
+            throw std::runtime_error("analyzed plan: " + aggName(a.func) + " in a hash group-by");
+        }
+    }
+    auto scan = scanFor(plan, table, cols, tune);
+    auto f = selectIf(std::move(scan), combineFilters(aq.filters, "i"));
+    // every row may be its own group: the table is sized by the row count
+    auto gb = std::make_unique<CudaHashGroupBy>(std::move(f), "irg", "(long long)" + key.column + "[i]", "long long",
+                                                "2 * max(n_" + table + ", 1)", tune.hashLayout, tune.maxProbe);
+    for (const auto& [n, v] : aggs) gb->addAggregate(n, v);
+    gb->setWarpAggregate(tune.warpAggregate);
+    gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
+    appendPhase(plan, plan.name + "_aggregate", std::move(gb), tune);
+    plan.decorate.push_back([keyName](CudaResultSchema& rs) { rs.hashAgg.keyName = keyName; });
+    return plan;
+}
+
+// dim JOIN probe ON b_key = p_fk (the Q3 shape).
+CudaQueryPlan planJoin(const AnalyzedQuery& aq, const TuneConfig& tune) {
+    if (aq.joins.size() != 1) throw std::runtime_error("analyzed plan: joins of two tables on one key are planned");
+    const auto& j = aq.joins[0];
+    const ResolvedColumn l = resolveColumn(j.leftTable, j.leftCol), r = resolveColumn(j.rightTable, j.rightCol);
+    const bool ok = (l.table == "dim" && l.column == "b_key" && r.table == "probe" && r.column == "p_fk") ||
+                    (r.table == "dim" && r.column == "b_key" && l.table == "probe" && l.column == "p_fk");
+    if (!ok) throw std::runtime_error("analyzed plan: the join is planned on dim.b_key = probe.p_fk");
+    JoinAggParts jp;
+    std::vector<PredPtr> bf, pf;
+    for (const auto& f : aq.filters) {
+        const std::string t = predicateTable(f);
+        if (t == "dim") bf.push_back(f);
+        else if (t == "probe") pf.push_back(f);
+        else throw std::runtime_error("analyzed plan: a filter on neither joined table");
+    }
+    jp.buildPred = combineFilters(bf, "i");
+    jp.probePred = combineFilters(pf, "i");
+    if (aq.groupBy.size() != 1) throw std::runtime_error("analyzed plan: the join groups by its key");
+    auto g = plainColumn(aq.groupBy[0]);
+    if (!g || !((g->table == "probe" && g->column == "p_fk") || (g->table == "dim" && g->column == "b_key")))
+        throw std::runtime_error("analyzed plan: the join groups by its key (p_fk / b_key)");
+    std::string sumAlias;
+    int nsum = 0;
+    for (size_t i = 0; i < aq.targets.size(); i++) {
+        const auto& t = aq.targets[i];
+        if (!t.isAgg || !t.agg) continue;
+        if (t.agg->func != AggFunc::SUM) throw std::runtime_error("analyzed plan: the join aggregates one SUM");
+        std::vector<ResolvedColumn> cols;
+        collectColumns(t.agg->innerExpr, cols);
+        for (const auto& c : cols)
+            if (c.table != "probe" || (c.column != "p_price" && c.column != "p_discount"))
+                throw std::runtime_error("analyzed plan: the join's SUM reads probe price / discount");
+        jp.revenue = exprToCuda(t.agg->innerExpr, "i").code;
+        sumAlias = aliasOf(t, i);
+        nsum++;
+    }
+    if (nsum != 1) throw std::runtime_error("analyzed plan: the join aggregates one SUM");
+    jp.k = 0;
+    if (aq.limit >= 0) {
+        if (aq.limit < 1 || aq.limit > 32) throw std::runtime_error("analyzed plan: LIMIT must be in [1, 32] for the GPU top-k");
+        if (aq.orderBy.empty() || !aq.orderBy[0].descending ||
+            !(isAliasRef(aq.orderBy[0].expr, sumAlias) || aq.orderBy.size() > 2))
+            throw std::runtime_error("analyzed plan: LIMIT needs ORDER BY the SUM DESC (ties by key ASC)");
+        if (aq.orderBy.size() == 2) {
+            auto k2 = plainColumn(aq.orderBy[1].expr);
+            if (!k2 || aq.orderBy[1].descending || !(k2->column == "p_fk" || k2->column == "b_key"))
+                throw std::runtime_error("analyzed plan: ties are broken by the key ascending");
+        }
+        jp.k = aq.limit;
+    }
+    CudaQueryPlan plan = buildJoinAgg(jp, tune);
+    plan.decorate.push_back([sumAlias](CudaResultSchema& rs) {
+        rs.topk.valueName = sumAlias;
+        if (!rs.hashAgg.aggs.empty()) rs.hashAgg.aggs[0].name = sumAlias;
+    });
+    if (plan.cpuSort) plan.cpuSort->keys[0].column = sumAlias;
+    return plan;
+}
+
+}  // namespace
+
+CudaQueryPlan buildCudaPlan(const ir::AnalyzedQuery& aq, const std::string& queryName, const TuneConfig& tune) {
+    if (aq.tables.empty()) throw std::runtime_error("analyzed plan: no table");
+    for (char ch : queryName)
+        if (!(std::isalnum((unsigned char)ch) || ch == '_'))
+            throw std::runtime_error("analyzed plan: the query name becomes a kernel name: letters, digits, '_'");
+    if (!aq.hasAggregation()) throw std::runtime_error("analyzed plan: only aggregating queries are planned");
+    CudaQueryPlan plan;
+    if (aq.tables.size() == 2 || !aq.joins.empty()) {
+        plan = planJoin(aq, tune);
+    } else if (aq.isSingleTable()) {
+        const std::string table = resolveTable(aq.tables[0]);
+        catalogTable(table);  // throws on an unknown table
+        if (!aq.hasGroupBy()) {
+            if (!aq.orderBy.empty() || aq.limit >= 0)
+                throw std::runtime_error("analyzed plan: ORDER BY / LIMIT of a one-row aggregate");
+            plan = planScalarAgg(aq, table, queryName, tune);
+        } else {
+            std::vector<ResolvedColumn> keys;
+            std::vector<std::string> names;
+            bool allDomains = true;
+            for (const auto& g : aq.groupBy) {
+                auto c = plainColumn(g);
+                if (!c || c->table != table) throw std::runtime_error("analyzed plan: GROUP BY a column of the table");
+                keys.push_back(*c);
+                names.push_back(std::get<ColRef>(g->node).column);
+                allDomains &= !catalogTable(c->table).col(c->column).domain.empty();
+            }
+            if (!aq.orderBy.empty() || aq.limit >= 0)
+                throw std::runtime_error("analyzed plan: ORDER BY / LIMIT of a group-by is planned for joins only");
+            if (allDomains) plan = planKeyedAgg(aq, table, keys, names, queryName, tune);
+            else if (keys.size() == 1 && keys[0].cudaType != "unsigned char")
+                plan = planHashGroupBy(aq, table, keys[0], names[0], queryName, tune);
+            else throw std::runtime_error("analyzed plan: GROUP BY several columns needs known value sets");
+        }
+    } else {
+        throw std::runtime_error("analyzed plan: more than two tables");
+    }
+    if (!queryName.empty()) plan.name = queryName;
+    plan.spec = "analyzed=" + (queryName.empty() ? plan.name : queryName);
     return plan;
 }
 

@@ -13,9 +13,11 @@
 //     labels, FP64 derived columns).
 //
 // The reference builds plans from an AnalyzedQuery produced by its SQL
-// front end (buildMetalPlan, metal_plan_builder.cpp:2035); the SQL parser
-// is out of scope here, so plans are built from a `key=value;...` spec
-// naming a pipeline template and its constants (buildCudaPlan).
+// front end (buildMetalPlan, metal_plan_builder.cpp:2035). Here plans are
+// built from such an analysis (buildCudaPlan(const ir::AnalyzedQuery&),
+// query_ir.h) or from a `key=value;...` spec naming a pipeline template
+// and its constants (buildCudaPlan(spec)), which also covers the reference
+// chains that no analysis shape reaches (anti-join, histogram, ...).
 // ===================================================================
 
 #include <functional>
@@ -36,6 +38,8 @@ namespace gpudb {
 struct ColumnDef {
     std::string name;
     std::string cudaType;  // "int", "long long", "unsigned char"
+    int scale = 0;         // decimal digits of a fixed-point decimal (2: cents / hundredths)
+    std::string domain;    // CHAR1 columns with a known value set, in bucket order ("ANR")
 };
 struct TableDef {
     std::string name;
@@ -130,6 +134,29 @@ std::string canonicalSpec(const SpecMap& m);
 // Build a plan for `spec` (template=...; constants). Throws
 // std::runtime_error on an unknown template / bad constant.
 CudaQueryPlan buildCudaPlan(const std::string& spec, const TuneConfig& tune = {});
+
+namespace ir {
+struct AnalyzedQuery;
+}
+// Plan an analyzed query (reference: buildMetalPlan(const AnalyzedQuery&,
+// name), metal_plan_builder.cpp:2035-2109): the analysis' shape selects the
+// operator chain and its expressions are lowered with ir::exprToCuda /
+// predToCuda:
+//   * one table, aggregates, no GROUP BY      -> Scan -> Selection -> TGReduce
+//     (the Q6 shape, buildQ6Plan :253-303);
+//   * one table, GROUP BY character columns with known value sets (at most
+//     64 groups)                              -> Scan -> Selection -> KeyedAgg
+//     (the Q1 shape, buildQ1Plan :309-354); AVG becomes SUM / COUNT derived
+//     on the host;
+//   * one table, GROUP BY one integer column  -> hash group-by (the Q18
+//     shape, :1529-1545, with an open-addressing table for any key range);
+//   * dim JOIN probe ON b_key = p_fk, GROUP BY the key, one SUM over probe
+//     columns, optionally ORDER BY it DESC (then the key ASC) LIMIT k <= 32
+//                                             -> the semi-join group-by and
+//     GPU top-k (the Q3 shape, :1170-1239).
+// Throws std::runtime_error naming what it cannot plan (the reference
+// returns nullopt).
+CudaQueryPlan buildCudaPlan(const ir::AnalyzedQuery& aq, const std::string& queryName, const TuneConfig& tune = {});
 
 // Generate CUDA source metadata from a plan. Reference:
 // generateFromPlan (metal_plan_builder.cpp:2115-2154).

@@ -111,11 +111,14 @@ def _result_from_c(res) -> Result:
 class Query:
     """A planned + generated (+ compiled) query."""
 
-    def __init__(self, spec: str, tune: str = "", ctx: Optional["Context"] = None):
+    def __init__(self, spec: str, tune: str = "", ctx: Optional["Context"] = None, handle=None):
         self._lib = _lib.load()
         self.spec = spec
         self.tune = tune
         self.ctx = ctx
+        if handle is not None:  # prepared elsewhere (an analyzed query)
+            self.handle = handle
+            return
         h = C.c_void_p()
         st = self._lib.gpudb_query_prepare(ctx.handle if ctx else None, spec.encode(), tune.encode(), C.byref(h))
         check(st, ctx.handle if ctx else None)

@@ -4,9 +4,10 @@
  * What the reference's driver does per query (codegen/codegen_main.cpp:
  * runCodegenQuery :271-1776): plan -> generate source -> compile -> size
  * (max-key pass, exact counts) -> execute -> collect -> post-process. Here
- * the plan comes from a `key=value;...` spec naming a pipeline template
- * (the SQL front end of the reference is out of scope) and the generated
- * language is CUDA C++ for sm_100a.
+ * the plan comes from an analyzed query (the reference's planning input,
+ * built through the gpudb_aq_* functions below), from a `key=value;...`
+ * spec naming a pipeline template, or from SQL through the engine's own
+ * front end; the generated language is CUDA C++ for sm_100a.
  */
 #ifndef GPUDB_ENGINE_H
 #define GPUDB_ENGINE_H
@@ -99,6 +100,81 @@ int gpudb_register_max_key(gpudb_ctx* ctx, const char* column, long long* max_ou
  * and returns GPUDB_OK, or GPUDB_E_PLAN with the reason in
  * gpudb_last_error(NULL, ...). */
 int gpudb_sql_to_spec(const char* sql, char* spec, size_t cap);
+
+/* ---- analyzed queries: the planning layer's input ----------------------
+ * The reference plans from an AnalyzedQuery (codegen/planning/query_plan.h:
+ * 14-183: Expr / Predicate / AggSpec; query_analyzer.h:14-81: joins, select
+ * targets, GROUP BY / ORDER BY / LIMIT) with buildMetalPlan(aq, name)
+ * (planning/metal_plan_builder.h:73, .cpp:2035-2109). A caller holding one
+ * rebuilds it node for node through these functions and plans it with
+ * gpudb_query_prepare_analyzed. Tables and columns are the engine's
+ * catalog names, or lineitem's TPC-H names for the fact table. Decimal
+ * literals (e.g. 0.05) are converted exactly to the columns' fixed point.
+ * Nodes belong to their gpudb_aq and live until gpudb_aq_free; a builder
+ * given a NULL or foreign node returns NULL / GPUDB_E_INVALID. */
+typedef struct gpudb_aq gpudb_aq;
+typedef struct gpudb_expr gpudb_expr;
+typedef struct gpudb_pred gpudb_pred;
+
+/* ExprOp (query_plan.h:25) */
+#define GPUDB_EXPR_ADD 0
+#define GPUDB_EXPR_SUB 1
+#define GPUDB_EXPR_MUL 2
+#define GPUDB_EXPR_DIV 3
+/* CmpOp (query_plan.h:27) */
+#define GPUDB_CMP_EQ 0
+#define GPUDB_CMP_NE 1
+#define GPUDB_CMP_LT 2
+#define GPUDB_CMP_LE 3
+#define GPUDB_CMP_GT 4
+#define GPUDB_CMP_GE 5
+/* AggFunc (query_plan.h:26) */
+#define GPUDB_AGGF_SUM 0
+#define GPUDB_AGGF_COUNT 1
+#define GPUDB_AGGF_AVG 2
+#define GPUDB_AGGF_MIN 3
+#define GPUDB_AGGF_MAX 4
+
+int gpudb_aq_create(gpudb_aq** out);
+void gpudb_aq_free(gpudb_aq* aq);
+/* Expr::col / lit / litf / lits / binary (query_plan.h:60-90). A column
+ * with table "" refers to a select target's alias (ORDER BY revenue). */
+gpudb_expr* gpudb_aq_col(gpudb_aq* aq, const char* table, const char* column);
+gpudb_expr* gpudb_aq_lit_int(gpudb_aq* aq, int64_t v);
+gpudb_expr* gpudb_aq_lit_decimal(gpudb_aq* aq, double v);
+gpudb_expr* gpudb_aq_lit_str(gpudb_aq* aq, const char* v);
+gpudb_expr* gpudb_aq_binary(gpudb_aq* aq, int op, gpudb_expr* l, gpudb_expr* r);
+/* Predicate::cmp / between / inList / logAnd / logOr / logNot (:130-160). */
+gpudb_pred* gpudb_aq_cmp(gpudb_aq* aq, int op, gpudb_expr* l, gpudb_expr* r);
+gpudb_pred* gpudb_aq_between(gpudb_aq* aq, gpudb_expr* e, gpudb_expr* lo, gpudb_expr* hi);
+gpudb_pred* gpudb_aq_in_list(gpudb_aq* aq, gpudb_expr* e, gpudb_expr* const* values, int n);
+gpudb_pred* gpudb_aq_and(gpudb_aq* aq, gpudb_pred* const* children, int n);
+gpudb_pred* gpudb_aq_or(gpudb_aq* aq, gpudb_pred* const* children, int n);
+gpudb_pred* gpudb_aq_not(gpudb_aq* aq, gpudb_pred* child);
+/* AnalyzedQuery fields (query_analyzer.h:38-81). */
+int gpudb_aq_add_table(gpudb_aq* aq, const char* table);
+int gpudb_aq_add_join(gpudb_aq* aq, const char* left_table, const char* left_col, const char* right_table,
+                      const char* right_col);
+int gpudb_aq_add_filter(gpudb_aq* aq, gpudb_pred* p);
+/* A plain select target (a GROUP BY column). */
+int gpudb_aq_add_target(gpudb_aq* aq, gpudb_expr* e, const char* alias);
+/* An aggregate target (SelectTarget with AggTarget); e = NULL is COUNT(*). */
+int gpudb_aq_add_agg(gpudb_aq* aq, int func, gpudb_expr* e, const char* alias);
+int gpudb_aq_add_group_by(gpudb_aq* aq, gpudb_expr* e);
+int gpudb_aq_add_order_by(gpudb_aq* aq, gpudb_expr* e, int descending);
+int gpudb_aq_set_limit(gpudb_aq* aq, int limit);
+/* The kernel expressions an expression / predicate lowers to, with the
+ * decimal scale of the expression's value (for callers that print or
+ * check the lowering; no GPU needed). */
+int gpudb_aq_lower_expr(gpudb_expr* e, char* code, size_t cap, int* scale);
+int gpudb_aq_lower_pred(gpudb_pred* p, char* code, size_t cap);
+/* Plan + generate + compile an analyzed query (reference: buildMetalPlan
+ * (aq, name) then generateFromPlan and RuntimeCompiler::compile). `name`
+ * (may be NULL) names the plan and its kernels; `tune` as for
+ * gpudb_query_prepare; ctx == NULL plans and compiles without loading.
+ * GPUDB_E_PLAN with the reason when the analysis has no plan here. */
+int gpudb_query_prepare_analyzed(gpudb_ctx* ctx, const gpudb_aq* aq, const char* name, const char* tune,
+                                 gpudb_query** out);
 
 /* Template names understood by gpudb_query_prepare, comma separated. */
 size_t gpudb_list_templates(char* buf, size_t cap);

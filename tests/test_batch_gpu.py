@@ -15,25 +15,12 @@ from gpudbmetalcodegen_b200 import batch as B
 from gpudbmetalcodegen_b200 import workloads as W
 from oracle import mlp_oracle as M
 from oracle import oracle_py as O
+from mix_oracle import oracle_result
 
 pytestmark = pytest.mark.gpu
 
 GRAD_RTOL = 2e-3   # |g_gpu - g_cpu| <= GRAD_RTOL * max|g_cpu| + 1e-7, per parameter tensor
 FWD_RTOL = 1e-4
-
-
-def oracle_result(tables, q):
-    m = tables.slice_host(q)
-    if q.tmpl == "agg":
-        c, s = O.mix_agg(m, q.thr)
-        return ("scalar", c, s)
-    if q.tmpl == "join":
-        c, s = O.mix_join(tables.dim_host, m, q.attr_lt, q.thr)
-        return ("scalar", c, s)
-    k, c, s = O.mix_groupby(m, q.key, q.thr, q.card)
-    if q.tmpl == "groupby":
-        return B.canonical_groups(k, c, s)
-    return ("topk", tuple(O.topk(k, s, q.k)))
 
 
 @pytest.fixture(scope="module")

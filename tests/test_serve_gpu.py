@@ -1,19 +1,21 @@
 """GPU: the continuous-batching server. Every answer served in the mix of a
-Poisson trace equals the same query run alone (bit-exact), at two offered
-rates, with overflow re-runs counted and the HBM budget respected."""
+Poisson trace equals the same query run alone and the CPU oracle's answer
+(bit-exact), at two offered rates, with overflow re-runs counted and the
+HBM budget respected."""
 import numpy as np
 import pytest
 
 from gpudbmetalcodegen_b200 import batch as B
 from gpudbmetalcodegen_b200 import serve as S
 from gpudbmetalcodegen_b200 import workloads as W
+from mix_oracle import oracle_result
 
 pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
 def setup(ctx):
-    tables = B.MixTables(rows=2_000_000, zipf_s=(1.1,), nranks=1 << 20, dim_rows=200_000, seed=31)
+    tables = B.MixTables(rows=2_000_000, zipf_s=(1.1,), nranks=1 << 20, dim_rows=200_000, seed=31, host=True)
     log = B.ExecutionLog()
     B.log_executions(tables, W.gen_mixed_queries(4000, seed=7, table_rows=tables.rows, n_tables=1,
                                                  min_rows=10_000, max_rows=tables.rows, max_card=1 << 20), log)
@@ -34,6 +36,10 @@ def test_served_results_equal_queries_alone(setup, rate):
     srv.close()
     alone = [plain.run(q) for q in qs]
     bad = [(i, B.describe_difference(a, b)) for i, (a, b) in enumerate(zip(served, alone))
+           if not B.same_result(a, b)]
+    assert not bad, bad[:3]
+    expect = [oracle_result(tables, q) for q in qs]
+    bad = [(i, qs[i], B.describe_difference(a, b)) for i, (a, b) in enumerate(zip(served, expect))
            if not B.same_result(a, b)]
     assert not bad, bad[:3]
     s = rep.summary()
