@@ -1,7 +1,9 @@
-"""ctypes bindings for libgpudb.so (include/gpudb_rt.h, gpudb_engine.h, gpudb_datagen.h).
+"""ctypes bindings for libgpudb.so (include/gpudb_rt.h, gpudb_engine.h,
+gpudb_batch.h) and for the data generators' own library libgpudb_datagen.so
+(include/gpudb_datagen.h).
 
-The shared library is built in-tree by ``build_native.build()``. Loading fails
-loudly when it is missing: there is no Python or CPU fallback for any
+Both are built in-tree by ``build_native.build()``. Loading fails loudly
+when a library is missing: there is no Python or CPU fallback for any
 operation of the engine.
 """
 from __future__ import annotations
@@ -11,6 +13,7 @@ import os
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgpudb.so"
+DATAGEN_PATH = Path(__file__).resolve().parent / "lib" / "libgpudb_datagen.so"
 
 GPUDB_OK = 0
 STATUS_NAMES = {0: "OK", -1: "INVALID", -2: "PLAN", -3: "ALLOC", -4: "LAUNCH", -5: "COMPILE", -6: "CUDA",
@@ -125,6 +128,7 @@ _SIGNATURES = [
     ("gpudb_query_prepare_analyzed", C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p, C.c_char_p,
                                                C.POINTER(C.c_void_p)]),
     # gpudb_engine.h
+    ("gpudb_query_collect", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     ("gpudb_query_prepare", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     ("gpudb_query_free", None, [C.c_void_p]),
     ("gpudb_query_source", C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
@@ -149,21 +153,6 @@ _SIGNATURES = [
     ("gpudb_register_max_key", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_longlong)]),
     ("gpudb_list_templates", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("gpudb_version", C.c_char_p, []),
-    # gpudb_datagen.h
-    ("gpudb_gen_fact", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 7 + [C.c_int]),
-    ("gpudb_gen_dim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 3 + [C.c_int]),
-    ("gpudb_gen_probe", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 4 + [C.c_int]),
-    ("gpudb_gen_order_day", C.c_int32, [C.c_uint64, C.c_int64]),
-    ("gpudb_gen_zbuild", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
-    ("gpudb_gen_zprobe", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_void_p,
-                                   C.c_void_p, C.c_int]),
-    ("gpudb_gen_zkey", C.c_int64, [C.c_uint64, C.c_uint64]),
-    ("gpudb_gen_mix", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
-     + [C.c_void_p] * 5 + [C.c_int]),
-    ("gpudb_gen_mixdim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
-    ("gpudb_gen_mix_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
-     + [C.c_void_p] * 6),
-    ("gpudb_gen_mixdim_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     # gpudb_batch.h
     ("gpudb_sizer_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     ("gpudb_sizer_free", None, [C.c_void_p]),
@@ -197,9 +186,29 @@ _SIGNATURES = [
     ("gpudb_batch_stage_ms", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
 
+_DATAGEN_SIGNATURES = [
+    ("gpudb_gen_fact", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 7 + [C.c_int]),
+    ("gpudb_gen_dim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 3 + [C.c_int]),
+    ("gpudb_gen_probe", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 4 + [C.c_int]),
+    ("gpudb_gen_order_day", C.c_int32, [C.c_uint64, C.c_int64]),
+    ("gpudb_gen_zbuild", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_zprobe", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_void_p,
+                                   C.c_void_p, C.c_int]),
+    ("gpudb_gen_zkey", C.c_int64, [C.c_uint64, C.c_uint64]),
+    ("gpudb_gen_mix", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
+     + [C.c_void_p] * 5 + [C.c_int]),
+    ("gpudb_gen_mixdim", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_mix_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64]
+     + [C.c_void_p] * 6),
+    ("gpudb_gen_mixdim_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gpudb_datagen_last_error", C.c_char_p, []),
+]
+
 EXPORTED = [s[0] for s in _SIGNATURES]
+DATAGEN_EXPORTED = [s[0] for s in _DATAGEN_SIGNATURES]
 
 _lib = None
+_datagen = None
 
 
 class GpudbError(RuntimeError):
@@ -224,6 +233,27 @@ def load() -> C.CDLL:
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def load_datagen() -> C.CDLL:
+    """Load libgpudb_datagen.so, the seeded table generators (raises if it
+    was not built). It maps no engine code."""
+    global _datagen
+    if _datagen is not None:
+        return _datagen
+    if not DATAGEN_PATH.exists():
+        raise RuntimeError(f"{DATAGEN_PATH} is missing: run gpudbmetalcodegen_b200.build_native.build()")
+    lib = C.CDLL(str(DATAGEN_PATH), mode=os.RTLD_NOW)
+    for name, res, args in _DATAGEN_SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _datagen = lib
+    return lib
+
+
+def datagen_error() -> str:
+    return (load_datagen().gpudb_datagen_last_error() or b"").decode(errors="replace")
 
 
 def last_error(ctx) -> str:

@@ -41,7 +41,6 @@ HOST_SOURCES = [
     "execution/executor.cpp",
     "execution/query_engine.cpp",
     "capi/gpudb_capi.cpp",
-    "datagen/datagen.cpp",
     "io/colbin.cpp",
     "sql/sql_frontend.cpp",
 ]
@@ -49,10 +48,14 @@ CUDA_SOURCES: list[str] = [
     "kernels/noalloc_distinct.cu",
     "kernels/sizer_mlp.cu",
     "kernels/batch_kernels.cu",
-    "kernels/datagen_device.cu",
 ]
 
 LIB_NAME = "libgpudb.so"
+# the seeded synthetic-table generators: their own library, so that data
+# generation (CPU baselines, fixtures) maps no engine code
+DATAGEN_HOST_SOURCES = ["datagen/datagen.cpp"]
+DATAGEN_CUDA_SOURCES = ["kernels/datagen_device.cu"]
+DATAGEN_LIB_NAME = "libgpudb_datagen.so"
 
 
 def _headers() -> list[Path]:
@@ -94,31 +97,38 @@ def embed_device_header() -> Path:
     return out
 
 
+def _build_lib(name: str, host: list[str], cuda: list[str], extra: list[str], headers: list[Path], force: bool,
+               log: list[str]) -> Path:
+    objs = []
+    for rel in host:
+        src = CSRC / rel
+        obj = BUILD / (rel.replace("/", "_") + ".o")
+        if force or _stale(obj, [src] + headers):
+            _run([CXX, *CXXFLAGS, "-c", str(src), "-o", str(obj)], log)
+        objs.append(obj)
+    for rel in cuda:
+        src = CSRC / rel
+        obj = BUILD / (rel.replace("/", "_") + ".o")
+        if force or _stale(obj, [src] + headers):
+            _run([NVCC, *NVCCFLAGS, "-c", str(src), "-o", str(obj)], log)
+        objs.append(obj)
+    lib = LIB / name
+    if force or _stale(lib, objs):
+        cudalib = CUDA_HOME / "lib64"
+        _run([NVCC, "-shared", *ARCH, "-o", str(lib), *map(str, objs),
+              f"-L{cudalib}", *extra, "-cudart", "static", "-ldl", "-lpthread", "-lrt",
+              f"-Xlinker", f"-rpath={cudalib}"], log)
+    return lib
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     LIB.mkdir(exist_ok=True)
     embed_device_header()
     headers = _headers()
     log: list[str] = []
-    objs = []
-    for rel in HOST_SOURCES:
-        src = CSRC / rel
-        obj = BUILD / (rel.replace("/", "_") + ".o")
-        if force or _stale(obj, [src] + headers):
-            _run([CXX, *CXXFLAGS, "-c", str(src), "-o", str(obj)], log)
-        objs.append(obj)
-    for rel in CUDA_SOURCES:
-        src = CSRC / rel
-        obj = BUILD / (rel.replace("/", "_") + ".o")
-        if force or _stale(obj, [src] + headers):
-            _run([NVCC, *NVCCFLAGS, "-c", str(src), "-o", str(obj)], log)
-        objs.append(obj)
-    lib = LIB / LIB_NAME
-    if force or _stale(lib, objs):
-        cudalib = CUDA_HOME / "lib64"
-        _run([NVCC, "-shared", *ARCH, "-o", str(lib), *map(str, objs),
-              f"-L{cudalib}", "-lnvrtc", "-cudart", "static", "-ldl", "-lpthread", "-lrt",
-              f"-Xlinker", f"-rpath={cudalib}"], log)
+    lib = _build_lib(LIB_NAME, HOST_SOURCES, CUDA_SOURCES, ["-lnvrtc"], headers, force, log)
+    _build_lib(DATAGEN_LIB_NAME, DATAGEN_HOST_SOURCES, DATAGEN_CUDA_SOURCES, [], headers, force, log)
     if verbose:
         print("\n".join(log))
     return lib

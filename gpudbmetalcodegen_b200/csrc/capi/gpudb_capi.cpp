@@ -533,6 +533,19 @@ int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gp
     })
 }
 
+int gpudb_query_collect(gpudb_ctx* ctx, gpudb_query* q, gpudb_result** result) {
+    if (!ctx || !q || !result) return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    *result = nullptr;
+    GPUDB_GUARD(ctx, {
+        cudaSetDevice(ctx->qc->ex.device());
+        if (!q->q->compiled) return fail(ctx, GPUDB_E_INVALID, "the query has not run in this context");
+        if (cudaStreamSynchronize(static_cast<cudaStream_t>(ctx->qc->ex.stream())) != cudaSuccess)
+            return fail(ctx, GPUDB_E_CUDA, "stream synchronize failed");
+        *result = new gpudb_result{ctx->qc->ex.collectResult(q->q->cg.getResultSchema())};
+        return GPUDB_OK;
+    })
+}
+
 int gpudb_query_enqueue(gpudb_ctx* ctx, gpudb_query* q) {
     if (!ctx || !q) return fail(ctx, GPUDB_E_INVALID, "bad argument");
     GPUDB_GUARD(ctx, {

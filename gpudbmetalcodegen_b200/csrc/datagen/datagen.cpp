@@ -4,6 +4,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -97,13 +98,21 @@ inline int64_t zkey(uint64_t seed, uint64_t rank) {
 
 }  // namespace
 
-namespace gpudb {
+namespace gpudb_gen {
 // Zipf(s) CDF over [0, n) (cached for the process), shared with the device
 // generators so both search the same table.
 const std::vector<double>& zipfCdf(uint64_t n, double s) { return zipf(n, s)->cdf; }
-}  // namespace gpudb
+
+// The last failure of a device generator on this thread (the generators'
+// own library keeps its own error text).
+thread_local std::string tlError;
+void setError(const std::string& message) { tlError = message; }
+}  // namespace gpudb_gen
 
 extern "C" {
+
+const char* gpudb_datagen_last_error(void) { return gpudb_gen::tlError.c_str(); }
+
 
 int gpudb_gen_fact(uint64_t seed, uint64_t row0, uint64_t n, int32_t* ship_day, int64_t* quantity, int64_t* price,
                    int64_t* discount, int64_t* tax, uint8_t* flag_a, uint8_t* flag_b, int threads) {

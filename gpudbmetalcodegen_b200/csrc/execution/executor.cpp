@@ -261,7 +261,8 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
     l.name = ph.name;
     l.block = ph.isSingleThread ? 1u : (unsigned)ph.threadgroupSize;
     l.smem = (unsigned)ph.dynamicSmemBytes;
-    auto sc = smemConfigured_.find(l.fn);
+    const std::pair<uint64_t, CUfunction> fkey{cq.loadId, l.fn};
+    auto sc = smemConfigured_.find(fkey);
     if (l.smem > 48 * 1024 && (sc == smemConfigured_.end() || sc->second < (int)l.smem)) {
         const CUresult r = api.cuFuncSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)l.smem);
         if (r != CUDA_SUCCESS) {
@@ -269,10 +270,10 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
                     cuErrorString(r) + ")";
             return false;
         }
-        smemConfigured_[l.fn] = (int)l.smem;
+        smemConfigured_[fkey] = (int)l.smem;
     }
     if (ph.smemCarveout >= 0 && l.smem > 0) {
-        auto cv = carveoutSet_.find(l.fn);
+        auto cv = carveoutSet_.find(fkey);
         if (cv == carveoutSet_.end() || cv->second != ph.smemCarveout) {
             const CUresult r = api.cuFuncSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT,
                                                       ph.smemCarveout);
@@ -280,7 +281,7 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
                 error = "phase '" + ph.name + "': cannot set the shared-memory carveout (" + cuErrorString(r) + ")";
                 return false;
             }
-            carveoutSet_[l.fn] = ph.smemCarveout;
+            carveoutSet_[fkey] = ph.smemCarveout;
         }
     }
     int occ = 0;
@@ -469,7 +470,10 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
     }
     const int total = warmup + measured;
     if (useGraphs_) {
-        std::string key = cq.key + ":" + std::to_string(first) + ":" + std::to_string(last);
+        // the load id: a graph captured from a module that was unloaded and
+        // loaded again (same source key) must never be replayed
+        std::string key = cq.key + "#" + std::to_string(cq.loadId) + ":" + std::to_string(first) + ":" +
+                          std::to_string(last);
         for (const auto& l : launches) {
             key += ":" + std::to_string(l.grid);
             for (auto s : l.slots) key += "," + std::to_string(s);

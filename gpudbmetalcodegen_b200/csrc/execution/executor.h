@@ -145,8 +145,9 @@ private:
     std::unordered_map<std::string, Buffer> ownedColumns_;
     std::unordered_map<std::string, long long> scalarInts_;
     std::unordered_map<std::string, double> scalarFloats_;
-    std::map<CUfunction, int> smemConfigured_;
-    std::map<CUfunction, int> carveoutSet_;
+    // keyed by (load id, function): handles of an unloaded module recur
+    std::map<std::pair<uint64_t, CUfunction>, int> smemConfigured_;
+    std::map<std::pair<uint64_t, CUfunction>, int> carveoutSet_;
     std::vector<cudaEvent_t> events_;
     struct GraphEntry {
         cudaGraph_t graph = nullptr;

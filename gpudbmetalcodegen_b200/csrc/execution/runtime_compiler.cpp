@@ -1,5 +1,7 @@
 #include "runtime_compiler.h"
 
+#include <atomic>
+
 #include <dlfcn.h>
 #include <nvrtc.h>
 #include <sys/stat.h>
@@ -203,7 +205,9 @@ std::shared_ptr<RuntimeCompiler::CompiledQuery> RuntimeCompiler::compileAndLoad(
         error = "CUDA driver API unavailable: " + api.error;
         return nullptr;
     }
+    static std::atomic<uint64_t> loads{0};
     auto cq = std::make_shared<CompiledQuery>();
+    cq->loadId = ++loads;
     cq->key = art.key;
     cq->log = art.log;
     cq->compileMs = art.compileMs;

@@ -52,6 +52,10 @@ public:
         std::string log;
         double compileMs = 0.0;
         bool cached = false;
+        // Unique per load: a module unloaded and loaded again may reuse its
+        // CUfunction handles, so per-function caches (shared-memory
+        // attributes, captured graphs) are keyed by this, not by handles.
+        uint64_t loadId = 0;
         ~CompiledQuery();
     };
 

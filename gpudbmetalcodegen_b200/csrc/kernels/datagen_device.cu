@@ -11,10 +11,10 @@
 #include "../../../include/gpudb_datagen.h"
 #include "../datagen/datagen_core.h"
 
-namespace gpudb {
+namespace gpudb_gen {
 const std::vector<double>& zipfCdf(uint64_t n, double s);
-void setThreadError(const std::string& message);
-}  // namespace gpudb
+void setError(const std::string& message);  // datagen.cpp: gpudb_datagen_last_error
+}  // namespace gpudb_gen
 
 namespace {
 
@@ -52,7 +52,7 @@ int gridFor(uint64_t n) {
     do {                                                                                          \
         const cudaError_t _e = (call);                                                            \
         if (_e != cudaSuccess) {                                                                  \
-            gpudb::setThreadError(std::string("datagen: ") + #call + ": " + cudaGetErrorString(_e)); \
+            gpudb_gen::setError(std::string("datagen: ") + #call + ": " + cudaGetErrorString(_e)); \
             return -1;                                                                            \
         }                                                                                         \
     } while (0)
@@ -69,7 +69,7 @@ int gpudb_gen_mix_device(uint64_t seed, uint64_t nranks, double s, uint64_t dim_
         return -1;
     if (n == 0) return 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const std::vector<double>& cdf = gpudb::zipfCdf(nranks, s);
+    const std::vector<double>& cdf = gpudb_gen::zipfCdf(nranks, s);
     double* dcdf = nullptr;
     G_CHECK(cudaMallocAsync((void**)&dcdf, sizeof(double) * nranks, st));
     G_CHECK(cudaMemcpyAsync(dcdf, cdf.data(), sizeof(double) * nranks, cudaMemcpyHostToDevice, st));

@@ -121,6 +121,44 @@ __device__ __forceinline__ void gpudb_acc64_add(unsigned long long* word, long l
 }
 
 // ------------------------------------------------------------------
+// Remainder by a divisor known only at run time but the same for every
+// row (a group key k % card with card a kernel argument): division by an
+// invariant integer through a multiply-high (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994,
+// Fig. 4.1). With l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), t = mulhi(m, n),
+// exact for 32-bit n and 1 <= d < 2^32. Each thread derives (m, l) once.
+// ------------------------------------------------------------------
+struct gpudb_divmagic {
+    unsigned magic;
+    int sh1, sh2;
+    long long d;
+};
+
+__device__ __forceinline__ gpudb_divmagic gpudb_divmagic_make(long long d) {
+    gpudb_divmagic m;
+    m.d = d < 1 ? 1 : d;
+    const unsigned long long ud = (unsigned long long)m.d;
+    int l = 0;
+    while (l < 32 && (1ull << l) < ud) l++;
+    m.magic = (unsigned)(((1ull << 32) * ((1ull << l) - ud)) / ud + 1ull);
+    m.sh1 = l < 1 ? l : 1;
+    m.sh2 = l - 1 > 0 ? l - 1 : 0;
+    return m;
+}
+
+// k % d for a 32-bit key, with the sign of k (C semantics) for negative k.
+__device__ __forceinline__ long long gpudb_mod_i32(int k, const gpudb_divmagic& m) {
+    if (k >= 0 && m.d < (1ll << 32)) {
+        const unsigned n = (unsigned)k;
+        const unsigned t = __umulhi(n, m.magic);
+        const unsigned quo = (t + ((n - t) >> m.sh1)) >> m.sh2;
+        return (long long)(n - quo * (unsigned)m.d);
+    }
+    return (long long)k % m.d;
+}
+
+// ------------------------------------------------------------------
 // Bitmaps (semi / anti joins). Reference: bitmap_test / bitmap_set,
 // metal_common_header.h:103-111.
 // ------------------------------------------------------------------

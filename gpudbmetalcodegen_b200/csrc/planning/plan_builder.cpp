@@ -678,17 +678,63 @@ CudaQueryPlan buildColMax(Spec& s, const TuneConfig& tune) {
 
 // ---- distinct: exact distinct count of (key % card) over rows passing a
 // filter; the exact count pass of the mixed group-by templates.
+// Constants of the mixed templates: compiled into the source, or (spec
+// params=1) kernel arguments bound at launch from the registered symbols
+// mix_thr / mix_card / mix_attr_lt, so one module serves every query of a
+// template (a group key's remainder then goes through the invariant-divisor
+// multiply-high, gpudb_mod_i32).
+struct MixConsts {
+    bool params = false;
+    std::string thr, card, attrLt, keyMod;
+    std::vector<CudaQueryPlan::Phase::SizeScalar> scalars;
+    std::vector<std::string> prologue;
+};
+
+MixConsts mixConsts(Spec& s, const std::string& keyCol, bool grouped, bool join) {
+    MixConsts c;
+    c.params = s.num("params", 0) != 0;
+    if (!c.params) {
+        c.thr = std::to_string(s.num("thr", 10000));
+        if (grouped) {
+            c.card = L(s.num("card", 1024));
+            c.keyMod = "(long long)" + keyCol + "[i] % " + c.card;
+        }
+        if (join) c.attrLt = std::to_string(s.num("attr_lt", 500));
+        return c;
+    }
+    for (const char* k : {"thr", "card", "attr_lt"})
+        if (s.has(k)) throw std::runtime_error(std::string("spec: '") + k + "' with params=1 (bound at launch from the symbol)");
+    c.thr = "mix_thr";
+    c.scalars.push_back({"mix_thr", "int", "mix_thr"});
+    if (grouped) {
+        c.card = "mix_card";
+        c.scalars.push_back({"mix_card", "long long", "mix_card"});
+        c.prologue.push_back("const gpudb_divmagic _mix_div = gpudb_divmagic_make(mix_card);");
+        c.keyMod = "gpudb_mod_i32(" + keyCol + "[i], _mix_div)";
+    }
+    if (join) {
+        c.attrLt = "mix_attr_lt";
+        c.scalars.push_back({"mix_attr_lt", "int", "mix_attr_lt"});
+    }
+    return c;
+}
+
+void bindConsts(CudaQueryPlan::Phase& ph, const MixConsts& c) {
+    for (const auto& x : c.scalars) ph.sizeScalars.push_back(x);
+    for (const auto& l : c.prologue) ph.prologue.push_back(l);
+}
+
 CudaQueryPlan buildDistinct(Spec& s, const TuneConfig& tune) {
     CudaQueryPlan plan;
     plan.name = "DISTINCT";
     const std::string keyCol = s.str("key", "m_rank_u");
-    const long long card = s.num("card", 1024), thr = s.num("thr", 10000);
+    const MixConsts mc = mixConsts(s, keyCol, true, false);
+    const std::string bits = mc.params ? "mix_card / 32 + 1" : std::to_string(s.num("card", 1024) / 32 + 1);
     auto scan = makeScan(plan, "mix", {keyCol, "m_filter"}, tune);
-    auto f = std::make_unique<CudaSelection>(std::move(scan), "m_filter[i] < " + std::to_string(thr));
-    auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "dc_bitmap", "(long long)" + keyCol + "[i] % " + L(card),
-                                                std::to_string(card / 32 + 1));
+    auto f = std::make_unique<CudaSelection>(std::move(scan), "m_filter[i] < " + mc.thr);
+    auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "dc_bitmap", mc.keyMod, bits);
     bm->setDistinctCounter("dc_distinct");
-    appendPhase(plan, "DC_count", std::move(bm), tune);
+    bindConsts(appendPhase(plan, "DC_count", std::move(bm), tune), mc);
     plan.decorate.push_back([](CudaResultSchema& rs) {
         rs.kind = CudaResultSchema::SCALAR_AGG;
         rs.scalarAggs = {{"distinct", "dc_distinct", false, 0}};
@@ -704,24 +750,25 @@ CudaQueryPlan buildDistinct(Spec& s, const TuneConfig& tune) {
 CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune) {
     CudaQueryPlan plan;
     plan.name = tmpl;
-    const long long thr = s.num("thr", 10000);
-    const std::string filt = "m_filter[i] < " + std::to_string(thr);
+    const bool grouped = tmpl == "mix_groupby" || tmpl == "mix_topk";
+    const std::string keyCol = grouped ? s.str("key", "m_rank_u") : "m_rank_u";
+    const MixConsts mc = mixConsts(s, keyCol, grouped, tmpl == "mix_join");
+    const std::string filt = "m_filter[i] < " + mc.thr;
     if (tmpl == "mix_agg") {
         auto scan = makeScan(plan, "mix", {"m_filter", "m_value"}, tune);
         auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
         auto r = std::make_unique<CudaTGReduce>(std::move(f), "d_mix");
         r->addAccumulator("count", "1", "long");
         r->addAccumulator("sum", "m_value[i]", "wide");
-        appendPhase(plan, "MIX_agg", std::move(r), tune);
+        bindConsts(appendPhase(plan, "MIX_agg", std::move(r), tune), mc);
         return plan;
     }
     if (tmpl == "mix_join") {
-        const long long attrLt = s.num("attr_lt", 500);
         {
             auto scan = makeScan(plan, "mixdim", {"md_key", "md_attr"}, tune);
-            auto f = std::make_unique<CudaSelection>(std::move(scan), "md_attr[i] < " + std::to_string(attrLt));
+            auto f = std::make_unique<CudaSelection>(std::move(scan), "md_attr[i] < " + mc.attrLt);
             auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "mj_bitmap", "md_key[i]", "max_md_key / 32 + 1");
-            appendPhase(plan, "MIXJ_build", std::move(bm), tune);
+            bindConsts(appendPhase(plan, "MIXJ_build", std::move(bm), tune), mc);
         }
         auto scan = makeScan(plan, "mix", {"m_fk", "m_filter"}, tune, true, {"m_value"});
         auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
@@ -729,24 +776,26 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
         auto r = std::make_unique<CudaTGReduce>(std::move(pr), "d_mixj");
         r->addAccumulator("count", "1", "long");
         r->addAccumulator("sum", "m_value[i]", "wide");
-        appendPhase(plan, "MIXJ_probe", std::move(r), tune);
+        bindConsts(appendPhase(plan, "MIXJ_probe", std::move(r), tune), mc);
         return plan;
     }
-    const std::string keyCol = s.str("key", "m_rank_u");
-    const long long card = s.num("card", 1024);
     const long long k = s.num("k", 10);
     const std::string groups = s.str("groups", "mix_groups");
     const std::string cap = "2 * max(" + groups + ", 1)";
+    // compact=1: the created groups are gathered on the device into dense
+    // (key, count, sum) arrays, so collecting the result copies groups x 24
+    // bytes instead of the whole table
+    const bool compact = tmpl == "mix_groupby" && s.num("compact", 0) != 0;
     auto scan = makeScan(plan, "mix", {keyCol, "m_filter", "m_value"}, tune);
     auto f = std::make_unique<CudaSelection>(std::move(scan), filt);
-    auto gb = std::make_unique<CudaHashGroupBy>(std::move(f), "mg", "(long long)" + keyCol + "[i] % " + L(card),
-                                                "long long", cap, tune.hashLayout, tune.maxProbe);
+    auto gb = std::make_unique<CudaHashGroupBy>(std::move(f), "mg", mc.keyMod, "long long", cap, tune.hashLayout,
+                                                tune.maxProbe);
     gb->addAggregate("count", "1");
     gb->addAggregate("sum", "m_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
     gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
-    gb->setSlotList(tmpl == "mix_topk");
-    appendPhase(plan, "MIXG_group", std::move(gb), tune);
+    gb->setSlotList(tmpl == "mix_topk" || compact);
+    bindConsts(appendPhase(plan, "MIXG_group", std::move(gb), tune), mc);
     if (tmpl == "mix_topk") {
         auto lscan = std::make_unique<CudaSlotListScan>("mg_slotlist", "mg_nslots");
         auto tk = std::make_unique<CudaTopK>(std::move(lscan), "mt_top", "(long long)mg_keys[i]", "(long long)mg_sum[i]",
@@ -756,6 +805,18 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
         ph.extraBuffers.push_back({"mg_keys", "unsigned long long", true, false});
         ph.extraBuffers.push_back({"mg_sum", "unsigned long long", true, false});
         plan.decorate.push_back([](CudaResultSchema& rs) { rs.topk.valueName = "sum"; });
+    }
+    if (compact) {
+        auto lscan = std::make_unique<CudaSlotListScan>("mg_slotlist", "mg_nslots");
+        auto mt = std::make_unique<CudaMaterialize>(std::move(lscan), "mgc_n", "max(" + groups + ", 1)");
+        mt->addColumn("mgc_key", "long long", "(long long)mg_keys[i]", "key");
+        mt->addColumn("mgc_count", "long long", "(long long)mg_count[i]", "count");
+        mt->addColumn("mgc_sum", "long long", "(long long)mg_sum[i]", "sum");
+        auto& ph = appendPhase(plan, "MIXG_compact", std::move(mt), tune);
+        ph.minBlocksPerSM = 1;
+        ph.extraBuffers.push_back({"mg_keys", "unsigned long long", true, false});
+        ph.extraBuffers.push_back({"mg_count", "unsigned long long", true, false});
+        ph.extraBuffers.push_back({"mg_sum", "unsigned long long", true, false});
     }
     return plan;
 }
@@ -1155,10 +1216,12 @@ CudaCodegen generateFromPlan(const CudaQueryPlan& plan) {
         cg.setPhaseSmemCarveout(ph.smemCarveout);
         for (const auto& [n, sz] : ph.bitmapReads) cg.addBitmapReadParam(n, sz);
         for (const auto& [n, t] : ph.scalarParams) cg.addScalarParam(n, t);
+        for (const auto& ss : ph.sizeScalars) cg.addSizeScalarParam(ss.name, ss.type, ss.expr);
         for (const auto& eb : ph.extraBuffers) {
             if (eb.readOnly) cg.addReadBufferParam(eb.name, eb.type);
             else cg.addBufferParam(eb.name, eb.type, "", eb.zeroInit);
         }
+        for (const auto& line : ph.prologue) cg.addLine(line);
         if (ph.root) ph.root->produce(cg, []() {});
         cg.endPhase();
     }

@@ -60,6 +60,13 @@ struct CudaQueryPlan {
         bool singleThread = false;
         std::vector<std::pair<std::string, std::string>> bitmapReads;   // (name, sizeExpr)
         std::vector<std::pair<std::string, std::string>> scalarParams;  // (name, type)
+        // scalars whose value is a size expression over registered symbols
+        // (name, type, expression): constants bound at launch, not compiled in
+        struct SizeScalar {
+            std::string name, type, expr;
+        };
+        std::vector<SizeScalar> sizeScalars;
+        std::vector<std::string> prologue;  // lines before the root operator's code
         struct ExtraBuffer {
             std::string name, type;
             bool readOnly = true;

@@ -313,6 +313,16 @@ class Context:
                 self._lib.gpudb_result_free(res)
         return out, timing
 
+    def collect(self, query: "Query") -> Result:
+        """The result the last execution of `query` left in the buffers
+        (e.g. the last of many enqueued graph replays), without running it."""
+        res = C.c_void_p()
+        check(self._lib.gpudb_query_collect(self.handle, query.handle, C.byref(res)), self.handle)
+        try:
+            return _result_from_c(res)
+        finally:
+            self._lib.gpudb_result_free(res)
+
     def enqueue(self, spec_or_query, tune: str = "") -> None:
         """Enqueue one execution and return without waiting (no timing, no
         result). Device errors surface at the next sync() or run()."""

@@ -45,7 +45,7 @@ def _p(a: np.ndarray) -> int:
 
 def gen_fact(n: int = FACT_ROWS, seed: int = SEED, row0: int = 0, threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(FACT_COLUMNS, n)
-    st = _lib.load().gpudb_gen_fact(seed, row0, n, *(_p(t[c]) for c in FACT_COLUMNS), threads)
+    st = _lib.load_datagen().gpudb_gen_fact(seed, row0, n, *(_p(t[c]) for c in FACT_COLUMNS), threads)
     assert st == 0
     return t
 
@@ -54,7 +54,7 @@ def gen_dim(n: int = DIM_ROWS, seed: int = SEED, row0: int = 0, count: int = -1,
             threads: int = 0) -> Dict[str, np.ndarray]:
     count = n - row0 if count < 0 else count
     t = _alloc(DIM_COLUMNS, count)
-    st = _lib.load().gpudb_gen_dim(seed, n, row0, count, *(_p(t[c]) for c in DIM_COLUMNS), threads)
+    st = _lib.load_datagen().gpudb_gen_dim(seed, n, row0, count, *(_p(t[c]) for c in DIM_COLUMNS), threads)
     assert st == 0
     return t
 
@@ -62,14 +62,14 @@ def gen_dim(n: int = DIM_ROWS, seed: int = SEED, row0: int = 0, count: int = -1,
 def gen_probe(n: int = PROBE_ROWS, dim_rows: int = DIM_ROWS, seed: int = SEED, row0: int = 0,
               threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(PROBE_COLUMNS, n)
-    st = _lib.load().gpudb_gen_probe(seed, dim_rows, row0, n, *(_p(t[c]) for c in PROBE_COLUMNS), threads)
+    st = _lib.load_datagen().gpudb_gen_probe(seed, dim_rows, row0, n, *(_p(t[c]) for c in PROBE_COLUMNS), threads)
     assert st == 0
     return t
 
 
 def gen_zbuild(nkeys: int = ZKEYS, seed: int = SEED, threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(ZBUILD_COLUMNS, nkeys)
-    st = _lib.load().gpudb_gen_zbuild(seed, 0, nkeys, _p(t["zb_key"]), _p(t["zb_payload"]), threads)
+    st = _lib.load_datagen().gpudb_gen_zbuild(seed, 0, nkeys, _p(t["zb_key"]), _p(t["zb_payload"]), threads)
     assert st == 0
     return t
 
@@ -77,7 +77,7 @@ def gen_zbuild(nkeys: int = ZKEYS, seed: int = SEED, threads: int = 0) -> Dict[s
 def gen_zprobe(n: int = ZPROBE_ROWS, nkeys: int = ZKEYS, s: float = ZIPF_S, seed: int = SEED, row0: int = 0,
                threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(ZPROBE_COLUMNS, n)
-    st = _lib.load().gpudb_gen_zprobe(seed, nkeys, s, row0, n, _p(t["z_key"]), _p(t["z_value"]), threads)
+    st = _lib.load_datagen().gpudb_gen_zprobe(seed, nkeys, s, row0, n, _p(t["z_key"]), _p(t["z_value"]), threads)
     assert st == 0
     return t
 
@@ -85,14 +85,14 @@ def gen_zprobe(n: int = ZPROBE_ROWS, nkeys: int = ZKEYS, s: float = ZIPF_S, seed
 def gen_mix(n: int, nranks: int = 1 << 22, s: float = ZIPF_S, dim_rows: int = 1_000_000, seed: int = SEED,
             row0: int = 0, threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(MIX_COLUMNS, n)
-    st = _lib.load().gpudb_gen_mix(seed, nranks, s, dim_rows, row0, n, *(_p(t[c]) for c in MIX_COLUMNS), threads)
+    st = _lib.load_datagen().gpudb_gen_mix(seed, nranks, s, dim_rows, row0, n, *(_p(t[c]) for c in MIX_COLUMNS), threads)
     assert st == 0
     return t
 
 
 def gen_mixdim(n: int = 1_000_000, seed: int = SEED, threads: int = 0) -> Dict[str, np.ndarray]:
     t = _alloc(MIXDIM_COLUMNS, n)
-    st = _lib.load().gpudb_gen_mixdim(seed, 0, n, _p(t["md_key"]), _p(t["md_attr"]), threads)
+    st = _lib.load_datagen().gpudb_gen_mixdim(seed, 0, n, _p(t["md_key"]), _p(t["md_attr"]), threads)
     assert st == 0
     return t
 

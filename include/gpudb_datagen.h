@@ -11,6 +11,10 @@
  *
  * All functions fill caller-provided host arrays and return 0, or -1 on a
  * bad argument. `threads` <= 0 means all hardware threads.
+ *
+ * The generators live in their own library, libgpudb_datagen.so, next to
+ * libgpudb.so: a program that only needs the data (a CPU baseline, a test
+ * fixture) loads no engine code.
  */
 #ifndef GPUDB_DATAGEN_H
 #define GPUDB_DATAGEN_H
@@ -63,6 +67,8 @@ int gpudb_gen_mix_device(uint64_t seed, uint64_t nranks, double s, uint64_t dim_
                          int32_t* rank_u, int32_t* rank_z, int32_t* filter, int64_t* value, int32_t* fk,
                          void* stream);
 int gpudb_gen_mixdim_device(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* attr, void* stream);
+/* Text of the last device-generator failure on this thread ("" if none). */
+const char* gpudb_datagen_last_error(void);
 
 #ifdef __cplusplus
 }

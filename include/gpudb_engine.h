@@ -60,6 +60,13 @@ int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gp
  * reads them. The reference runs one blocking execution per invocation
  * (MetalGenericExecutor::execute); this is the pipelined form of it. */
 int gpudb_query_enqueue(gpudb_ctx* ctx, gpudb_query* q);
+/* Collect the result the last execution of `q` left in the context's
+ * buffers (after gpudb_ctx_sync for enqueued runs), without executing:
+ * e.g. the answer of the last of many back-to-back graph replays
+ * (reference: MetalGenericExecutor::collectResult,
+ * metal_generic_executor.h:110). The buffers must not have been reused by
+ * another query since. */
+int gpudb_query_collect(gpudb_ctx* ctx, gpudb_query* q, gpudb_result** result);
 /* Wait for everything enqueued on the context's stream; *device_error
  * (may be NULL) receives the accumulated device error bits, which are
  * then cleared. Returns GPUDB_E_DEVICE when any bit was set. */

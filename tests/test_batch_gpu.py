@@ -232,7 +232,7 @@ def test_learned_sizer_gain(ctx, tables):
 def test_device_generators_match_host():
     import torch
     from gpudbmetalcodegen_b200 import _lib
-    lib = _lib.load()
+    lib = _lib.load_datagen()
     for s, row0, n in ((0.8, 0, 100_000), (1.3, 123_456_789, 77_777)):
         host = W.gen_mix(n, nranks=1 << 20, s=s, dim_rows=5000, seed=9, row0=row0)
         dev = {c: torch.empty(n, dtype={np.int32: torch.int32, np.int64: torch.int64}[dt], device="cuda")

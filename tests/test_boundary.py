@@ -9,14 +9,20 @@ import pytest
 ROOT = Path(__file__).resolve().parent.parent
 
 
-def declared_symbols():
+def declared_symbols(headers=None):
     names = set()
     for h in (ROOT / "include").glob("*.h"):
+        if headers is not None and h.name not in headers:
+            continue
         text = h.read_text()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"\b(gpudb_[a-z0-9_]+)\s*\(", text):
             names.add(m.group(1))
     return sorted(names)
+
+
+def engine_symbols():
+    return [s for s in declared_symbols() if s not in set(declared_symbols({"gpudb_datagen.h"}))]
 
 
 def test_headers_declare_entry_points():
@@ -28,13 +34,20 @@ def test_headers_declare_entry_points():
 def test_library_exports_every_declared_symbol():
     from gpudbmetalcodegen_b200 import _lib
     lib = _lib.load()
-    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    missing = [s for s in engine_symbols() if not hasattr(lib, s)]
     assert not missing, missing
+    # the data generators live in their own library, which maps no engine code
+    dg = _lib.load_datagen()
+    missing = [s for s in declared_symbols({"gpudb_datagen.h"}) if not hasattr(dg, s)]
+    assert not missing, missing
+    assert not hasattr(dg, "gpudb_create") and not hasattr(dg, "gpudb_query_run")
+    assert not [s for s in declared_symbols({"gpudb_datagen.h"}) if hasattr(lib, s)]
 
 
 def test_python_bindings_cover_every_declared_symbol():
     from gpudbmetalcodegen_b200 import _lib
-    assert set(declared_symbols()) <= set(_lib.EXPORTED)
+    assert set(engine_symbols()) <= set(_lib.EXPORTED)
+    assert set(declared_symbols({"gpudb_datagen.h"})) <= set(_lib.DATAGEN_EXPORTED)
 
 
 def test_no_gpu_create_fails_cleanly():

@@ -12,6 +12,9 @@ SPECS = [
     "template=groupby", "template=hashjoin", "template=colmax;table=dim;col=b_key",
     "template=distinct;card=1000;thr=5000", "template=mix_agg;thr=5000", "template=mix_groupby;card=1000",
     "template=mix_topk;card=1000;k=5", "template=mix_join;attr_lt=300",
+    "template=distinct;params=1;key=m_rank_z", "template=mix_agg;params=1", "template=mix_join;params=1",
+    "template=mix_groupby;params=1;compact=1", "template=mix_topk;params=1;k=10", "template=join_direct",
+    "template=anti_join", "template=histogram", "template=q6_selvec",
 ]
 TUNES = ["", "bs=256;scan=direct", "bs=512;scan=tma;tile=2048;stages=3", "bs=1024;scan=tma;tile=1024;stages=2",
          "layout=bucket8;smem=11", "keyed=2", "keyed=3;warp=0"]
@@ -129,3 +132,13 @@ def test_compare_canonical_semantics():
     assert "row count" in engine.compare_canonical(a, "k,v\n1,10.0\n")
     assert engine.compare_canonical(a, "k,v\n1,11.0\n2,20.0\n").startswith("row 1")
     assert engine.compare_canonical("x,k,v\nq,1,10\n", "k,v\n1,10\n") == ""  # shared columns only
+
+
+def test_launch_bound_constants_are_not_compiled_in():
+    """params=1: one module per template whatever the constants; the
+    constants are kernel arguments bound from symbols at launch."""
+    q = engine.Query("template=mix_groupby;params=1;compact=1;key=m_rank_z")
+    assert "mix_thr" in q.source and "gpudb_mod_i32(m_rank_z[i], _mix_div)" in q.source
+    assert "ConstantScalar long long mix_card  [mix_card]" in q.plan
+    with pytest.raises(GpudbError):
+        engine.Query("template=mix_agg;params=1;thr=5")  # a constant and params=1 at once

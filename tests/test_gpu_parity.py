@@ -355,3 +355,21 @@ def test_autotuner_never_changes_an_answer(ctx, tmp_path):
     assert cache.get("q1", ctx.largest_table_rows()) == tune
     ctx._tune_cache = cache
     assert ctx.prepare("template=q1", "auto").tune == tune
+
+
+def test_collect_reads_the_last_graphed_replay(ctx):
+    """Back-to-back graph replays enqueued without a host wait, then the
+    result the last one left in the buffers is collected without running
+    the plan again, and equals the oracle's (what the benchmark checks after
+    its timed steps)."""
+    d, p = load_join(ctx, 100_000, 400_000, seed=17)
+    q = ctx.prepare("template=join_topk", "")
+    ctx.set_use_graphs(True)
+    try:
+        for _ in range(6):
+            ctx.enqueue(q)
+        ctx.sync()
+        res = ctx.collect(q)
+    finally:
+        ctx.set_use_graphs(False)
+    assert res.rows == O.join_topk(d, p, k=10)[0]
