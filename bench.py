@@ -240,9 +240,12 @@ class FactScan(Workload):
         self.which = which
         self.n = args.fact_rows
         self.spec = f"template={which}"
-        self.kernel = "Q1_reduce" if which == "q1" else "Q6_reduce"
-        self.description = (f"{which}: scan-filter-group-aggregate over {self.n} rows x 38 B" if which == "q1"
-                            else f"{which}: scan-filter-sum over {self.n} rows x 28 B")
+        self.kernel = {"q1": "Q1_reduce", "q6": "Q6_reduce", "q6_selvec": "Q6S_select"}[which]
+        self.description = {
+            "q1": f"q1: scan-filter-group-aggregate over {self.n} rows x 38 B",
+            "q6": f"q6: scan-filter-sum over {self.n} rows x 28 B",
+            "q6_selvec": f"q6_selvec: the q6 predicate into a selection bitmap (20 B/row), then the sum over the "
+                         f"selected rows of {self.n}"}[which]
 
     def generate(self):
         from gpudbmetalcodegen_b200 import workloads as W
@@ -254,20 +257,24 @@ class FactScan(Workload):
     def expected(self):
         from oracle import oracle_py as O
         f = self.tables["fact"]
-        if self.which == "q6":
+        if self.which != "q1":
             return [(O.q6(f),)]
         return O.q1(f)
 
     def matches(self, res):
         exp = self.expected()
-        if self.which == "q6":
+        if self.which != "q1":
             return res.rows == exp
         got = res.as_dicts()
         from oracle import oracle_py as O
         return len(got) == len(exp) and all(g[k] == e[k] for g, e in zip(got, exp) for k in O.Q1_AGGS)
 
     def algorithmic_bytes(self, tune):
-        return {"algorithmic_bytes": self.n * (38 if self.which == "q1" else 28)}
+        # every referenced column once at its declared width; the selection
+        # bitmap plan's dominant (first) kernel reads the predicate's three
+        # columns, 20 B/row
+        per_row = {"q1": 38, "q6": 28, "q6_selvec": 20}[self.which]
+        return {"algorithmic_bytes": self.n * per_row, "query_bytes": self.n * (38 if self.which == "q1" else 28)}
 
     def cpu_run(self, threads):
         from oracle import oracle_py as O
@@ -320,7 +327,7 @@ class Skew(Workload):
 def make_workload(args) -> Workload:
     if args.workload == "join_topk":
         return JoinTopK(args)
-    if args.workload in ("q1", "q6"):
+    if args.workload in ("q1", "q6", "q6_selvec"):
         return FactScan(args, args.workload)
     if args.workload in ("groupby", "hashjoin"):
         return Skew(args, args.workload)
@@ -339,6 +346,14 @@ def time_cpu(w: Workload, budget_s: float = 12.0, max_runs: int = 20):
     return statistics.median(times), threads, len(times)
 
 
+def workload_config(w: Workload, world: int) -> dict:
+    """The `config` object of both arms' lines: the workload and its sizes,
+    how L2 is kept out of the timing, and the replica count."""
+    cfg = w.config()
+    cfg.update({"l2": "inputs larger than the 126 MB L2; no flush", "parallelism": f"replicas x{world}"})
+    return cfg
+
+
 def run_reference(args, w: Workload):
     """The reference's operator semantics restated on the CPU (the oracle
     port: the reference's own kernels are Metal and cannot run here), on all
@@ -349,7 +364,7 @@ def run_reference(args, w: Workload):
     line = {"metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": n,
             "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": w.description},
+            "config": workload_config(w, args.gpus),
             "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
                              "sample": f"full workload ({w.rows()} rows) per step, {n} steps, median"},
             "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -390,7 +405,38 @@ def mixed_oracle_seconds(args, queries, budget_s: float, dim_rows=None, zipf=Non
     return done, spent, threads
 
 
-def run_mixed(args):
+def mixed_oracle_check(tables, queries, results, n: int = 24) -> dict:
+    """The oracle (the reference's operator semantics on the CPU) on a
+    seeded subset of the batch that holds every template: each query's
+    slice is regenerated on the host from the table's seed and compared
+    with the engine's answer bit for bit."""
+    import numpy as np
+    from gpudbmetalcodegen_b200 import batch as B, workloads as W
+    from oracle import oracle_py as O
+    rng = np.random.default_rng(2024)
+    pick = set(int(i) for i in rng.choice(len(queries), min(n, len(queries)), replace=False))
+    for t in B.TEMPLATES:
+        pick.update([i for i, q in enumerate(queries) if q.tmpl == t][:1])
+    md = W.gen_mixdim(tables.dim_rows, seed=tables.seed)
+    bad, t0 = [], time.perf_counter()
+    for i in sorted(pick):
+        q = queries[i]
+        m = W.gen_mix(q.rows, nranks=tables.nranks, s=tables.zipf_s[q.table], dim_rows=tables.dim_rows,
+                      seed=tables.table_seed(q.table), row0=q.row0)
+        if q.tmpl == "agg":
+            e = ("scalar",) + tuple(O.mix_agg(m, q.thr))
+        elif q.tmpl == "join":
+            e = ("scalar",) + tuple(O.mix_join(md, m, q.attr_lt, q.thr))
+        else:
+            k, c, sm = O.mix_groupby(m, q.key, q.thr, q.card)
+            e = B.canonical_groups(k, c, sm) if q.tmpl == "groupby" else ("topk", tuple(O.topk(k, sm, q.k)))
+        if not B.same_result(results[i], e):
+            bad.append(i)
+    return {"queries": len(pick), "templates": sorted({queries[i].tmpl for i in pick}), "mismatches": bad,
+            "ok": not bad, "host_s": time.perf_counter() - t0}
+
+
+def run_mixed(args, pg=None):
     """Config: 256 seeded mixed queries over slices (1M-120M rows) of four
     resident 120M-row mix tables. One step = the whole batch through the
     batched, learned-sizing path (4096-row sample features, MLP prediction,
@@ -407,7 +453,7 @@ def run_mixed(args):
             qs = W.gen_mixed_queries(args.mix_queries, seed=W.SEED, table_rows=args.mix_rows)
             done, spent, threads = mixed_oracle_seconds(args, qs, budget_s=max(10.0, 2.0 * args.steps))
             v = done / spent
-            print(json.dumps({
+            return ({
                 "metric": "mixed_queries_per_s", "value": v, "unit": "queries/s", "n_gpus": args.gpus,
                 "steps": 1, "warmup": 0, "ms_per_step": 1e3 * spent / done * args.mix_queries,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
@@ -415,13 +461,14 @@ def run_mixed(args):
                 "config": {"workload": f"mixed: {args.mix_queries} queries over slices of 120M-row tables"},
                 "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
                                  "sample": f"first {done} of the {args.mix_queries} queries"},
-                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
-                flush=True)
-        return
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return None
 
     torch.cuda.set_device(local)
     from gpudbmetalcodegen_b200 import replicas
-    pg = replicas.init("nccl", 300)
+    own_pg = pg is None
+    if own_pg:
+        pg = replicas.init("nccl", 300)
 
     t0 = time.perf_counter()
     tables = B.MixTables(rows=args.mix_rows, zipf_s=W.MIX_ZIPF_S, nranks=W.MIX_NRANKS,
@@ -487,6 +534,9 @@ def run_mixed(args):
         replicas.barrier(pg)
     verified = all(B.same_result(a, b) for a, b in zip(res, plain_res)) and \
         all(B.same_result(a, b) for a, b in zip(exact_res, plain_res))
+    # a seeded subset (every template) against the oracle, on slices
+    # regenerated on the host from the tables' seeds
+    oracle_check = mixed_oracle_check(tables, queries, res, n=24) if rank == 0 else None
 
     # per-kernel device times (one execute without a graph) for the roofline
     learned.batch.execute(use_graph=False)
@@ -522,7 +572,7 @@ def run_mixed(args):
                            "algorithmic_bytes_per_step": alg_bytes, "table_gen_s": gen_s,
                            "l2": "inputs larger than the 126 MB L2; no flush",
                            "parallelism": f"replicas x{world}"},
-                "verified": verified,
+                "verified": verified, "verified_vs_oracle": oracle_check,
                 "plain_per_query": {"queries_per_s": len(queries) / plain_s, "ms_per_batch": plain_s * 1e3,
                                     "count_passes": plain.count_passes},
                 "batched_exact": {"queries_per_s": len(queries) / exact_s, "ms_per_batch": exact_s * 1e3,
@@ -544,15 +594,15 @@ def run_mixed(args):
                         "note": "wall clock through BatchRunner.run; tables resident in HBM by the workload's "
                                 "definition, per-step inputs are the query descriptors"},
                 "gpu_launches": launches, "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
     learned.close()
     sizer.close()
     ctx.close()
-    if pg:
+    if own_pg and pg:
         replicas.shutdown(pg)
+    return line if rank == 0 else None
 
 
-def run_serve(args):
+def run_serve(args, pg=None):
     """Config: a 120M-row table and a 30M-row dimension resident in HBM;
     mixed queries (the mixed generator, slices of 1M-120M rows) arriving as
     a Poisson process at each offered rate; the continuous-batching server
@@ -570,16 +620,15 @@ def run_serve(args):
             done, spent, threads = mixed_oracle_seconds(args, qs, budget_s=max(10.0, 2.0 * args.steps),
                                                         dim_rows=args.serve_dim_rows, zipf=(W.ZIPF_S,))
             v = done / spent
-            print(json.dumps({
+            return ({
                 "metric": "serve_queries_per_s", "value": v, "unit": "queries/s", "n_gpus": args.gpus, "steps": 1,
                 "warmup": 0, "ms_per_step": 1e3 * spent / done, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
                 "config": {"workload": "serve: mixed queries over a resident 120M-row table, one at a time"},
                 "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
                                  "sample": f"first {done} queries of the trace"},
-                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
-                flush=True)
-        return
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return None
     torch.cuda.set_device(local)
     tables = B.MixTables(rows=args.serve_rows, zipf_s=(W.ZIPF_S,), nranks=W.MIX_NRANKS,
                          dim_rows=args.serve_dim_rows, seed=W.SEED + 5)
@@ -609,6 +658,10 @@ def run_serve(args):
     ex = B.BatchRunner(tables, sizing="exact", plain=plain)
     exact_res, _ = ex.run(qs)
     exact_fp = [B.result_fingerprint(r) for r in exact_res]
+    # the exact batch itself against the oracle on a seeded subset (slices
+    # regenerated on the host): the served answers are then checked
+    # against it, every one of them
+    oracle_check = mixed_oracle_check(tables, qs, exact_res, n=16) if rank == 0 else None
     del exact_res
     ex.close()
     srv = S.Server(tables, sizer, plain=plain, workers=args.serve_workers, hbm_budget=150e9)
@@ -644,7 +697,7 @@ def run_serve(args):
                                        f"{args.serve_rows}-row table + {args.serve_dim_rows}-row dimension, Poisson "
                                        f"arrivals, HBM budget 150 GB, {args.serve_workers} workers",
                            "rates": rates, "parallelism": "replicas x1"},
-                "verified": verified, "per_rate": per_rate,
+                "verified": verified, "verified_vs_oracle": oracle_check, "per_rate": per_rate,
                 "plain_service_ms": {"warm_mean": float(service.mean() * 1e3),
                                      "warm_p50": float(np.median(service) * 1e3),
                                      "first_run_with_compile_mean": float(np.mean(compile_s) * 1e3),
@@ -654,9 +707,9 @@ def run_serve(args):
                         "d2h_bytes_per_step": None,
                         "note": "wall clock from first arrival to last answer on the host, at the highest offered rate"},
                 "gpu_launches": launches, "clocks": clocks}
-        print(json.dumps(line), flush=True)
     sizer.close()
     ctx.close()
+    return line if rank == 0 else None
 
 
 def run_aggmodes(args):
@@ -667,17 +720,18 @@ def run_aggmodes(args):
     world, rank, local = dist_info()
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "a measurement of the engine's own aggregation strategies only"}))
-        return
+            return {"impl": "reference", "unavailable": "a measurement of the engine's own aggregation strategies only"}
+        return None
     torch.cuda.set_device(local)
     rows = args.zprobe_rows // 2
     tables = B.MixTables(rows=rows, zipf_s=(W.ZIPF_S,), nranks=W.MIX_NRANKS, dim_rows=1_000_000, seed=W.SEED)
     table = autotune.measure_agg_modes(tables, rows)
     if rank == 0:
-        print(json.dumps({"metric": "group_stage_ms_per_strategy", "value": None, "unit": "ms", "n_gpus": 1,
+        return ({"metric": "group_stage_ms_per_strategy", "value": None, "unit": "ms", "n_gpus": 1,
                           "steps": 3, "warmup": 1, "higher_is_better": False, "dtype": "int64",
                           "data": "synthetic (seeded)", "config": {"workload": f"aggmodes: {rows} rows, thr 5000"},
-                          "table": table}), flush=True)
+                          "table": table})
+    return None
 
 
 def load_traffic(kernel: str):
@@ -690,61 +744,16 @@ def load_traffic(kernel: str):
     return None
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="join_topk",
-                    choices=["join_topk", "q1", "q6", "groupby", "hashjoin", "mixed", "serve", "aggmodes"])
-    ap.add_argument("--tune", default="auto", help='tuning string, "" for the defaults, or "auto"')
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-verify", action="store_true")
-    ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
-    ap.add_argument("--build-rows", type=int, default=15_000_000)
-    ap.add_argument("--probe-rows", type=int, default=60_000_000)
-    ap.add_argument("--fact-rows", type=int, default=6_001_215)
-    ap.add_argument("--zprobe-rows", type=int, default=120_000_000)
-    ap.add_argument("--zkeys", type=int, default=1 << 22)
-    ap.add_argument("--mix-rows", type=int, default=120_000_000)
-    ap.add_argument("--mix-dim-rows", type=int, default=1_000_000)
-    ap.add_argument("--mix-queries", type=int, default=256)
-    ap.add_argument("--train-executions", type=int, default=200_000)
-    ap.add_argument("--sizer-epochs", type=int, default=30)
-    ap.add_argument("--plain-passes", type=int, default=1)
-    ap.add_argument("--serve-rows", type=int, default=120_000_000)
-    ap.add_argument("--serve-dim-rows", type=int, default=30_000_000)
-    ap.add_argument("--serve-queries", type=int, default=1000)
-    ap.add_argument("--serve-rates", default="500,2000,8000")
-    ap.add_argument("--serve-workers", type=int, default=2)
-    ap.add_argument("--serve-plain-queries", type=int, default=200)
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-    if args.workload == "mixed":
-        return run_mixed(args)
-    if args.workload == "serve":
-        return run_serve(args)
-    if args.workload == "aggmodes":
-        return run_aggmodes(args)
-    world, rank, local = dist_info()
-    w = make_workload(args)
-
-    if args.impl == "reference":
-        if rank == 0:
-            run_reference(args, w)
-        return
-
+def measure(args, w: Workload, pg, world: int, rank: int, local: int):
+    """One workload through the engine on this rank's GPU: verified first
+    run, timed back-to-back graph replays (max over ranks), per-kernel
+    times, roofline, end to end from pinned host buffers, and the CPU
+    baseline on rank 0. Returns rank 0's JSON line (None elsewhere)."""
     import ctypes as C
     import numpy as np
     import torch
 
-    torch.cuda.set_device(local)
-    from gpudbmetalcodegen_b200 import replicas
-    pg = replicas.init("nccl", 120)
-
-    from gpudbmetalcodegen_b200 import Context, _lib
+    from gpudbmetalcodegen_b200 import Context, _lib, replicas
 
     w.generate()
     ctx = Context(local)
@@ -759,10 +768,15 @@ def main():
         tpl = dict(kv.split("=", 1) for kv in w.spec.split(";")).get("template")
         rows = ctx.largest_table_rows()
         if cache.get(tpl, rows) is None:
+            # no stored choice for this device: the default and the seed
+            # tunings are measured (answers checked against the first run),
+            # the fastest is stored; the full coordinate descent runs with
+            # --tune search
             t0 = time.perf_counter()
             tlog = []
-            autotune.tune_query(ctx, w.spec, rows, cache=cache, log=tlog)
-            tuner = {"tuned_s": time.perf_counter() - t0, "candidates": len(tlog) + 1}
+            autotune.tune_query(ctx, w.spec, rows, cache=cache, log=tlog, rounds=0 if not args.tune_search else 2)
+            tuner = {"tuned_s": time.perf_counter() - t0, "candidates": len(tlog) + 1,
+                     "mode": "search" if args.tune_search else "seeds"}
         e = cache.data.get(cache.key(tpl, rows), {})
         tuner = {**(tuner or {}), "chosen": e.get("tune"), "tuned_ms": e.get("ms"), "default_ms": e.get("default_ms")}
         tune = ctx.resolve_tune(w.spec, "auto")
@@ -798,6 +812,8 @@ def main():
         ev1.synchronize()
     ctx.sync()
     torch.cuda.synchronize()
+    # the answer the last timed replay left in the buffers, against the oracle
+    verified_timed = None if args.no_verify else w.matches(ctx.collect(q))
     launches = len(kernels) * args.steps
     step_ms = ev0.elapsed_time(ev1) / args.steps
     ctx.set_use_graphs(False)
@@ -889,19 +905,142 @@ def main():
         cpu = {"value": w.rows() / step, "unit": "rows/s", "cores": threads, "kind": "port",
                "sample": f"full workload ({w.rows()} rows) x {n} runs, median"}
 
+    line = None
     if rank == 0:
-        cfg = w.config()
-        cfg.update({"l2": "inputs larger than the 126 MB L2; no flush", "tune": q.tune or "default",
-                    "parallelism": f"replicas x{world}", "cuda_graphs": not args.no_graphs})
-        if tuner:
-            cfg["autotune"] = tuner
         line = {"metric": "rows_per_s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "config": cfg,
-                "verified": verified, "phase_ms": phase_ms, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+                "config": workload_config(w, world),
+                "execution": {"tune": q.tune or "default", "autotune": tuner, "cuda_graphs": not args.no_graphs,
+                              "steps_enqueued_back_to_back": True},
+                "verified": verified, "verified_last_timed_step": verified_timed, "phase_ms": phase_ms,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
     ctx.close()
+    return line
+
+
+def sub_args(args, **over):
+    a = argparse.Namespace(**vars(args))
+    for k, v in over.items():
+        setattr(a, k, v)
+    return a
+
+
+def run_extras(args, pg, world, rank, local) -> dict:
+    """The rest of the benchmark set's metric beside the headline join:
+    the plain scan-filter-aggregate (config 0: q1, and the predicate
+    variant q6) with their rooflines and CPU baselines, the batched mixed
+    form (config 3: learned / exact / plain queries per second, checked
+    against the oracle), and serving (config 4: p50 / p99 at two offered
+    rates). Each part reports its own wall time and, if it fails, why."""
+    import torch
+    out = {}
+    for which in ("q1", "q6"):
+        t0 = time.perf_counter()
+        try:
+            a = sub_args(args, workload=which, steps=max(args.steps, 30))
+            line = measure(a, make_workload(a), pg, world, rank, local)
+            if line:
+                out[which] = {k: line[k] for k in ("value", "unit", "ms_per_step", "config", "execution", "verified",
+                                                   "verified_last_timed_step", "phase_ms", "roofline", "cpu_baseline",
+                                                   "e2e", "gpu_launches", "clocks")}
+                out[which]["metric"] = "rows_per_s"
+                out[which]["wall_s"] = time.perf_counter() - t0
+        except Exception as e:  # a failed part is reported, the headline stands
+            out[which] = {"error": f"{type(e).__name__}: {e}"[:500]}
+        torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    try:
+        line = run_mixed(sub_args(args, workload="mixed", steps=5, train_executions=args.extras_train_executions,
+                                  sizer_epochs=args.extras_sizer_epochs, no_cpu_baseline=True), pg=pg)
+        if line:
+            line["wall_s"] = time.perf_counter() - t0
+            out["mixed"] = line
+    except Exception as e:
+        out["mixed"] = {"error": f"{type(e).__name__}: {e}"[:500]}
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    try:
+        line = run_serve(sub_args(args, workload="serve", train_executions=args.extras_train_executions,
+                                  sizer_epochs=args.extras_sizer_epochs, serve_queries=args.extras_serve_queries,
+                                  serve_rates="500,2000", serve_plain_queries=100), pg=pg)
+        if line:
+            line["wall_s"] = time.perf_counter() - t0
+            out["serve"] = line
+    except Exception as e:
+        out["serve"] = {"error": f"{type(e).__name__}: {e}"[:500]}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="join_topk",
+                    choices=["join_topk", "q1", "q6", "q6_selvec", "groupby", "hashjoin", "mixed", "serve",
+                             "aggmodes"])
+    ap.add_argument("--tune", default="auto", help='tuning string, "" for the defaults, "auto" (stored or seed '
+                                                   'tunings) or "search" (the full autotuner search)')
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="the headline join only (no q1 / q6 / mixed / serve objects on the line)")
+    ap.add_argument("--build-rows", type=int, default=15_000_000)
+    ap.add_argument("--probe-rows", type=int, default=60_000_000)
+    ap.add_argument("--fact-rows", type=int, default=6_001_215)
+    ap.add_argument("--zprobe-rows", type=int, default=120_000_000)
+    ap.add_argument("--zkeys", type=int, default=1 << 22)
+    ap.add_argument("--mix-rows", type=int, default=120_000_000)
+    ap.add_argument("--mix-dim-rows", type=int, default=1_000_000)
+    ap.add_argument("--mix-queries", type=int, default=256)
+    ap.add_argument("--train-executions", type=int, default=200_000)
+    ap.add_argument("--sizer-epochs", type=int, default=30)
+    ap.add_argument("--extras-train-executions", type=int, default=200_000)
+    ap.add_argument("--extras-sizer-epochs", type=int, default=30)
+    ap.add_argument("--extras-serve-queries", type=int, default=600)
+    ap.add_argument("--plain-passes", type=int, default=1)
+    ap.add_argument("--serve-rows", type=int, default=120_000_000)
+    ap.add_argument("--serve-dim-rows", type=int, default=30_000_000)
+    ap.add_argument("--serve-queries", type=int, default=1000)
+    ap.add_argument("--serve-rates", default="500,2000,8000")
+    ap.add_argument("--serve-workers", type=int, default=2)
+    ap.add_argument("--serve-plain-queries", type=int, default=200)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    args.tune_search = args.tune == "search"
+    if args.tune_search:
+        args.tune = "auto"
+    if args.workload in ("mixed", "serve", "aggmodes"):
+        line = {"mixed": run_mixed, "serve": run_serve, "aggmodes": run_aggmodes}[args.workload](args)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+    world, rank, local = dist_info()
+    w = make_workload(args)
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, w)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from gpudbmetalcodegen_b200 import replicas
+    pg = replicas.init("nccl", 120)
+    line = measure(args, w, pg, world, rank, local)
+    # the rest of the metric rides on the headline line of a one-GPU run
+    # (under torchrun every rank would have to take the same steps)
+    if args.workload == "join_topk" and not args.no_extras and world == 1:
+        extras = run_extras(args, pg, world, rank, local)
+        if line is not None:
+            line.update(extras)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     if pg:
         replicas.shutdown(pg)
 

@@ -202,6 +202,12 @@ _DATAGEN_SIGNATURES = [
      + [C.c_void_p] * 6),
     ("gpudb_gen_mixdim_device", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gpudb_datagen_last_error", C.c_char_p, []),
+    ("gpudb_gen_snow_cust", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_snow_supp", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gpudb_gen_snow_orders", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_int]),
+    ("gpudb_gen_snow_lines", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
 ]
 
 EXPORTED = [s[0] for s in _SIGNATURES]

@@ -676,9 +676,9 @@ class PlainRunner:
 
     def exact_groups(self, q: MixQuery) -> int:
         self._register_slice(q)
-        res, _ = self.ctx.run(self._query(f"template=distinct;params=1;key={q.key}"))
+        res, _ = self.ctx.run(self._query(f"template=distinct;params=1;key={q.key}"), arrays=True)
         self.count_passes += 1
-        return int(res.rows[0][0])
+        return int(res["distinct"][0])
 
     def run(self, q: MixQuery) -> tuple:
         with self._lock:
@@ -692,13 +692,15 @@ class PlainRunner:
             self.ctx.register_symbol("mix_groups", max(1, groups))
             spec += f";key={q.key}"
             spec += f";k={q.k}" if q.tmpl == "topk" else ";compact=1"
-        res, _ = self.ctx.run(self._query(spec))
         if q.tmpl in ("agg", "join"):
+            # an exact 128-bit sum: the (small) row form keeps its high word
+            res, _ = self.ctx.run(self._query(spec))
             c, s = res.rows[0]
             return ("scalar", int(c), int(s))
+        res, _ = self.ctx.run(self._query(spec), arrays=True)
         if q.tmpl == "groupby":
-            return canonical_groups(res.column("key"), res.column("count"), res.column("sum"))
-        return ("topk", tuple((int(k), int(v)) for k, v in res.rows))
+            return canonical_groups(res["key"], res["count"], res["sum"])
+        return ("topk", tuple((int(k), int(v)) for k, v in zip(res["key"], res["sum"])))
 
 
 @dataclass

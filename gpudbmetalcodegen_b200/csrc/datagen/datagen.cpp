@@ -228,4 +228,61 @@ int gpudb_gen_mixdim(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int
     return 0;
 }
 
+
+// ---- the snowflake of the multi-join (Q5-shape) plan ----------------------
+int gpudb_gen_snow_cust(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* nation, int threads) {
+    if (n && (!key || !nation)) return -1;
+    parallelFor(n, threads, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; i++) {
+            const uint64_t r = row0 + i;
+            key[i] = (int32_t)(r + 1);
+            nation[i] = (int32_t)uni(rnd(seed, S_CNAT, r), 0, 24);
+        }
+    });
+    return 0;
+}
+
+int gpudb_gen_snow_supp(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* nation, int threads) {
+    if (n && (!key || !nation)) return -1;
+    parallelFor(n, threads, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; i++) {
+            const uint64_t r = row0 + i;
+            key[i] = (int32_t)(r + 1);
+            nation[i] = (int32_t)uni(rnd(seed, S_SNAT, r), 0, 24);
+        }
+    });
+    return 0;
+}
+
+int gpudb_gen_snow_orders(uint64_t seed, uint64_t ncust, uint64_t row0, uint64_t n, int32_t* key, int32_t* cust,
+                          int32_t* day, int threads) {
+    if ((n && (!key || !cust || !day)) || ncust == 0 || ncust > 0x7FFFFFFFull) return -1;
+    parallelFor(n, threads, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; i++) {
+            const uint64_t r = row0 + i;
+            key[i] = (int32_t)(r + 1);
+            cust[i] = (int32_t)uni(rnd(seed, S_OCUST, r), 1, (int64_t)ncust);
+            day[i] = (int32_t)uni(rnd(seed, S_ODAY2, r), 0, 2405);
+        }
+    });
+    return 0;
+}
+
+int gpudb_gen_snow_lines(uint64_t seed, uint64_t norders, uint64_t nsupp, uint64_t row0, uint64_t n, int32_t* okey,
+                         int32_t* supp, int64_t* price, int64_t* discount, int threads) {
+    if ((n && (!okey || !supp || !price || !discount)) || norders == 0 || nsupp == 0 || norders > 0x7FFFFFFFull ||
+        nsupp > 0x7FFFFFFFull)
+        return -1;
+    parallelFor(n, threads, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; i++) {
+            const uint64_t r = row0 + i;
+            okey[i] = (int32_t)uni(rnd(seed, S_LOKEY, r), 1, (int64_t)norders);
+            supp[i] = (int32_t)uni(rnd(seed, S_LSUPP, r), 1, (int64_t)nsupp);
+            price[i] = uni(rnd(seed, S_LPRICE, r), 90000, 10500000);
+            discount[i] = uni(rnd(seed, S_LDISC, r), 0, 10);
+        }
+    });
+    return 0;
+}
+
 }  // extern "C"

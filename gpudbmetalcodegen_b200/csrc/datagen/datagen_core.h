@@ -35,7 +35,8 @@ enum : uint64_t {
     S_SHIP = 1, S_QTY, S_PRICE, S_DISC, S_TAX, S_FLAG_A, S_RECV,
     S_PERM, S_ODAY, S_SEG, S_FK, S_SHIPD, S_PPRICE, S_PDISC,
     S_ZKEY, S_ZPAY, S_ZRANK, S_ZVAL,
-    S_MRU, S_MRZ, S_MF, S_MV, S_MFK, S_MDA
+    S_MRU, S_MRZ, S_MF, S_MV, S_MFK, S_MDA,
+    S_CNAT, S_SNAT, S_OCUST, S_ODAY2, S_LOKEY, S_LSUPP, S_LPRICE, S_LDISC
 };
 
 // Inverse CDF by binary search: the first rank whose CDF exceeds u.

@@ -43,6 +43,13 @@ std::vector<TableDef> buildCatalog() {
           {"m_fk", "int"}}},
         // Mixed-workload dimension (join-agg build side).
         {"mixdim", {{"md_key", "int"}, {"md_attr", "int"}}},
+        // The multi-join snowflake (the reference's Q5 shape): nation ->
+        // customer / supplier -> orders -> lines.
+        {"nation", {{"n_key", "int"}, {"n_region", "int"}}},
+        {"cust", {{"c_key", "int"}, {"c_nation", "int"}}},
+        {"supp", {{"s_key", "int"}, {"s_nation", "int"}}},
+        {"ord", {{"o_key", "int"}, {"o_cust", "int"}, {"o_day", "int"}}},
+        {"line", {{"l_okey", "int"}, {"l_supp", "int"}, {"l_price", "long long", 2}, {"l_discount", "long long", 2}}},
     };
 }
 
@@ -591,6 +598,67 @@ CudaQueryPlan buildQ6SelVec(Spec& s, const TuneConfig& tune) {
     return plan;
 }
 
+// ---- multi_join: the reference's Q5 plan shape (metal_plan_builder.cpp:
+// 894-1015), five phases over the snowflake: a bitmap of the region's
+// nations; customer and supplier nation maps of those nations (BitmapProbe
+// -> ArrayStore); the date-filtered orders' customer nation (ArrayLookup ->
+// ArrayStore); then every line looks up its order's and its supplier's
+// nation, keeps the lines whose two nations agree (Selection) and adds its
+// revenue per nation (AtomicAgg, 25 bins).
+CudaQueryPlan buildMultiJoin(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "MULTI_JOIN";
+    const long long region = s.num("region", 2), dayGe = s.num("day_ge", 730), dayLt = s.num("day_lt", 1095);
+    {
+        auto scan = makeScan(plan, "nation", {"n_key", "n_region"}, tune, false);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "n_region[i] == " + std::to_string(region));
+        auto bm = std::make_unique<CudaBitmapBuild>(std::move(f), "mj_nations", "n_key[i]", "1");
+        auto& ph = appendPhase(plan, "MJ_nations", std::move(bm), tune);
+        ph.threadgroupSize = 32;
+    }
+    {
+        auto scan = makeScan(plan, "cust", {"c_key", "c_nation"}, tune);
+        auto pr = std::make_unique<CudaBitmapProbe>(std::move(scan), "mj_nations", "c_nation[i]");
+        auto st = std::make_unique<CudaArrayStore>(std::move(pr), "mj_cust_nation", "c_key[i]", "c_nation[i]", "int",
+                                                   "max_c_key + 1");
+        appendPhase(plan, "MJ_cust", std::move(st), tune);
+    }
+    {
+        auto scan = makeScan(plan, "supp", {"s_key", "s_nation"}, tune);
+        auto pr = std::make_unique<CudaBitmapProbe>(std::move(scan), "mj_nations", "s_nation[i]");
+        auto st = std::make_unique<CudaArrayStore>(std::move(pr), "mj_supp_nation", "s_key[i]", "s_nation[i]", "int",
+                                                   "max_s_key + 1");
+        appendPhase(plan, "MJ_supp", std::move(st), tune);
+    }
+    {
+        auto scan = makeScan(plan, "ord", {"o_key", "o_cust", "o_day"}, tune);
+        auto f = std::make_unique<CudaSelection>(std::move(scan), "o_day[i] >= " + std::to_string(dayGe) +
+                                                                      " && o_day[i] < " + std::to_string(dayLt));
+        auto lk = std::make_unique<CudaArrayLookup>(std::move(f), "mj_cust_nation", "o_cust[i]", "_cn", "int", -1);
+        auto st = std::make_unique<CudaArrayStore>(std::move(lk), "mj_ord_nation", "o_key[i]", "_cn", "int",
+                                                   "max_o_key + 1");
+        appendPhase(plan, "MJ_orders", std::move(st), tune);
+    }
+    {
+        auto scan = makeScan(plan, "line", {"l_okey", "l_supp"}, tune, true, {"l_price", "l_discount"});
+        auto lo = std::make_unique<CudaArrayLookup>(std::move(scan), "mj_ord_nation", "l_okey[i]", "_cn", "int", -1);
+        auto ls = std::make_unique<CudaArrayLookup>(std::move(lo), "mj_supp_nation", "l_supp[i]", "_sn", "int", -1);
+        auto same = std::make_unique<CudaSelection>(std::move(ls), "_cn == _sn");
+        auto ag = std::make_unique<CudaAtomicAgg>(std::move(same), "mj_revenue", "_cn",
+                                                  "l_price[i] * (100ll - l_discount[i])", "25");
+        ag->setWarpAggregate(true);
+        ag->setSharedCache(5, 2);
+        appendPhase(plan, "MJ_lines", std::move(ag), tune);
+    }
+    plan.decorate.push_back([](CudaResultSchema& rs) {
+        rs.kind = CudaResultSchema::DIRECT_AGG;
+        rs.directAgg.sizeExpr = "25";
+        rs.directAgg.keyName = "nation";
+        rs.directAgg.aggs = {{"revenue", "mj_revenue"}};
+    });
+    return plan;
+}
+
 // ---- groupby: high-cardinality hash group-by, count + sum (reference
 // Q18 shape metal_plan_builder.cpp:1529-1545, which aggregates into a
 // direct-address array; here an open-addressing table keyed by int64).
@@ -824,7 +892,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
 }  // namespace
 
 std::vector<std::string> planTemplates() {
-    return {"q1", "q6", "q6_selvec", "join_topk", "join_rows", "join_direct", "anti_join", "histogram", "groupby",
+    return {"q1", "q6", "q6_selvec", "join_topk", "join_rows", "join_direct", "anti_join", "histogram", "multi_join", "groupby",
             "hashjoin", "colmax", "distinct", "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
 }
 
@@ -840,6 +908,7 @@ CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) 
     else if (tmpl == "anti_join") plan = buildAntiJoin(s, tune);
     else if (tmpl == "histogram") plan = buildHistogram(s, tune);
     else if (tmpl == "q6_selvec") plan = buildQ6SelVec(s, tune);
+    else if (tmpl == "multi_join") plan = buildMultiJoin(s, tune);
     else if (tmpl == "groupby") plan = buildGroupBy(s, tune);
     else if (tmpl == "hashjoin") plan = buildHashJoin(s, tune);
     else if (tmpl == "colmax") plan = buildColMax(s, tune);

@@ -108,6 +108,25 @@ def _result_from_c(res) -> Result:
     return Result(names, types, rows, canonical, exact)
 
 
+def _arrays_from_c(res) -> Dict[str, np.ndarray]:
+    """Integer result columns as numpy int64 arrays (one bulk export per
+    column, no per-row Python objects) — for large results."""
+    lib = _lib.load()
+    nc, nr = C.c_int(), C.c_longlong()
+    lib.gpudb_result_shape(res, C.byref(nc), C.byref(nr))
+    out = {}
+    for c in range(nc.value):
+        buf = C.create_string_buffer(256)
+        t = C.c_int()
+        lib.gpudb_result_column(res, c, buf, 256, C.byref(t))
+        if t.value != 0:
+            continue
+        a = np.zeros(nr.value, dtype=np.int64)
+        check(lib.gpudb_result_export_i64(res, c, a.ctypes.data, nr.value))
+        out[buf.value.decode()] = a
+    return out
+
+
 class Query:
     """A planned + generated (+ compiled) query."""
 
@@ -293,8 +312,9 @@ class Context:
         return q
 
     def run(self, spec_or_query, tune: str = "", warmup: int = 0, measured: int = 1,
-            collect: bool = True) -> tuple:
-        """Plan/compile (cached), size, execute, collect. Returns (Result|None, Timing)."""
+            collect: bool = True, arrays: bool = False) -> tuple:
+        """Plan/compile (cached), size, execute, collect. Returns (Result|None, Timing);
+        with arrays=True the result is a dict of int64 numpy columns instead."""
         q = spec_or_query if isinstance(spec_or_query, Query) else self.prepare(spec_or_query, tune)
         res = C.c_void_p()
         t = _lib.Timing()
@@ -308,7 +328,7 @@ class Context:
         out = None
         if collect:
             try:
-                out = _result_from_c(res)
+                out = _arrays_from_c(res) if arrays else _result_from_c(res)
             finally:
                 self._lib.gpudb_result_free(res)
         return out, timing

@@ -1,11 +1,13 @@
-"""Seeded synthetic tables for the measured workloads (numpy, via libgpudb's
-generators in include/gpudb_datagen.h) and their registration.
+"""Seeded synthetic tables for the measured workloads (numpy, via the
+generators of libgpudb_datagen.so, include/gpudb_datagen.h) and their
+registration.
 
 Workloads (sizes from the benchmark configurations this backend is measured on):
   scan_filter_groupagg  fact 6,001,215 rows x 38 B
   join_topk             dim 15M rows (key, order_day, segment) + probe 60M rows (fk, ship_day, price, discount)
   skew                  zbuild 2^22 keys + zprobe 120M rows, Zipf(1.1) keys
   mix                   mix table up to 120M rows + mixdim
+  multi_join            the snowflake nation (25) / cust / supp / ord / line (the Q5 shape)
 """
 from __future__ import annotations
 
@@ -33,6 +35,8 @@ ZPROBE_COLUMNS = {"z_key": np.int64, "z_value": np.int64}
 MIX_COLUMNS = {"m_rank_u": np.int32, "m_rank_z": np.int32, "m_filter": np.int32, "m_value": np.int64,
                "m_fk": np.int32}
 MIXDIM_COLUMNS = {"md_key": np.int32, "md_attr": np.int32}
+SNOW_CUST_ROWS, SNOW_SUPP_ROWS, SNOW_ORDER_ROWS, SNOW_LINE_ROWS = 1_500_000, 100_000, 15_000_000, 60_000_000
+LINE_COLUMNS = {"l_okey": np.int32, "l_supp": np.int32, "l_price": np.int64, "l_discount": np.int64}
 
 
 def _alloc(cols, n):
@@ -141,3 +145,23 @@ def gen_mixed_queries(n: int = MIX_QUERIES, seed: int = SEED, table_rows: int = 
         out.append(MixQuery(tmpl=tmpl, table=table, row0=row0, rows=rows, thr=thr, key=key, card=card, k=k,
                             attr_lt=attr_lt))
     return out
+
+
+def gen_snowflake(ncust: int = SNOW_CUST_ROWS, nsupp: int = SNOW_SUPP_ROWS, norders: int = SNOW_ORDER_ROWS,
+                  nlines: int = SNOW_LINE_ROWS, seed: int = SEED, threads: int = 0) -> Dict[str, Dict[str, np.ndarray]]:
+    """The multi-join snowflake: nation (key 0..24, region key % 5), cust,
+    supp, ord and line tables (include/gpudb_datagen.h)."""
+    lib = _lib.load_datagen()
+    nation = {"n_key": np.arange(25, dtype=np.int32), "n_region": (np.arange(25) % 5).astype(np.int32)}
+    cust = {"c_key": np.empty(ncust, np.int32), "c_nation": np.empty(ncust, np.int32)}
+    supp = {"s_key": np.empty(nsupp, np.int32), "s_nation": np.empty(nsupp, np.int32)}
+    ords = {"o_key": np.empty(norders, np.int32), "o_cust": np.empty(norders, np.int32),
+            "o_day": np.empty(norders, np.int32)}
+    line = _alloc(LINE_COLUMNS, nlines)
+    assert lib.gpudb_gen_snow_cust(seed, 0, ncust, _p(cust["c_key"]), _p(cust["c_nation"]), threads) == 0
+    assert lib.gpudb_gen_snow_supp(seed, 0, nsupp, _p(supp["s_key"]), _p(supp["s_nation"]), threads) == 0
+    assert lib.gpudb_gen_snow_orders(seed, ncust, 0, norders, _p(ords["o_key"]), _p(ords["o_cust"]),
+                                     _p(ords["o_day"]), threads) == 0
+    assert lib.gpudb_gen_snow_lines(seed, norders, nsupp, 0, nlines, *(_p(line[c]) for c in LINE_COLUMNS),
+                                    threads) == 0
+    return {"nation": nation, "cust": cust, "supp": supp, "ord": ords, "line": line}

@@ -67,6 +67,18 @@ int gpudb_gen_mix_device(uint64_t seed, uint64_t nranks, double s, uint64_t dim_
                          int32_t* rank_u, int32_t* rank_z, int32_t* filter, int64_t* value, int32_t* fk,
                          void* stream);
 int gpudb_gen_mixdim_device(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* attr, void* stream);
+/* The snowflake of the multi-join plan (the reference's Q5 shape:
+ * region -> nation -> customer / supplier -> orders -> lineitem). nation is
+ * 25 rows (key 0..24, region key % 5) built by the caller. cust / supp:
+ * key = row + 1, nation U[0,24]. orders: key = row + 1, cust U[1, ncust],
+ * day U[0,2405]. lines: order key U[1, norders], supplier U[1, nsupp],
+ * price / discount as the fact table. */
+int gpudb_gen_snow_cust(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* nation, int threads);
+int gpudb_gen_snow_supp(uint64_t seed, uint64_t row0, uint64_t n, int32_t* key, int32_t* nation, int threads);
+int gpudb_gen_snow_orders(uint64_t seed, uint64_t ncust, uint64_t row0, uint64_t n, int32_t* key, int32_t* cust,
+                          int32_t* day, int threads);
+int gpudb_gen_snow_lines(uint64_t seed, uint64_t norders, uint64_t nsupp, uint64_t row0, uint64_t n, int32_t* okey,
+                         int32_t* supp, int64_t* price, int64_t* discount, int threads);
 /* Text of the last device-generator failure on this thread ("" if none). */
 const char* gpudb_datagen_last_error(void);
 

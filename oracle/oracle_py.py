@@ -217,3 +217,33 @@ def histogram(dim, probe, ship_gt=1170, nbins=256, threads: int = 0) -> List[tup
     if st != 0:
         raise ValueError("histogram: a probe key beyond the build keys, or a count beyond the bins")
     return [(c, int(hist[c])) for c in range(nbins) if hist[c]]
+
+
+def multi_join(snow, region=2, day_ge=730, day_lt=1095) -> List[tuple]:
+    """The reference's Q5 plan shape (metal_plan_builder.cpp:894-1015) over
+    the snowflake: nations of `region`; customers and suppliers of those
+    nations; orders with day_ge <= day < day_lt and such a customer; lines
+    of those orders whose supplier's nation equals the customer's nation;
+    per nation the exact sum of price * (100 - discount). Rows (nation,
+    revenue) of non-zero nations in nation order. numpy, exact int64."""
+    nat = snow["nation"]
+    in_region = np.zeros(25, dtype=bool)
+    in_region[nat["n_key"][nat["n_region"] == region]] = True
+    cust, supp, ords, line = snow["cust"], snow["supp"], snow["ord"], snow["line"]
+    cn = np.full(int(cust["c_key"].max(initial=0)) + 1, -1, np.int64)
+    keep = in_region[cust["c_nation"]]
+    cn[cust["c_key"][keep]] = cust["c_nation"][keep]
+    sn = np.full(int(supp["s_key"].max(initial=0)) + 1, -1, np.int64)
+    keep = in_region[supp["s_nation"]]
+    sn[supp["s_key"][keep]] = supp["s_nation"][keep]
+    on = np.full(int(ords["o_key"].max(initial=0)) + 1, -1, np.int64)
+    dk = (ords["o_day"] >= day_ge) & (ords["o_day"] < day_lt)
+    c_of = cn[ords["o_cust"][dk]]
+    on[ords["o_key"][dk][c_of >= 0]] = c_of[c_of >= 0]
+    lc = on[line["l_okey"]]
+    ls = sn[line["l_supp"]]
+    ok = (lc >= 0) & (lc == ls)
+    rev = line["l_price"][ok] * (100 - line["l_discount"][ok])
+    sums = np.zeros(25, np.int64)
+    np.add.at(sums, lc[ok], rev)
+    return [(n, int(sums[n])) for n in range(25) if sums[n]]

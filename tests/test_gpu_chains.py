@@ -8,12 +8,16 @@ C-ABI against the CPU oracle on the same seeded tables (bit-exact):
 * histogram  — Q13's count-of-counts (AtomicCount -> ArrayLookup ->
   AtomicCount);
 * q6_selvec  — the predicate variant over a warp-built selection bitmap
-  consumed by a second phase (Selection bitmap -> SelectionScan).
+  consumed by a second phase (Selection bitmap -> SelectionScan);
+* multi_join — Q5's five-phase plan over a snowflake (nation bitmap ->
+  customer / supplier nation maps -> orders map -> lines' double lookup,
+  same-nation selection and per-nation sum).
 
 Each runs at small sizes under several tunings, twice through the same
 buffers, on edge cases (nothing qualifies, everything qualifies, ragged
-row counts), and once at the join configuration's full size (15M build +
-60M probe rows) or the fact table's (6,001,215 rows).
+row counts), and once at full size: the join configuration's tables (15M
+build + 60M probe rows), the fact table (6,001,215 rows), or a snowflake of
+1.5M customers, 100k suppliers, 15M orders and 60M lines.
 """
 import numpy as np
 import pytest
@@ -155,3 +159,36 @@ def test_q6_selection_bitmap_full_size(ctx):
     sel = (f["f_ship_day"] >= 365) & (f["f_ship_day"] < 730) & (d >= 5) & (d <= 7) & (f["f_quantity"] < 24)
     bits = ctx.read_buffer("q6_sel", np.uint32, W.FACT_ROWS // 32 + 1)
     assert np.array_equal(np.unpackbits(bits.view(np.uint8), bitorder="little")[:W.FACT_ROWS].astype(bool), sel)
+
+
+def load_snow(ctx, scale=1.0, seed=3):
+    snow = W.gen_snowflake(int(W.SNOW_CUST_ROWS * scale), int(W.SNOW_SUPP_ROWS * scale),
+                           int(W.SNOW_ORDER_ROWS * scale), int(W.SNOW_LINE_ROWS * scale), seed=seed)
+    for t, cols in snow.items():
+        ctx.upload_table(t, cols)
+    return snow
+
+
+@pytest.mark.parametrize("tune", TUNES)
+def test_multi_join_parity(ctx, tune):
+    """The reference's Q5 plan shape: five phases (nation bitmap, two
+    nation maps, the orders' map, the lines' double lookup + same-nation
+    selection + per-nation sum), against the oracle for several regions and
+    date ranges, twice through the same buffers."""
+    snow = load_snow(ctx, scale=0.02, seed=41)
+    for spec, kw in (("template=multi_join", {}), ("template=multi_join;region=0;day_ge=0;day_lt=2406",
+                                                   dict(region=0, day_ge=0, day_lt=2406)),
+                     ("template=multi_join;region=4;day_ge=1000;day_lt=1001", dict(region=4, day_ge=1000, day_lt=1001)),
+                     ("template=multi_join;region=7", dict(region=7))):  # no nation in the region: no rows
+        exp = O.multi_join(snow, **kw)
+        for _ in range(2):
+            res, t = ctx.run(spec, tune)
+            assert t.device_error == 0
+            assert res.columns == ["nation", "revenue"]
+            assert res.rows == exp
+
+
+def test_multi_join_full_size(ctx):
+    snow = load_snow(ctx, scale=1.0, seed=W.SEED)
+    res, t = ctx.run("template=multi_join")
+    assert t.device_error == 0 and res.rows == O.multi_join(snow)

@@ -219,3 +219,21 @@ def test_zipf_top_key_share():
     zb = W.gen_zbuild(1 << 16)
     assert np.unique(zb["zb_key"]).shape[0] == 1 << 16
     assert not (zb["zb_key"] == -1).any()
+
+
+def test_multi_join_known_answer():
+    """Q5 shape on a hand-built snowflake: nations 2 and 7 are region 2."""
+    nation = {"n_key": np.arange(25, dtype=np.int32), "n_region": (np.arange(25) % 5).astype(np.int32)}
+    cust = {"c_key": np.array([1, 2, 3], np.int32), "c_nation": np.array([2, 7, 3], np.int32)}
+    supp = {"s_key": np.array([1, 2, 3], np.int32), "s_nation": np.array([2, 7, 2], np.int32)}
+    ords = {"o_key": np.array([1, 2, 3, 4], np.int32), "o_cust": np.array([1, 2, 3, 1], np.int32),
+            "o_day": np.array([800, 800, 800, 5], np.int32)}
+    # order 1 (cust nation 2), 2 (nation 7), 3 (nation 3, not in the region), 4 (too early)
+    line = {"l_okey": np.array([1, 1, 2, 2, 3, 4], np.int32), "l_supp": np.array([1, 2, 2, 3, 1, 1], np.int32),
+            "l_price": np.array([100, 200, 300, 400, 500, 600], np.int64),
+            "l_discount": np.array([0, 0, 10, 0, 0, 0], np.int64)}
+    snow = {"nation": nation, "cust": cust, "supp": supp, "ord": ords, "line": line}
+    # line 0: order nation 2, supplier nation 2 -> 100 * 100; line 1: 2 vs 7 no;
+    # line 2: 7 vs 7 -> 300 * 90; line 3: 7 vs 2 no; line 4: order not kept; line 5: too early
+    assert O.multi_join(snow) == [(2, 10000), (7, 27000)]
+    assert O.multi_join(snow, region=3) == []  # nation 3 is region 3, but suppliers are not
