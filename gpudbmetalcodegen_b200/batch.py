@@ -13,8 +13,9 @@ overflows. Every path returns the same canonical results:
     topk       : ("topk", ((key, sum), ...))     best first
 
 The batched path hands group-by results over unsorted, as
-("groups_raw", rows[n, 3]) in table order (a GROUP BY has no row order);
-`canonical` sorts them when a comparison needs it.
+("groups_raw", rows[n, 3]) or ("groups_cols", keys, counts, sums) in table
+order (a GROUP BY has no row order); `canonical` sorts them when a
+comparison needs it.
 """
 from __future__ import annotations
 
@@ -86,6 +87,8 @@ def canonical(r):
     if r[0] == "groups_raw":
         blk = r[1]
         return canonical_groups(blk[:, 0], blk[:, 1], blk[:, 2])
+    if r[0] == "groups_cols":  # (keys, counts, sums) in table order
+        return canonical_groups(r[1], r[2], r[3])
     return r
 
 
@@ -697,9 +700,15 @@ class PlainRunner:
             res, _ = self.ctx.run(self._query(spec))
             c, s = res.rows[0]
             return ("scalar", int(c), int(s))
-        res, _ = self.ctx.run(self._query(spec), arrays=True)
         if q.tmpl == "groupby":
-            return canonical_groups(res["key"], res["count"], res["sum"])
+            # the compacted groups straight from their device buffers, in
+            # table order (a GROUP BY has no row order; `canonical` sorts
+            # when a comparison needs it)
+            self.ctx.run(self._query(spec), collect=False)
+            n = int(self.ctx.read_buffer("mgc_n", np.uint64, 1)[0])
+            return ("groups_cols", self.ctx.read_buffer("mgc_key", np.int64, n),
+                    self.ctx.read_buffer("mgc_count", np.int64, n), self.ctx.read_buffer("mgc_sum", np.int64, n))
+        res, _ = self.ctx.run(self._query(spec), arrays=True)
         return ("topk", tuple((int(k), int(v)) for k, v in zip(res["key"], res["sum"])))
 
 

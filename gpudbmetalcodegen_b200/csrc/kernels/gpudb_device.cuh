@@ -159,6 +159,57 @@ __device__ __forceinline__ long long gpudb_mod_i32(int k, const gpudb_divmagic& 
 }
 
 // ------------------------------------------------------------------
+// Order of group rows in an ORDER BY value DESC, key ASC: a before b.
+// ------------------------------------------------------------------
+__device__ __forceinline__ bool gpudb_row_before(long long va, long long ka, long long vb, long long kb) {
+    return va > vb || (va == vb && ka < kb);
+}
+
+// Merge passes a sort of n rows in chunks of `chunk` rows needs: the
+// smallest q with chunk << q >= n.
+__device__ __forceinline__ int gpudb_merge_passes(long long n, int chunk) {
+    int q = 0;
+    while (((long long)chunk << q) < n) q++;
+    return q;
+}
+
+// The same split found by one warp together: each round its 32 lanes test
+// 32 evenly spaced candidates (the test is monotone: true for every index
+// below the split), so the range shrinks 32-fold per round of loads. All
+// lanes of the warp call it and get the split.
+__device__ __forceinline__ int gpudb_merge_path_warp(const long long* av, const long long* ak, int na,
+                                                     const long long* bv, const long long* bk, int nb, int d) {
+    const int lane = (int)(threadIdx.x & 31u);
+    int lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const int step = (hi - lo + 31) / 32;
+        const int i = lo + lane * step;
+        const bool t = i < hi && !gpudb_row_before(bv[d - 1 - i], bk[d - 1 - i], av[i], ak[i]);
+        const int c = __popc(__ballot_sync(0xffffffffu, t));
+        if (c == 0) break;  // the split is lo
+        const int nlo = lo + (c - 1) * step + 1, nhi = lo + c * step;
+        lo = nlo;
+        hi = nhi < hi ? nhi : hi;
+    }
+    return lo;
+}
+
+// Merge path split of diagonal d between sorted A[0..na) and B[0..nb)
+// (arrays of value / key, row order gpudb_row_before): the number of A rows
+// among the first d merged rows (ties take A first).
+__device__ __forceinline__ int gpudb_merge_path(const long long* av, const long long* ak, int na, const long long* bv,
+                                                const long long* bk, int nb, int d) {
+    int lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        // A[mid] goes before B[d - 1 - mid]: more A rows belong to the prefix
+        if (!gpudb_row_before(bv[d - 1 - mid], bk[d - 1 - mid], av[mid], ak[mid])) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------
 // Bitmaps (semi / anti joins). Reference: bitmap_test / bitmap_set,
 // metal_common_header.h:103-111.
 // ------------------------------------------------------------------

@@ -1713,4 +1713,160 @@ std::string CudaTopK::describe() const {
     return "TopK(k=" + S(k_) + ", key=" + keyExpr_ + ", value=" + valueExpr_ + ") <- " + describeChain();
 }
 
+// ===================================================================
+// CudaSortPass
+// ===================================================================
+CudaSortPass::CudaSortPass(Mode mode, const std::string& prefix, const std::string& countBuffer,
+                           const std::string& capacityExpr, int pass)
+    : mode_(mode), prefix_(prefix), count_(countBuffer), cap_(capacityExpr), pass_(pass) {}
+
+void CudaSortPass::setInput(const std::string& keys, const std::string& counts, const std::string& values) {
+    inK_ = keys;
+    inC_ = counts;
+    inV_ = values;
+}
+
+void CudaSortPass::setOutputNames(const std::string& key, const std::string& count, const std::string& value) {
+    outK_ = key;
+    outC_ = count;
+    outV_ = value;
+}
+
+void CudaSortPass::produce(CudaCodegen& cg, ConsumerFn consume) {
+    (void)consume;
+    const int bs = cg.currentThreadgroupSize();
+    if (kChunk % bs != 0) throw std::runtime_error("CudaSortPass: the block size must divide 2048");
+    const std::string CH = S(kChunk), VT = S(kChunk / bs), P = prefix_;
+    const std::string kMax = "0x7fffffffffffffffll", kMin = "(-0x7fffffffffffffffll - 1ll)";
+    cg.addReadBufferParam(count_, "unsigned long long");
+    cg.addSizeScalarParam("cap_" + P, "long long", cap_);
+    auto set = [&](int which, bool write) {
+        for (const char* c : {"k", "c", "v"}) {
+            const std::string n = P + "_" + c + S(which);
+            if (write) cg.addBufferParam(n, "long long", cap_, false);
+            else cg.addReadBufferParam(n, "long long");
+        }
+    };
+    cg.addLine("const long long _sn = min((long long)__ldcg(" + count_ + "), cap_" + P + ");");
+    cg.addLine("const int _sneed = gpudb_merge_passes(_sn, " + CH + ");");
+    if (mode_ == Mode::Chunks) {
+        cg.addReadBufferParam(inK_, "long long");
+        cg.addReadBufferParam(inC_, "long long");
+        cg.addReadBufferParam(inV_, "long long");
+        set(0, true);
+        const int off = cg.allocDynamicSmem(3 * kChunk * 8);
+        cg.addComment("sort " + CH + "-row chunks in shared memory (bitonic network), value desc, key asc");
+        cg.addLine("long long* _sk = reinterpret_cast<long long*>(gpudb_smem + " + S(off) + ");");
+        cg.addLine("long long* _sv = _sk + " + CH + ";");
+        cg.addLine("long long* _sc = _sv + " + CH + ";");
+        cg.addBlock("for (long long _t = blockIdx.x; _t * " + CH + "ll < _sn; _t += gridDim.x)", [&]() {
+            cg.addLine("const long long _b = _t * " + CH + "ll;");
+            cg.addBlock("for (int _e = threadIdx.x; _e < " + CH + "; _e += blockDim.x)", [&]() {
+                cg.addLine("const long long _r = _b + _e;");
+                cg.addLine("if (_r < _sn) { _sk[_e] = " + inK_ + "[_r]; _sv[_e] = " + inV_ + "[_r]; _sc[_e] = " + inC_ +
+                           "[_r]; } else { _sk[_e] = " + kMax + "; _sv[_e] = " + kMin + "; _sc[_e] = 0ll; }");
+            });
+            cg.addLine("__syncthreads();");
+            cg.addBlock("for (int _size = 2; _size <= " + CH + "; _size <<= 1)", [&]() {
+                cg.addBlock("for (int _st = _size >> 1; _st > 0; _st >>= 1)", [&]() {
+                    cg.addBlock("for (int _e = threadIdx.x; _e < " + S(kChunk / 2) + "; _e += blockDim.x)", [&]() {
+                        cg.addLine("const int _i = 2 * _e - (_e & (_st - 1)), _j = _i + _st;");
+                        cg.addLine("const bool _up = (_i & _size) == 0;");
+                        cg.addLine("const bool _jb = gpudb_row_before(_sv[_j], _sk[_j], _sv[_i], _sk[_i]);");
+                        cg.addBlock("if (_up ? _jb : !_jb)", [&]() {
+                            cg.addLine("long long _x = _sk[_i]; _sk[_i] = _sk[_j]; _sk[_j] = _x;");
+                            cg.addLine("_x = _sv[_i]; _sv[_i] = _sv[_j]; _sv[_j] = _x;");
+                            cg.addLine("_x = _sc[_i]; _sc[_i] = _sc[_j]; _sc[_j] = _x;");
+                        });
+                    });
+                    cg.addLine("__syncthreads();");
+                });
+            });
+            cg.addBlock("for (int _e = threadIdx.x; _e < " + CH + "; _e += blockDim.x)", [&]() {
+                cg.addLine("const long long _r = _b + _e;");
+                cg.addLine("if (_r < _sn) { " + P + "_k0[_r] = _sk[_e]; " + P + "_v0[_r] = _sv[_e]; " + P +
+                           "_c0[_r] = _sc[_e]; }");
+            });
+            cg.addLine("__syncthreads();");
+        });
+    } else if (mode_ == Mode::Merge) {
+        const int src = pass_ & 1, dst = src ^ 1;
+        set(src, false);
+        set(dst, true);
+        const std::string SR = P + "_", SS = S(src), DS = S(dst);
+        const int off = cg.allocDynamicSmem(3 * kChunk * 8);
+        cg.addComment("merge pass " + S(pass_) + ": runs of " + CH + " << " + S(pass_) + " rows merge pairwise");
+        cg.addLine("if (" + S(pass_) + " >= _sneed) return;  // the runs already cover all rows");
+        cg.addLine("long long* _sk = reinterpret_cast<long long*>(gpudb_smem + " + S(off) + ");");
+        cg.addLine("long long* _sv = _sk + " + CH + ";");
+        cg.addLine("long long* _sc = _sv + " + CH + ";");
+        cg.addLine("__shared__ int _ssplit[2];");
+        cg.addLine("const long long _L = " + CH + "ll << " + S(pass_) + ";");
+        cg.addBlock("for (long long _t = blockIdx.x; _t * " + CH + "ll < _sn; _t += gridDim.x)", [&]() {
+            cg.addLine("const long long _o0 = _t * " + CH + "ll, _base = (_o0 / (2 * _L)) * (2 * _L);");
+            cg.addLine("const long long _aB = _base, _aE = min(_base + _L, _sn), _bE = min(_base + 2 * _L, _sn);");
+            cg.addLine("const int _na = (int)(_aE - _aB), _nb = (int)(_bE - _aE);");
+            cg.addLine("const int _d0 = (int)(_o0 - _base), _d1 = (int)(min(_o0 + " + CH + "ll, _bE) - _base);");
+            cg.addComment("the tile's split of the two runs: warps 0 and 1 search its two diagonals");
+            cg.addBlock("if (threadIdx.x < 64u)", [&]() {
+                cg.addLine("const int _sp = gpudb_merge_path_warp(" + SR + "v" + SS + " + _aB, " + SR + "k" + SS +
+                           " + _aB, _na, " + SR + "v" + SS + " + _aE, " + SR + "k" + SS + " + _aE, _nb, threadIdx.x < 32u ? _d0 : _d1);");
+                cg.addLine("if ((threadIdx.x & 31u) == 0u) _ssplit[threadIdx.x >> 5] = _sp;");
+            });
+            cg.addLine("__syncthreads();");
+            cg.addLine("const int _a0 = _ssplit[0], _a1 = _ssplit[1], _b0 = _d0 - _a0, _b1 = _d1 - _a1;");
+            cg.addLine("const int _ca = _a1 - _a0, _cb = _b1 - _b0, _tot = _ca + _cb;");
+            cg.addBlock("for (int _e = threadIdx.x; _e < _tot; _e += blockDim.x)", [&]() {
+                cg.addLine("const long long _r = _e < _ca ? _aB + _a0 + _e : _aE + _b0 + (_e - _ca);");
+                cg.addLine("_sk[_e] = " + SR + "k" + SS + "[_r]; _sv[_e] = " + SR + "v" + SS + "[_r]; _sc[_e] = " + SR +
+                           "c" + SS + "[_r];");
+            });
+            cg.addLine("__syncthreads();");
+            cg.addBlock("", [&]() {
+                cg.addLine("const int _dd = (int)threadIdx.x * " + VT + ";");
+                cg.addBlock("if (_dd < _tot)", [&]() {
+                    cg.addLine("int _ia = gpudb_merge_path(_sv, _sk, _ca, _sv + _ca, _sk + _ca, _cb, _dd), _ib = _dd - _ia;");
+                    cg.addBlock("for (int _q = 0; _q < " + VT + " && _dd + _q < _tot; ++_q)", [&]() {
+                        cg.addLine("const bool _ta = _ib >= _cb || (_ia < _ca && !gpudb_row_before(_sv[_ca + _ib], "
+                                   "_sk[_ca + _ib], _sv[_ia], _sk[_ia]));");
+                        cg.addLine("const int _x = _ta ? _ia++ : _ca + _ib++;");
+                        cg.addLine("const long long _w = _o0 + _dd + _q;");
+                        cg.addLine(SR + "k" + DS + "[_w] = _sk[_x]; " + SR + "v" + DS + "[_w] = _sv[_x]; " + SR + "c" + DS +
+                                   "[_w] = _sc[_x];");
+                    });
+                });
+            });
+            cg.addLine("__syncthreads();");
+        });
+    } else {
+        set(0, false);
+        set(1, false);
+        const std::string n = P + "_n";
+        cg.addAtomicBufferParam(n, "unsigned long long", "1");
+        cg.addBufferParam(P + "_out_k", "long long", cap_, false);
+        cg.addBufferParam(P + "_out_c", "long long", cap_, false);
+        cg.addBufferParam(P + "_out_v", "long long", cap_, false);
+        cg.addComment("the sorted rows, in order, from the buffer set the last merge pass wrote");
+        cg.addLine("const long long* _ok = (_sneed & 1) ? " + P + "_k1 : " + P + "_k0;");
+        cg.addLine("const long long* _oc = (_sneed & 1) ? " + P + "_c1 : " + P + "_c0;");
+        cg.addLine("const long long* _ov = (_sneed & 1) ? " + P + "_v1 : " + P + "_v0;");
+        cg.addBlock("for (long long _r = tid; _r < _sn; _r += tpg)", [&]() {
+            cg.addLine(P + "_out_k[_r] = _ok[_r]; " + P + "_out_c[_r] = _oc[_r]; " + P + "_out_v[_r] = _ov[_r];");
+        });
+        cg.addLine("if (tid == 0) " + n + "[0] = (unsigned long long)_sn;");
+        cg.registerMaterializeOutput(n);
+        cg.registerOutputColumn(outK_, P + "_out_k", "long long");
+        cg.registerOutputColumn(outC_, P + "_out_c", "long long");
+        cg.registerOutputColumn(outV_, P + "_out_v", "long long");
+    }
+}
+
+std::string CudaSortPass::describe() const {
+    switch (mode_) {
+        case Mode::Chunks: return "SortChunks(" + prefix_ + ", " + S(kChunk) + " rows, value desc, key asc)";
+        case Mode::Merge: return "SortMerge(" + prefix_ + ", pass " + S(pass_) + ")";
+        default: return "SortEmit(" + prefix_ + ")";
+    }
+}
+
 }  // namespace gpudb

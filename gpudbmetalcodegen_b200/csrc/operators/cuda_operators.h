@@ -571,4 +571,40 @@ private:
     int k_, maxBlocks_;
 };
 
+// ------------------------------------------------------------------
+// GPU sort of group rows for an ORDER BY without LIMIT (the reference
+// sorts its group rows on the host, codegen_main.cpp:1105-1721): rows of
+// three int64 columns (key, count, value) in dense arrays, ordered by value
+// descending, then key ascending. A merge sort in phases:
+//   Chunks : each block sorts 2048-row chunks in shared memory (bitonic);
+//   Merge p: runs of 2048 << p rows merge pairwise (merge path: each block
+//            finds its output tile's split of the two runs by binary
+//            search, stages both ranges in shared memory, and every thread
+//            merges its own span); a pass whose runs already cover all rows
+//            returns at once, so a plan carries passes for its largest size;
+//   Emit   : the sorted rows go to the output arrays, in order.
+// Rows live in two ping-pong buffer sets <prefix>_{k,c,v}{0,1}; the row
+// count is read on the device from `countBuffer`.
+// ------------------------------------------------------------------
+class CudaSortPass : public CudaOperator {
+public:
+    enum class Mode { Chunks, Merge, Emit };
+    static constexpr int kChunk = 2048;
+    CudaSortPass(Mode mode, const std::string& prefix, const std::string& countBuffer, const std::string& capacityExpr,
+                 int pass = 0);
+    // Chunks: the dense input arrays (key, count, value).
+    void setInput(const std::string& keys, const std::string& counts, const std::string& values);
+    // Emit: output column names.
+    void setOutputNames(const std::string& key, const std::string& count, const std::string& value);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    Mode mode_;
+    std::string prefix_, count_, cap_;
+    int pass_;
+    std::string inK_, inC_, inV_;
+    std::string outK_ = "key", outC_ = "count", outV_ = "value";
+};
+
 }  // namespace gpudb

@@ -677,6 +677,62 @@ CudaQueryPlan buildGroupBy(Spec& s, const TuneConfig& tune) {
     return plan;
 }
 
+// ---- groupby_sorted: the skewed-key group-by with every group returned
+// in ORDER BY sum DESC, key ASC — the reference sorts such group rows on
+// the host (the Q18 post-processing, codegen_main.cpp:1105-1721); here the
+// created groups are compacted and merge-sorted on the GPU. The plan
+// carries merge passes for up to 2048 << 15 groups; passes beyond what the
+// run's group count needs return at once.
+CudaQueryPlan buildGroupBySorted(Spec& s, const TuneConfig& tune) {
+    CudaQueryPlan plan;
+    plan.name = "GROUPBY_SORTED";
+    const std::string groupsExpr = s.str("groups", "zgroups");
+    const int passes = (int)s.num("passes", 15);
+    if (passes < 1 || passes > 20) throw std::runtime_error("groupby_sorted: passes must be in [1, 20]");
+    {
+        auto scan = makeScan(plan, "zprobe", {"z_key", "z_value"}, tune);
+        auto gb = std::make_unique<CudaHashGroupBy>(std::move(scan), "gs", "z_key[i]", "long long",
+                                                    "2 * (" + groupsExpr + ")", tune.hashLayout == HashLayout::Packed
+                                                        ? HashLayout::Linear : tune.hashLayout, tune.maxProbe);
+        gb->addAggregate("count", "1");
+        gb->addAggregate("sum", "z_value[i]");
+        gb->setWarpAggregate(tune.warpAggregate);
+        gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
+        gb->setSlotList(true);
+        appendPhase(plan, "GS_group", std::move(gb), tune);
+    }
+    const std::string cap = "max(" + groupsExpr + ", 1)";
+    {
+        auto ls = std::make_unique<CudaSlotListScan>("gs_slotlist", "gs_nslots");
+        auto mt = std::make_unique<CudaMaterialize>(std::move(ls), "gsc_n", cap);
+        mt->addColumn("gsc_key", "long long", "(long long)gs_keys[i]");
+        mt->addColumn("gsc_count", "long long", "(long long)gs_count[i]");
+        mt->addColumn("gsc_sum", "long long", "(long long)gs_sum[i]");
+        mt->setIntermediate(true);
+        auto& ph = appendPhase(plan, "GS_compact", std::move(mt), tune);
+        ph.extraBuffers.push_back({"gs_keys", "unsigned long long", true, false});
+        ph.extraBuffers.push_back({"gs_count", "unsigned long long", true, false});
+        ph.extraBuffers.push_back({"gs_sum", "unsigned long long", true, false});
+    }
+    TuneConfig st = tune;
+    st.blockSize = 512;
+    st.minBlocksPerSM = 1;
+    {
+        auto sp = std::make_unique<CudaSortPass>(CudaSortPass::Mode::Chunks, "gss", "gsc_n", cap);
+        sp->setInput("gsc_key", "gsc_count", "gsc_sum");
+        appendPhase(plan, "GS_sort_chunks", std::move(sp), st);
+    }
+    for (int p = 0; p < passes; p++)
+        appendPhase(plan, "GS_merge" + std::to_string(p),
+                    std::make_unique<CudaSortPass>(CudaSortPass::Mode::Merge, "gss", "gsc_n", cap, p), st);
+    {
+        auto sp = std::make_unique<CudaSortPass>(CudaSortPass::Mode::Emit, "gss", "gsc_n", cap);
+        sp->setOutputNames("key", "count", "sum");
+        appendPhase(plan, "GS_emit", std::move(sp), st);
+    }
+    return plan;
+}
+
 // ---- hashjoin: GPU hash build (64-bit CAS) -> probe -> per-key sum of
 // the build payload over matches (reference Q9/Q20 hash tables:
 // query_preprocessing.cpp:352-386/443-479 built on the host, probed by
@@ -892,7 +948,7 @@ CudaQueryPlan buildMix(const std::string& tmpl, Spec& s, const TuneConfig& tune)
 }  // namespace
 
 std::vector<std::string> planTemplates() {
-    return {"q1", "q6", "q6_selvec", "join_topk", "join_rows", "join_direct", "anti_join", "histogram", "multi_join", "groupby",
+    return {"q1", "q6", "q6_selvec", "join_topk", "join_rows", "join_direct", "anti_join", "histogram", "multi_join", "groupby", "groupby_sorted",
             "hashjoin", "colmax", "distinct", "mix_agg", "mix_groupby", "mix_topk", "mix_join"};
 }
 
@@ -910,6 +966,7 @@ CudaQueryPlan buildCudaPlan(const std::string& specStr, const TuneConfig& tune) 
     else if (tmpl == "q6_selvec") plan = buildQ6SelVec(s, tune);
     else if (tmpl == "multi_join") plan = buildMultiJoin(s, tune);
     else if (tmpl == "groupby") plan = buildGroupBy(s, tune);
+    else if (tmpl == "groupby_sorted") plan = buildGroupBySorted(s, tune);
     else if (tmpl == "hashjoin") plan = buildHashJoin(s, tune);
     else if (tmpl == "colmax") plan = buildColMax(s, tune);
     else if (tmpl == "distinct") plan = buildDistinct(s, tune);

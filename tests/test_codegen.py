@@ -14,7 +14,7 @@ SPECS = [
     "template=mix_topk;card=1000;k=5", "template=mix_join;attr_lt=300",
     "template=distinct;params=1;key=m_rank_z", "template=mix_agg;params=1", "template=mix_join;params=1",
     "template=mix_groupby;params=1;compact=1", "template=mix_topk;params=1;k=10", "template=join_direct",
-    "template=anti_join", "template=histogram", "template=q6_selvec",
+    "template=anti_join", "template=histogram", "template=q6_selvec", "template=multi_join", "template=groupby_sorted",
 ]
 TUNES = ["", "bs=256;scan=direct", "bs=512;scan=tma;tile=2048;stages=3", "bs=1024;scan=tma;tile=1024;stages=2",
          "layout=bucket8;smem=11", "keyed=2", "keyed=3;warp=0"]

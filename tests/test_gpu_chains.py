@@ -11,7 +11,9 @@ C-ABI against the CPU oracle on the same seeded tables (bit-exact):
   consumed by a second phase (Selection bitmap -> SelectionScan);
 * multi_join — Q5's five-phase plan over a snowflake (nation bitmap ->
   customer / supplier nation maps -> orders map -> lines' double lookup,
-  same-nation selection and per-nation sum).
+  same-nation selection and per-nation sum);
+* groupby_sorted — every group of the skewed-key group-by in ORDER BY sum
+  DESC, key ASC, merge-sorted on the GPU (the reference sorts on the host).
 
 Each runs at small sizes under several tunings, twice through the same
 buffers, on edge cases (nothing qualifies, everything qualifies, ragged
@@ -192,3 +194,42 @@ def test_multi_join_full_size(ctx):
     snow = load_snow(ctx, scale=1.0, seed=W.SEED)
     res, t = ctx.run("template=multi_join")
     assert t.device_error == 0 and res.rows == O.multi_join(snow)
+
+
+def sorted_groups(zp, nkeys):
+    k, c, s = O.groupby(zp["z_key"], zp["z_value"], cap=nkeys)
+    order = np.lexsort((k, -s))  # sum descending, then key ascending
+    return [(int(k[i]), int(c[i]), int(s[i])) for i in order]
+
+
+@pytest.mark.parametrize("nkeys,rows,tune", [(1 << 10, 200_000, ""), (1 << 16, 1_000_000, ""),
+                                             (1 << 16, 1_000_000, "smem=0;warp=0"), (3000, 3000, ""),
+                                             (1 << 14, 2_048 * 4, "bs=256"), (5, 100, "")])
+def test_groupby_sorted_parity(ctx, nkeys, rows, tune):
+    """ORDER BY sum DESC, key ASC over every group, sorted on the GPU
+    (chunk sort + merge passes), against the oracle's groups sorted on the
+    host — ragged group counts (a partial last chunk, fewer groups than one
+    chunk, exactly whole chunks) and several merge depths."""
+    zp = W.gen_zprobe(rows, nkeys=nkeys, s=1.1, seed=51)
+    ctx.upload_table("zprobe", zp)
+    ctx.register_symbol("zgroups", nkeys)
+    for _ in range(2):
+        res, t = ctx.run("template=groupby_sorted", tune)
+        assert t.device_error == 0
+        assert res.columns == ["key", "count", "sum"]
+        assert res.rows == sorted_groups(zp, nkeys)
+
+
+def test_groupby_sorted_full_size(ctx):
+    """120M Zipf(1.1) rows over 2^22 keys: ~3.3M groups, eleven merge passes."""
+    nkeys = 1 << 22
+    zp = W.gen_zprobe(120_000_000, nkeys=nkeys, s=1.1, seed=W.SEED)
+    ctx.upload_table("zprobe", zp)
+    ctx.register_symbol("zgroups", nkeys)
+    res, t = ctx.run("template=groupby_sorted", "", arrays=True)
+    assert t.device_error == 0
+    k, c, s = O.groupby(zp["z_key"], zp["z_value"], cap=nkeys)
+    order = np.lexsort((k, -s))
+    assert np.array_equal(res["key"], k[order])
+    assert np.array_equal(res["count"], c[order])
+    assert np.array_equal(res["sum"], s[order])
