@@ -883,6 +883,16 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
         e_ms = (time.perf_counter() - t0) / e_steps * 1e3
         if verified is not None:
             verified = verified and w.matches(r)
+        # where an end-to-end step goes: the uploads alone (every column's
+        # H2D, then a wait), against the whole step
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            for tname, cname, ptr, arr, in_place in pinned:
+                if not in_place:
+                    _lib.check(lib.gpudb_upload_column(ctx.handle, tname.encode(), cname.encode(), C.c_void_p(ptr),
+                                                       arr.shape[0], arr.itemsize), ctx.handle)
+            ctx.synchronize()
+        up_ms = (time.perf_counter() - t0) / e_steps * 1e3
         if pg:
             e_ms = replicas.max_over_ranks(pg, [e_ms], "cuda")[0]
         d2h = sum(len(row) for row in r.rows) * 16 + 8
@@ -890,6 +900,7 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
         e2e = {"value": rows_total / (e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": host_bytes + in_place_bytes,
                "d2h_bytes_per_step": d2h, "ms_per_step": e_ms,
                "uploaded_bytes": host_bytes, "read_in_place_bytes": in_place_bytes,
+               "upload_ms": up_ms, "upload_gbs": host_bytes / (up_ms / 1e3) / 1e9,
                "read_in_place_columns": sorted(f"{t}.{c}" for t, c in late)}
         # device copies of the in-place columns again before the host buffers go
         for tname, cname, ptr, arr, in_place in pinned:

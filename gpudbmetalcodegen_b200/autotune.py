@@ -42,7 +42,7 @@ HASH_SPACE = {
 }
 SPACES = {
     "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4", "5"], "vec": ["0", "2", "4"], "l2pf": ["0", "1", "2"]},
-    "q6": SCAN_SPACE,
+    "q6": {**SCAN_SPACE, "l2pf": ["0", "1", "2"], "vec": ["0", "2"]},
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["1", "0"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
@@ -60,7 +60,8 @@ SEEDS = {
            {"keyed": "5", "bs": "256", "tile": "512", "stages": "2", "occ": "2", "vec": "2"},
            {"keyed": "5", "bs": "256", "tile": "448", "stages": "2", "occ": "2", "vec": "2"},
            {"bs": "256", "stages": "2", "occ": "2"}, {"tile": "2048"}],
-    "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}],
+    "q6": [{"stages": "2"}, {"bs": "256", "stages": "2", "occ": "2"}, {"stages": "2", "l2pf": "1"},
+           {"bs": "256", "stages": "2", "occ": "2", "l2pf": "1"}],
     "join_topk": [{"split": "0", "stages": "2", "warp": "0"}, {"split": "1", "stages": "2"}, {"split": "1", "stages": "2", "occ": "3"},
                   {"split": "1", "stages": "2", "occ": "4", "warp": "0"}],
     "groupby": [{"bs": "256", "stages": "2", "smem": "8", "warp": "0"},

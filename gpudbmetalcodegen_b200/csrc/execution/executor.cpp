@@ -263,7 +263,9 @@ bool CudaGenericExecutor::buildLaunch(const RuntimeCompiler::CompiledQuery& cq, 
     l.smem = (unsigned)ph.dynamicSmemBytes;
     const std::pair<uint64_t, CUfunction> fkey{cq.loadId, l.fn};
     auto sc = smemConfigured_.find(fkey);
-    if (l.smem > 48 * 1024 && (sc == smemConfigured_.end() || sc->second < (int)l.smem)) {
+    // any dynamic shared memory gets the opt-in: 48 KB of it plus the
+    // kernel's static shared memory already exceeds the default limit
+    if (l.smem > 0 && (sc == smemConfigured_.end() || sc->second < (int)l.smem)) {
         const CUresult r = api.cuFuncSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)l.smem);
         if (r != CUDA_SUCCESS) {
             error = "phase '" + ph.name + "': cannot reserve " + std::to_string(l.smem) + " B shared memory (" +
