@@ -664,7 +664,8 @@ def run_serve(args, pg=None):
     oracle_check = mixed_oracle_check(tables, qs, exact_res, n=16) if rank == 0 else None
     del exact_res
     ex.close()
-    srv = S.Server(tables, sizer, plain=plain, workers=args.serve_workers, hbm_budget=150e9)
+    srv = S.Server(tables, sizer, plain=plain, workers=args.serve_workers, hbm_budget=150e9,
+                   max_batch=args.serve_max_batch)
     srv.serve(S.poisson_trace(qs, rate=rates[-1], seed=12))  # warm the workers, their arenas and pools
     per_rate, verified, clocks = [], True, None
     launches = 0
@@ -695,7 +696,8 @@ def run_serve(args, pg=None):
                 "data": "synthetic (seeded)",
                 "config": {"workload": f"serve: {len(qs)} mixed queries per trace over a resident "
                                        f"{args.serve_rows}-row table + {args.serve_dim_rows}-row dimension, Poisson "
-                                       f"arrivals, HBM budget 150 GB, {args.serve_workers} workers",
+                                       f"arrivals, HBM budget 150 GB, {args.serve_workers} workers, at most "
+                                       f"{args.serve_max_batch} queries per batch",
                            "rates": rates, "parallelism": "replicas x1"},
                 "verified": verified, "verified_vs_oracle": oracle_check, "per_rate": per_rate,
                 "plain_service_ms": {"warm_mean": float(service.mean() * 1e3),
@@ -1020,6 +1022,7 @@ def main():
     ap.add_argument("--serve-queries", type=int, default=1000)
     ap.add_argument("--serve-rates", default="500,2000,8000")
     ap.add_argument("--serve-workers", type=int, default=2)
+    ap.add_argument("--serve-max-batch", type=int, default=512)
     ap.add_argument("--serve-plain-queries", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -112,7 +112,7 @@ std::string TuneConfig::toString() const {
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
       << ";split=" << (splitJoin ? 1 : 0) << ";sprobe=" << smemProbe << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
-      << ";bvec=" << buildVectorRows;
+      << ";bvec=" << buildVectorRows << ";htf=" << hashFill;
     return o.str();
 }
 
@@ -152,6 +152,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "sprobe") t.smemProbe = std::stoi(v);
         else if (k == "bbs") t.buildBlockSize = std::stoi(v);
         else if (k == "bvec") t.buildVectorRows = std::stoi(v);
+        else if (k == "htf") t.hashFill = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -159,6 +160,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
     if (t.scan.tileRows < 0 || t.scan.tileRows % 16) throw std::runtime_error("tune: tile must be a multiple of 16 (0 = auto)");
     if (t.scan.prefetchRows < 0 || t.scan.prefetchRows > 16) throw std::runtime_error("tune: pf must be in [0,16]");
     if (t.smemCarveout < -1 || t.smemCarveout > 100) throw std::runtime_error("tune: carve must be -1 or in [0,100]");
+    if (t.hashFill < 100 || t.hashFill > 800) throw std::runtime_error("tune: htf must be in [100,800] (percent)");
     if (t.buildBlockSize != 0 && (t.buildBlockSize < 64 || t.buildBlockSize > 1024 || t.buildBlockSize % 32))
         throw std::runtime_error("tune: bbs must be 0 or a multiple of 32 in [64,1024]");
     return t;
@@ -194,6 +196,12 @@ struct Spec {
 };
 
 std::string L(long long v) { return std::to_string(v) + "ll"; }
+
+// Slots requested for a hash table of `groups` expected groups.
+std::string hashCapacity(const std::string& groups, const TuneConfig& tune) {
+    if (tune.hashFill == 200) return "2 * (" + groups + ")";
+    return "(" + groups + ") * " + std::to_string(tune.hashFill) + " / 100";
+}
 
 // `late` names columns read only by rows that survive a selective operator
 // (semi-join / hash probe); with late materialisation they are not staged.
@@ -668,7 +676,7 @@ CudaQueryPlan buildGroupBy(Spec& s, const TuneConfig& tune) {
     const std::string groupsExpr = s.str("groups", "zgroups");
     auto scan = makeScan(plan, "zprobe", {"z_key", "z_value"}, tune);
     auto gb = std::make_unique<CudaHashGroupBy>(std::move(scan), "zg", "z_key[i]", "long long",
-                                                "2 * (" + groupsExpr + ")", tune.hashLayout, tune.maxProbe);
+                                                hashCapacity(groupsExpr, tune), tune.hashLayout, tune.maxProbe);
     gb->addAggregate("count", "1");
     gb->addAggregate("sum", "z_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
@@ -692,7 +700,7 @@ CudaQueryPlan buildGroupBySorted(Spec& s, const TuneConfig& tune) {
     {
         auto scan = makeScan(plan, "zprobe", {"z_key", "z_value"}, tune);
         auto gb = std::make_unique<CudaHashGroupBy>(std::move(scan), "gs", "z_key[i]", "long long",
-                                                    "2 * (" + groupsExpr + ")", tune.hashLayout == HashLayout::Packed
+                                                    hashCapacity(groupsExpr, tune), tune.hashLayout == HashLayout::Packed
                                                         ? HashLayout::Linear : tune.hashLayout, tune.maxProbe);
         gb->addAggregate("count", "1");
         gb->addAggregate("sum", "z_value[i]");
@@ -741,7 +749,7 @@ CudaQueryPlan buildHashJoin(Spec& s, const TuneConfig& tune) {
     CudaQueryPlan plan;
     plan.name = "HASHJOIN";
     (void)s;
-    const std::string cap = "2 * n_zbuild";
+    const std::string cap = hashCapacity("n_zbuild", tune);
     {
         auto scan = makeScan(plan, "zbuild", {"zb_key", "zb_payload"}, tune);
         auto hb = std::make_unique<CudaHashBuild>(std::move(scan), "hj", "zb_key[i]", "long long", cap, tune.hashLayout,

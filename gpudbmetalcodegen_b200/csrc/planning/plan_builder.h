@@ -116,6 +116,10 @@ struct TuneConfig {
     bool warpAggregate = true;  // match_any pre-aggregation in hash / atomic aggregation
     int keyedStrategy = 0;      // CudaKeyedAgg::Strategy (0 = auto)
     int maxProbe = 128;
+    // Hash-table slots requested per expected group, in percent (200: the
+    // table is requested for twice the groups, then rounded up to a power of
+    // two). Lower fills keep a large table inside L2.
+    int hashFill = 200;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
     // join_topk: the probe lists matched rows and later phases aggregate
     // them, sized on the device (split=0: probe and group-by in one kernel,

@@ -142,3 +142,14 @@ def test_launch_bound_constants_are_not_compiled_in():
     assert "ConstantScalar long long mix_card  [mix_card]" in q.plan
     with pytest.raises(GpudbError):
         engine.Query("template=mix_agg;params=1;thr=5")  # a constant and params=1 at once
+
+
+def test_hash_fill_sizes_the_table():
+    default = engine.Query("template=groupby").plan
+    assert "pow2ceil(max(2 * (zgroups), 16))" in default
+    low = engine.Query("template=groupby", "htf=100").plan
+    assert "pow2ceil(max((zgroups) * 100 / 100, 16))" in low
+    join = engine.Query("template=hashjoin", "htf=125").plan
+    assert "(n_zbuild) * 125 / 100" in join
+    with pytest.raises(GpudbError):
+        engine.Query("template=groupby", "htf=50")
