@@ -436,6 +436,17 @@ def mixed_oracle_check(tables, queries, results, n: int = 24) -> dict:
             "ok": not bad, "host_s": time.perf_counter() - t0}
 
 
+def batch_tuning(args) -> dict:
+    """The batch kernels' launch shape from --batch-tune ("block=512;tile_rows=65536"), None for the defaults."""
+    if not args.batch_tune:
+        return None
+    out = {}
+    for kv in args.batch_tune.split(";"):
+        k, v = kv.split("=")
+        out[k.strip()] = int(v)
+    return out
+
+
 def run_mixed(args, pg=None):
     """Config: 256 seeded mixed queries over slices (1M-120M rows) of four
     resident 120M-row mix tables. One step = the whole batch through the
@@ -492,13 +503,31 @@ def run_mixed(args, pg=None):
     # plain one-query-at-a-time path (first pass compiles / warms)
     plain_res = [plain.run(q) for q in queries]
     torch.cuda.synchronize()
+    peak, peak_kind = peaks()
+    per_tmpl = {}  # template -> [queries, seconds, algorithmic bytes]
+    count_s0, count_n0 = plain.count_s, plain.count_passes
     t0 = time.perf_counter()
     for _ in range(args.plain_passes):
-        plain_res = [plain.run(q) for q in queries]
+        plain_res = []
+        for q in queries:
+            tq = time.perf_counter()
+            plain_res.append(plain.run(q))
+            d = per_tmpl.setdefault(q.tmpl, [0, 0.0, 0])
+            d[0] += 1
+            d[1] += time.perf_counter() - tq
+            d[2] += B.query_bytes(q, 0)
     torch.cuda.synchronize()
     plain_s = (time.perf_counter() - t0) / args.plain_passes
+    # per template: wall time per query against the HBM time of the bytes it
+    # must read (the count pass of a grouped query is part of its time)
+    plain_breakdown = {t: {"queries": n // args.plain_passes, "mean_ms": sec / n * 1e3,
+                           "hbm_ms": b / n / (peak * 1e9) * 1e3, "x_hbm": sec / (b / (peak * 1e9))}
+                       for t, (n, sec, b) in sorted(per_tmpl.items())}
+    count_n = plain.count_passes - count_n0
+    plain_breakdown["count_pass_mean_ms"] = (plain.count_s - count_s0) / count_n * 1e3 if count_n else None
 
-    exact = B.BatchRunner(tables, sizing="exact", plain=plain)
+    bt = batch_tuning(args)
+    exact = B.BatchRunner(tables, sizing="exact", plain=plain, tuning=bt)
     for _ in range(2):
         exact.run(queries)
     t0 = time.perf_counter()
@@ -507,7 +536,7 @@ def run_mixed(args, pg=None):
     exact_s = (time.perf_counter() - t0) / 3
     exact.close()
 
-    learned = B.BatchRunner(tables, sizing="learned", sizer=sizer, plain=plain)
+    learned = B.BatchRunner(tables, sizing="learned", sizer=sizer, plain=plain, tuning=bt)
     for _ in range(args.warmup):
         res, rep = learned.run(queries)
     stream = torch.cuda.current_stream()
@@ -543,7 +572,6 @@ def run_mixed(args, pg=None):
     stages = learned.batch.stage_ms()
     grouped_bytes = sum(B.query_bytes(q, 0) for q in queries if q.grouped)
     scalar_bytes = sum(B.query_bytes(q, 0) for q in queries if not q.grouped)
-    peak, peak_kind = peaks()
     dom = max(("group", "agg_probe"), key=lambda k: stages[k])
     dom_bytes = grouped_bytes if dom == "group" else scalar_bytes
     achieved = dom_bytes / (stages[dom] / 1e3) / 1e9 if stages[dom] else None
@@ -572,9 +600,9 @@ def run_mixed(args, pg=None):
                            "algorithmic_bytes_per_step": alg_bytes, "table_gen_s": gen_s,
                            "l2": "inputs larger than the 126 MB L2; no flush",
                            "parallelism": f"replicas x{world}"},
-                "verified": verified, "verified_vs_oracle": oracle_check,
+                "verified": verified, "verified_vs_oracle": oracle_check, "batch_tuning": bt or "default",
                 "plain_per_query": {"queries_per_s": len(queries) / plain_s, "ms_per_batch": plain_s * 1e3,
-                                    "count_passes": plain.count_passes},
+                                    "count_passes": plain.count_passes, "per_template": plain_breakdown},
                 "batched_exact": {"queries_per_s": len(queries) / exact_s, "ms_per_batch": exact_s * 1e3,
                                   "stats_ms": exact_rep.stats_ms, "execute_ms": exact_rep.execute_ms,
                                   "collect_ms": exact_rep.collect_ms, "overflowed": len(exact_rep.overflowed),
@@ -895,6 +923,13 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
                                                        arr.shape[0], arr.itemsize), ctx.handle)
             ctx.synchronize()
         up_ms = (time.perf_counter() - t0) / e_steps * 1e3
+        # ... and the query alone: the late columns still read in place from
+        # host memory, the eager ones already resident, the result collected
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            ctx.run(q, collect=True)
+        ctx.synchronize()
+        run_ms = (time.perf_counter() - t0) / e_steps * 1e3
         if pg:
             e_ms = replicas.max_over_ranks(pg, [e_ms], "cuda")[0]
         d2h = sum(len(row) for row in r.rows) * 16 + 8
@@ -902,7 +937,7 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
         e2e = {"value": rows_total / (e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": host_bytes + in_place_bytes,
                "d2h_bytes_per_step": d2h, "ms_per_step": e_ms,
                "uploaded_bytes": host_bytes, "read_in_place_bytes": in_place_bytes,
-               "upload_ms": up_ms, "upload_gbs": host_bytes / (up_ms / 1e3) / 1e9,
+               "upload_ms": up_ms, "upload_gbs": host_bytes / (up_ms / 1e3) / 1e9, "query_ms": run_ms,
                "read_in_place_columns": sorted(f"{t}.{c}" for t, c in late)}
         # device copies of the in-place columns again before the host buffers go
         for tname, cname, ptr, arr, in_place in pinned:
@@ -1017,6 +1052,7 @@ def main():
     ap.add_argument("--extras-sizer-epochs", type=int, default=30)
     ap.add_argument("--extras-serve-queries", type=int, default=600)
     ap.add_argument("--plain-passes", type=int, default=1)
+    ap.add_argument("--batch-tune", default="", help='batch kernels\' launch shape, e.g. "block=512;tile_rows=65536"')
     ap.add_argument("--serve-rows", type=int, default=120_000_000)
     ap.add_argument("--serve-dim-rows", type=int, default=30_000_000)
     ap.add_argument("--serve-queries", type=int, default=1000)

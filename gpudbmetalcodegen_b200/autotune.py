@@ -39,7 +39,6 @@ HASH_SPACE = {
     "smem": ["10", "0", "8", "12"],
     "sprobe": ["0", "4", "2"],
     "warp": ["1", "0"],
-    "htf": ["200", "150", "125", "100"],
 }
 SPACES = {
     "q1": {**SCAN_SPACE, "keyed": ["0", "1", "2", "3", "4", "5"], "vec": ["0", "2", "4"], "l2pf": ["0", "1", "2"]},
@@ -47,8 +46,7 @@ SPACES = {
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["1", "0"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
-                 "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"],
-                 "htf": ["200", "150", "125"]},
+                 "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"]},
 }
 # Joint moves coordinate descent cannot make one parameter at a time (a
 # shallower TMA ring frees the shared memory that a higher occupancy needs):

@@ -657,6 +657,7 @@ class PlainRunner:
         for c, t in tables.dim.items():
             ctx.register_column("mixdim", c, t.data_ptr(), t.numel(), t.element_size())
         self.count_passes = 0
+        self.count_s = 0.0  # wall time spent in exact count passes
         self._lock = threading.Lock()  # one engine context: queries from threads take turns
         self._queries = {}
 
@@ -678,9 +679,11 @@ class PlainRunner:
             self.ctx.register_symbol("mix_attr_lt", q.attr_lt)
 
     def exact_groups(self, q: MixQuery) -> int:
+        t0 = time.perf_counter()
         self._register_slice(q)
         res, _ = self.ctx.run(self._query(f"template=distinct;params=1;key={q.key}"), arrays=True)
         self.count_passes += 1
+        self.count_s += time.perf_counter() - t0
         return int(res["distinct"][0])
 
     def run(self, q: MixQuery) -> tuple:

@@ -126,6 +126,14 @@ __device__ __forceinline__ int findQuery(const WorkList& wl, long long w) {
     return lo;
 }
 
+// Filter words of rows b, b + step, ... (kUnroll of them); rows at or past
+// r1 read as `thr`, which no row passes.
+__device__ __forceinline__ void loadFilters(const int* __restrict__ filter, long long b, long long step, long long r1,
+                                            int thr, int (&f)[kUnroll]) {
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
+}
+
 // CTA-wide work pull; returns -1 when the list is exhausted.
 __device__ __forceinline__ long long pullWork(unsigned long long* counter, long long total, long long* s_item) {
     __syncthreads();
@@ -237,6 +245,10 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
         long long c = 0, s = 0;
+        // the filter words of a thread's next kUnroll rows are loaded while
+        // the current rows' dependent loads are in flight
+        int fn[kUnroll];
+        loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
         if (q.tmpl == GPUDB_TPL_JOIN) {
             const int* __restrict__ fk = q.fk;
             const unsigned* __restrict__ bm = q.bitmap;
@@ -244,7 +256,8 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
             for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
                 int f[kUnroll];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
+                for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
+                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
                 int key[kUnroll];
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) key[u] = f[u] < thr ? __ldcs(fk + b + u * step) : -1;
@@ -261,7 +274,8 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
             for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
                 int f[kUnroll];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
+                for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
+                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u)
                     if (f[u] < thr) {
@@ -297,9 +311,32 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
     }
     volatile unsigned* vKey = sKey;
     const long long total = __ldg(wl.prefix + wl.nq);
+    // the query whose groups the shared table holds (SHARED mode), -1 when
+    // empty: the table is flushed into that query's global table only when
+    // the CTA moves to another query's rows or runs out of work, so a query's
+    // work items on one CTA share one table and one flush
+    int heldQ = -1;
+    auto flushShared = [&](const QDesc& q) {
+        for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
+            const unsigned k = sKey[i];
+            globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
+            sKey[i] = 0u;
+            sCnt[i] = 0u;
+            sSum[i] = 0ull;
+        }
+    };
     for (long long w; (w = pullWork(counter, total, &s_item)) >= 0;) {
         const int qi = findQuery(wl, w);
-        const QDesc& q = qs[__ldg(wl.q + qi)];
+        const int qd = __ldg(wl.q + qi);
+        if (heldQ >= 0 && heldQ != qd) {
+            // pullWork's barriers ordered every add of the held query before
+            // this flush; the barrier after it orders the reset before the
+            // next rows' adds
+            flushShared(qs[heldQ]);
+            heldQ = -1;
+            __syncthreads();
+        }
+        const QDesc& q = qs[qd];
         const int* __restrict__ filter = q.filter;
         const int* __restrict__ keyc = q.key;
         const long long* __restrict__ value = q.value;
@@ -310,11 +347,14 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const int log2cap = q.log2cap;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
+        int fn[kUnroll];
+        loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
         for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
             int f[kUnroll], kr[kUnroll];
             long long v[kUnroll];
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
+            for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
+            loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
                 const bool p = f[u] < thr;
@@ -382,18 +422,10 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
             }
         }
-        if (mode == GPUDB_AGG_SHARED) {
-            __syncthreads();
-            // flush the shared table into the query's global table
-            for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
-                const unsigned k = sKey[i];
-                globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
-                sKey[i] = 0u;
-                sCnt[i] = 0u;
-                sSum[i] = 0ull;
-            }
-        }
+        if (mode == GPUDB_AGG_SHARED) heldQ = qd;
     }
+    // pullWork's barriers ordered the last adds before this flush
+    if (heldQ >= 0) flushShared(qs[heldQ]);
 }
 
 // Block-wide merge of per-thread sorted lists; warp 0 receives the result.
