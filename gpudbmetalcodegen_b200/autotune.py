@@ -270,7 +270,7 @@ def tune_batch(runner_factory: Callable[[dict], object], queries, space: Optiona
     return coordinate_descent(space, measure, rounds=rounds, log=log)
 
 
-def measure_agg_modes(tables, rows: int, cards=(16, 1024, 8192, 65536, 524288, 4194304),
+def measure_agg_modes(tables, rows: int, cards=(16, 256, 1024, 8192, 65536, 524288, 4194304),
                       keys=("m_rank_u", "m_rank_z"), thr: int = 5000, reps: int = 3) -> List[dict]:
     """Device time of the batched group-by stage for one query of `rows`
     rows per aggregation strategy, over key cardinalities and key skew
@@ -282,8 +282,10 @@ def measure_agg_modes(tables, rows: int, cards=(16, 1024, 8192, 65536, 524288, 4
         for card in cards:
             q = B.MixQuery("groupby", 0, 0, rows, thr, key=key, card=card)
             row = {"key": key, "card": card}
-            for mode, name in ((B.AGG_SHARED, "shared"), (B.AGG_GLOBAL_WARP, "global_warp"),
-                               (B.AGG_GLOBAL, "global")):
+            modes = ((B.AGG_SHARED, "shared"), (B.AGG_GLOBAL_WARP, "global_warp"), (B.AGG_GLOBAL, "global"))
+            if card <= B.DIRECT_MAX_CARD:
+                modes += ((B.AGG_SHARED_DIRECT, "direct"),)
+            for mode, name in modes:
                 b = B.Batch()
                 try:
                     b.set_queries([tables.query_struct(q)])

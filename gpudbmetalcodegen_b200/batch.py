@@ -33,7 +33,9 @@ from . import _lib
 from ._lib import check
 
 TEMPLATES = ("agg", "join", "groupby", "topk")
-AGG_AUTO, AGG_SHARED, AGG_GLOBAL_WARP, AGG_GLOBAL = 0, 1, 2, 3
+AGG_AUTO, AGG_SHARED, AGG_GLOBAL_WARP, AGG_GLOBAL, AGG_SHARED_DIRECT = 0, 1, 2, 3, 4
+DIRECT_MAX_CARD = 1024       # the direct shared table holds keys of (-card, card) in 2048 slots
+DIRECT_SKEW_SHARE = 0.01     # top sample-key share above which a small domain counts as skewed
 SHARED_MAX_GROUPS = 1024     # groups that fit the per-CTA shared table at load <= 1/2
 TPL = {name: i for i, name in enumerate(TEMPLATES)}
 DEVERR_HASH_OVERFLOW = 0x1
@@ -563,12 +565,20 @@ def groups_from_prediction(q: MixQuery, y0: float, margin: float) -> int:
 SKEW_SHARE = 0.004           # sample share of the most frequent key that counts as skew
 
 
-def agg_mode_for(groups: int, features: Optional[np.ndarray]) -> int:
-    """Aggregation strategy of a group-by from its expected group count and
-    the 4096-row sample (measured on B200, 60M rows: shared memory wins for
-    up to ~1K groups and for skewed keys at any cardinality, where hot keys
-    would serialise global atomics; the global table wins 2-3x for
-    unskewed keys beyond a few thousand groups)."""
+def agg_mode_for(groups: int, features: Optional[np.ndarray], card: Optional[int] = None) -> int:
+    """Aggregation strategy of a group-by from its key domain, its expected
+    group count and the 4096-row sample (measured on B200, 60M rows: a key
+    domain of at most 1024 values indexes the shared table directly; shared
+    memory wins for up to ~1K groups and for skewed keys at any
+    cardinality, where hot keys would serialise global atomics; the global
+    table wins 2-3x for unskewed keys beyond a few thousand groups)."""
+    if card is not None and card <= DIRECT_MAX_CARD:
+        # ... unless one key holds well above its uniform share: its slot's
+        # serialised shared atomics then cost more than warp aggregation
+        # (measured, 60M rows: uniform keys 2x faster direct; Zipf(1.1)
+        # keys 8-33 % slower)
+        skewed = features is not None and features[12] >= max(2.0 / card, DIRECT_SKEW_SHARE)
+        return AGG_SHARED if skewed else AGG_SHARED_DIRECT
     if groups <= SHARED_MAX_GROUPS or features is None:
         return AGG_SHARED
     return AGG_SHARED if features[12] >= SKEW_SHARE else AGG_GLOBAL
@@ -709,8 +719,12 @@ class PlainRunner:
             # when a comparison needs it)
             self.ctx.run(self._query(spec), collect=False)
             n = int(self.ctx.read_buffer("mgc_n", np.uint64, 1)[0])
-            return ("groups_cols", self.ctx.read_buffer("mgc_key", np.int64, n),
-                    self.ctx.read_buffer("mgc_count", np.int64, n), self.ctx.read_buffer("mgc_sum", np.int64, n))
+            # into pinned buffers (a pageable copy of millions of groups runs
+            # at a fraction of the link's rate); each returns to the pool
+            # when the caller drops the array
+            pool = pinned_pool()
+            return ("groups_cols",) + tuple(self.ctx.read_buffer(name, np.int64, n, out=pool.array(8 * n))
+                                            for name in ("mgc_key", "mgc_count", "mgc_sum"))
         res, _ = self.ctx.run(self._query(spec), arrays=True)
         return ("topk", tuple((int(k), int(v)) for k, v in zip(res["key"], res["sum"])))
 
@@ -789,7 +803,8 @@ class BatchRunner:
         self._features = None
         groups = self.size(queries, report)
         modes = [(self.agg_mode if self.agg_mode is not None else
-                  agg_mode_for(g, None if self._features is None else self._features[i])) if q.grouped else AGG_AUTO
+                  agg_mode_for(g, None if self._features is None else self._features[i], q.card))
+                 if q.grouped else AGG_AUTO
                  for i, (g, q) in enumerate(zip(groups, queries))]
         if (groups, modes) != self._groups:
             self._arr["groups"] = groups

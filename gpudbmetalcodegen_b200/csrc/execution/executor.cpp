@@ -82,10 +82,12 @@ void CudaGenericExecutor::registerTableRowCount(const std::string& table, size_t
     resolver_.registerSymbol("num" + table, rows);
 }
 
+// Registering a column frees nothing, so the captured graphs stay: a graph
+// is looked up by every launch argument (column pointers and sizes among
+// them), so one captured over other pointers is simply never matched.
 void CudaGenericExecutor::registerTableBuffer(const std::string& column, const void* dptr, size_t rows,
                                               size_t elemBytes) {
     columns_[column] = {dptr, rows, elemBytes, ++generationCounter_};
-    clearGraphs();
 }
 
 void CudaGenericExecutor::registerAllocatedBuffer(const std::string& name, void* dptr, size_t bytes, size_t elemBytes) {
@@ -147,7 +149,6 @@ void CudaGenericExecutor::registerHostColumn(const std::string& column, const st
     }
     columns_[column] = {dptr, rows, elemBytes, ++generationCounter_, true};
     registerTableRowCount(table, rows);
-    clearGraphs();
 }
 
 size_t CudaGenericExecutor::tableRows(const std::string& table) const {
@@ -483,6 +484,9 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
         for (const auto& f : fills) key += ";" + std::to_string((uintptr_t)f.ptr) + "/" + std::to_string(f.bytes);
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
+            // graphs of argument sets that no longer occur (columns
+            // registered elsewhere since) are dropped in bulk
+            if (graphs_.size() >= kMaxGraphs) clearGraphs();
             GraphEntry g;
             if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 error = "cudaStreamBeginCapture failed";

@@ -134,6 +134,7 @@ private:
     cudaStream_t stream_ = nullptr;
     unsigned* errWord_ = nullptr;
     unsigned* errHost_ = nullptr;
+    static constexpr size_t kMaxGraphs = 512;  // captured graphs kept per context
     bool skipZeroInit_ = false;
     bool useGraphs_ = false;
     bool deferSync_ = false;

@@ -72,7 +72,7 @@ struct QDesc {
     unsigned* bitmap;
     Slot* ht;
     int log2cap, maxProbe;
-    int aggMode;  // GPUDB_AGG_SHARED / GPUDB_AGG_GLOBAL_WARP / GPUDB_AGG_GLOBAL
+    int aggMode;  // GPUDB_AGG_SHARED / _GLOBAL_WARP / _GLOBAL / _SHARED_DIRECT
     unsigned* slots;
     long long* tk_part;  // [tk_chunks][kTopK] of (value, key)
     long long tk_chunks;
@@ -194,8 +194,8 @@ __device__ __forceinline__ void globalAddFrom(const QDesc& q, bool live, unsigne
     if (live) {
         slot = slotFrom(q.ht, q.log2cap, enc, s0, cur, (unsigned)q.maxProbe, q.err, &fresh);
         if (slot >= 0) {
-            atomicAdd(&q.ht[slot].count, (unsigned)c);
-            atomicAdd(&q.ht[slot].sum, v);
+            gpudb_red_add_u32(&q.ht[slot].count, (unsigned)c);
+            gpudb_red_add_u64(&q.ht[slot].sum, v);
         }
     }
     const unsigned long long pos = gpudb_warp_reserve(q.nslots, fresh);
@@ -317,8 +317,10 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
     // work items on one CTA share one table and one flush
     int heldQ = -1;
     auto flushShared = [&](const QDesc& q) {
+        const bool direct = q.aggMode == GPUDB_AGG_SHARED_DIRECT;
         for (int i = threadIdx.x; i < kSmemSlots; i += blockDim.x) {
-            const unsigned k = sKey[i];
+            // a direct slot i holds key i + 1 - card (encoded i + 1) once counted
+            const unsigned k = direct ? (sCnt[i] ? (unsigned)i + 1u : 0u) : sKey[i];
             globalAdd(q, k != 0u, k, sCnt[i], sSum[i]);
             sKey[i] = 0u;
             sCnt[i] = 0u;
@@ -371,13 +373,26 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 c[u] = 1ull;
                 val[u] = (unsigned long long)v[u];
             }
+            if (mode == GPUDB_AGG_SHARED_DIRECT) {
+                // keys in (-card, card): enc - 1 in [0, 2 card - 1) indexes
+                // the table directly, no probing and no warp aggregation
+                // (same-slot lanes of one warp serialise in the shared
+                // atomic unit, cheaper than a match and two peer sums)
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    if (!live[u]) continue;
+                    gpudb_red_add_shared_u32(&sCnt[enc[u] - 1u], 1u);
+                    gpudb_red_add_shared_u64(&sSum[enc[u] - 1u], val[u]);
+                }
+                continue;
+            }
             if (mode != GPUDB_AGG_GLOBAL) {
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
                     if (!live[u]) continue;
                     const unsigned am = __activemask();
                     const unsigned peers = __match_any_sync(am, enc[u]);
-                    c[u] = gpudb_peer_sum(am, peers, c[u]);
+                    c[u] = (unsigned long long)__popc(peers);  // every peer is one live row
                     val[u] = gpudb_peer_sum(am, peers, val[u]);
                     live[u] = (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
                 }
@@ -393,8 +408,8 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                         unsigned cur = vKey[h];
                         if (cur == 0u) cur = atomicCAS(&sKey[h], 0u, enc[u]) == 0u ? enc[u] : vKey[h];
                         if (cur == enc[u]) {
-                            atomicAdd(&sCnt[h], (unsigned)c[u]);
-                            atomicAdd(&sSum[h], val[u]);
+                            gpudb_red_add_shared_u32(&sCnt[h], (unsigned)c[u]);
+                            gpudb_red_add_shared_u64(&sSum[h], val[u]);
                             done = true;
                             break;
                         }
@@ -413,8 +428,8 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
                     if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
-                        atomicAdd(&ht[s0[u]].count, (unsigned)c[u]);
-                        atomicAdd(&ht[s0[u]].sum, val[u]);
+                        gpudb_red_add_u32(&ht[s0[u]].count, (unsigned)c[u]);
+                        gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
                         live[u] = false;
                     }
                 }
@@ -422,7 +437,7 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
             }
         }
-        if (mode == GPUDB_AGG_SHARED) heldQ = qd;
+        if (mode == GPUDB_AGG_SHARED || mode == GPUDB_AGG_SHARED_DIRECT) heldQ = qd;
     }
     // pullWork's barriers ordered the last adds before this flush
     if (heldQ >= 0) flushShared(qs[heldQ]);
@@ -831,6 +846,8 @@ int plan(gpudb_batch* b) {
         // table (with spill to the global one), which is never far off
         d.aggMode = q.agg_mode != GPUDB_AGG_AUTO ? q.agg_mode : GPUDB_AGG_SHARED;
         if (!b->warpAgg && d.aggMode == GPUDB_AGG_GLOBAL_WARP) d.aggMode = GPUDB_AGG_GLOBAL;
+        // the direct table holds the 2 card - 1 encoded keys of (-card, card)
+        if (d.aggMode == GPUDB_AGG_SHARED_DIRECT && 2 * d.card - 1 > kSmemSlots) d.aggMode = GPUDB_AGG_SHARED;
         char* p = zb + zOff[i];
         d.agg = reinterpret_cast<unsigned long long*>(p);
         d.topk_n = d.agg + 3;
@@ -1061,7 +1078,7 @@ int gpudb_batch_set_queries(gpudb_batch* b, const gpudb_batch_query* q, int n) {
             gpudb::setThreadError(who + " asks for more than 2^30 groups");
             return GPUDB_E_INVALID;
         }
-        if (x.agg_mode < GPUDB_AGG_AUTO || x.agg_mode > GPUDB_AGG_GLOBAL) {
+        if (x.agg_mode < GPUDB_AGG_AUTO || x.agg_mode > GPUDB_AGG_SHARED_DIRECT) {
             gpudb::setThreadError(who + " has an unknown agg_mode");
             return GPUDB_E_INVALID;
         }
@@ -1091,7 +1108,7 @@ int gpudb_batch_set_groups(gpudb_batch* b, int qi, uint64_t groups) {
 }
 
 int gpudb_batch_set_agg_mode(gpudb_batch* b, int qi, int mode) {
-    if (!b || qi < 0 || qi >= (int)b->queries.size() || mode < GPUDB_AGG_AUTO || mode > GPUDB_AGG_GLOBAL)
+    if (!b || qi < 0 || qi >= (int)b->queries.size() || mode < GPUDB_AGG_AUTO || mode > GPUDB_AGG_SHARED_DIRECT)
         return GPUDB_E_INVALID;
     if (b->queries[qi].agg_mode != mode) {
         b->queries[qi].agg_mode = mode;

@@ -302,6 +302,24 @@ __device__ __forceinline__ unsigned gpudb_smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
 }
 
+// ------------------------------------------------------------------
+// Fire-and-forget reductions (PTX `red`): an add whose old value nobody
+// reads, so the issuing thread never waits for the atomic unit's answer.
+// Relaxed, GPU scope: the semantics of atomicAdd.
+// ------------------------------------------------------------------
+__device__ __forceinline__ void gpudb_red_add_u32(unsigned* p, unsigned v) {
+    asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void gpudb_red_add_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void gpudb_red_add_shared_u32(unsigned* p, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(gpudb_smem_addr(p)), "r"(v) : "memory");
+}
+__device__ __forceinline__ void gpudb_red_add_shared_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(gpudb_smem_addr(p)), "l"(v) : "memory");
+}
+
 __device__ __forceinline__ void gpudb_mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(gpudb_smem_addr(bar)), "r"(count) : "memory");
 }

@@ -607,7 +607,11 @@ void CudaBitmapBuild::produce(CudaCodegen& cg, ConsumerFn consume) {
             cg.addLine("gpudb_bitmap_set(" + bitmapName_ + ", _bk);");
         } else {
             cg.addLine("const unsigned _bbit = 1u << (unsigned)(_bk & 31);");
-            cg.addLine("if ((atomicOr(" + bitmapName_ + " + (_bk >> 5), _bbit) & _bbit) == 0u) ++_bm_fresh;");
+            // a bit already set costs a load, not an atomic round trip: bits
+            // only go from 0 to 1 during the pass, so a stale 0 costs the
+            // atomic and nothing else (a repeated key's word stays in cache)
+            cg.addLine("if ((" + bitmapName_ + "[_bk >> 5] & _bbit) == 0u && (atomicOr(" + bitmapName_ +
+                       " + (_bk >> 5), _bbit) & _bbit) == 0u) ++_bm_fresh;");
         }
         consume();
         cg.decreaseIndent();

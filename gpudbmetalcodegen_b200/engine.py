@@ -364,8 +364,15 @@ class Context:
         check(self._lib.gpudb_query_algorithmic_bytes(self.handle, query.handle, C.byref(v)), self.handle)
         return v.value
 
-    def read_buffer(self, name: str, dtype, count: int) -> np.ndarray:
-        out = np.zeros(count, dtype=dtype)
+    def read_buffer(self, name: str, dtype, count: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The first `count` elements of device buffer `name`; into `out`
+        (a C-contiguous array of that dtype, e.g. a view of pinned memory)
+        when given."""
+        if out is None:
+            out = np.empty(count, dtype=dtype)
+        elif out.dtype != np.dtype(dtype) or out.size < count or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous array of the buffer's dtype with room for count elements")
+        out = out[:count]
         check(self._lib.gpudb_read_buffer(self.handle, name.encode(), out.ctypes.data, out.nbytes), self.handle)
         return out
 

@@ -91,6 +91,9 @@ typedef struct {
 #define GPUDB_AGG_SHARED 1       /* warp + per-CTA shared-memory table, flushed       */
 #define GPUDB_AGG_GLOBAL_WARP 2  /* warp aggregation, then the global table          */
 #define GPUDB_AGG_GLOBAL 3       /* the global table directly (mostly distinct keys) */
+#define GPUDB_AGG_SHARED_DIRECT 4 /* per-CTA shared-memory table indexed by the key   *
+                                   * itself, no warp aggregation; card <= 1024 (else  *
+                                   * SHARED), flushed like SHARED                     */
 
 int gpudb_batch_create(gpudb_ctx* ctx, gpudb_batch** out);
 void gpudb_batch_free(gpudb_batch* b);

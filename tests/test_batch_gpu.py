@@ -40,6 +40,8 @@ def edge_queries(rows):
         B.MixQuery("topk", 1, 9, 300_000, 7_000, key="m_rank_z", card=3, k=16),  # k > groups
         B.MixQuery("topk", 0, 0, rows, 2_500, card=1 << 16, k=1),
         B.MixQuery("topk", 1, 11, 500_000, 5_000, key="m_rank_z", card=1 << 20, k=10),  # ties at the top
+        B.MixQuery("groupby", 0, 2, rows - 2, 9_000, card=1024),        # the direct table's largest domain
+        B.MixQuery("groupby", 1, 0, rows, 6_000, key="m_rank_z", card=1025),  # one past it: hashed
     ]
 
 
@@ -78,7 +80,7 @@ def test_batch_tunings_and_bound_sizing(tables, tuning):
     r.close()
 
 
-@pytest.mark.parametrize("mode", [B.AGG_SHARED, B.AGG_GLOBAL_WARP, B.AGG_GLOBAL])
+@pytest.mark.parametrize("mode", [B.AGG_SHARED, B.AGG_GLOBAL_WARP, B.AGG_GLOBAL, B.AGG_SHARED_DIRECT])
 def test_every_aggregation_strategy(tables, mode):
     qs = [q for q in edge_queries(tables.rows) + mixed(tables, 80, seed=21) if q.grouped]
     r = B.BatchRunner(tables, sizing="exact", agg_mode=mode)

@@ -190,3 +190,24 @@ def test_result_fingerprint_is_order_independent_and_sensitive():
     c = ("groups_raw", np.array([[5, 1, 10], [2, 3, 31], [9, 2, 7]], dtype=np.int64))
     assert B.result_fingerprint(a) != B.result_fingerprint(c)
     assert B.result_fingerprint(("scalar", 3, 4)) == ("scalar", 3, 4)
+
+
+def test_aggregation_strategy_policy():
+    f = np.zeros(16, dtype=np.float32)
+    # a key domain of at most 1024 values indexes the shared table directly
+    assert B.agg_mode_for(5, f, card=1) == B.AGG_SHARED_DIRECT
+    assert B.agg_mode_for(1000, f, card=B.DIRECT_MAX_CARD) == B.AGG_SHARED_DIRECT
+    assert B.agg_mode_for(1000, f, card=B.DIRECT_MAX_CARD + 1) == B.AGG_SHARED
+    # ... unless one key holds well above its uniform share
+    f[12] = 0.07  # uniform over 16 keys: 1/16 plus sampling noise
+    assert B.agg_mode_for(16, f, card=16) == B.AGG_SHARED_DIRECT
+    f[12] = 0.18  # Zipf(1.1) ranks modulo 16
+    assert B.agg_mode_for(16, f, card=16) == B.AGG_SHARED
+    f[12] = 0.003  # uniform over 1024 keys
+    assert B.agg_mode_for(1024, f, card=1024) == B.AGG_SHARED_DIRECT
+    f[12] = 0.0
+    # beyond it: few groups or skewed keys -> shared, else the global table
+    assert B.agg_mode_for(1 << 20, f, card=1 << 22) == B.AGG_GLOBAL
+    f[12] = B.SKEW_SHARE
+    assert B.agg_mode_for(1 << 20, f, card=1 << 22) == B.AGG_SHARED
+    assert B.agg_mode_for(1 << 20, None, card=1 << 22) == B.AGG_SHARED
