@@ -155,6 +155,13 @@ class Workload:
         """(table, column) pairs the plan materialises late."""
         return set()
 
+    # the table the end-to-end run streams from host memory in chunks, and
+    # the tuning of the plan it streams (None: no streamed form)
+    stream_table = None
+
+    def stream_tune(self, tune: str):
+        return None
+
     def config(self) -> dict:
         return {"workload": self.description}
 
@@ -228,6 +235,14 @@ class JoinTopK(Workload):
         # read only by probe rows that pass the filter and the semi-join
         return set() if "late=0" in tune else {("probe", "p_price"), ("probe", "p_discount")}
 
+    stream_table = "probe"
+
+    def stream_tune(self, tune):
+        # the split plan's group phase reads the probe table after the
+        # probe, so the streamed form is the unsplit plan of the same tuning
+        kv = [t for t in tune.split(";") if t and not t.startswith("split=")]
+        return ";".join(kv + ["split=0"])
+
     def config(self):
         self.expected()
         return {"workload": self.description, "build_rows": self.build_rows, "probe_rows": self.probe_rows,
@@ -241,6 +256,9 @@ class FactScan(Workload):
         self.n = args.fact_rows
         self.spec = f"template={which}"
         self.kernel = {"q1": "Q1_reduce", "q6": "Q6_reduce", "q6_selvec": "Q6S_select"}[which]
+        # one scan phase accumulating into zero-filled aggregates: streamable
+        # (the selection-vector form's bitmap is indexed by chunk rows: not)
+        self.stream_table = "fact" if which in ("q1", "q6") else None
         self.description = {
             "q1": f"q1: scan-filter-group-aggregate over {self.n} rows x 38 B",
             "q6": f"q6: scan-filter-sum over {self.n} rows x 28 B",
@@ -253,6 +271,9 @@ class FactScan(Workload):
 
     def rows(self):
         return self.n
+
+    def stream_tune(self, tune):
+        return tune if self.stream_table else None
 
     def expected(self):
         from oracle import oracle_py as O
@@ -939,10 +960,45 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
                "uploaded_bytes": host_bytes, "read_in_place_bytes": in_place_bytes,
                "upload_ms": up_ms, "upload_gbs": host_bytes / (up_ms / 1e3) / 1e9, "query_ms": run_ms,
                "read_in_place_columns": sorted(f"{t}.{c}" for t, c in late)}
-        # device copies of the in-place columns again before the host buffers go
+        # the same through the chunked streaming entry: the streamed table's
+        # copies overlap the kernels of earlier chunks (and its late columns'
+        # in-place reads overlap later chunks' copies)
+        stune = w.stream_tune(q.tune)
+        if stune is not None and args.e2e_chunk_rows > 0:
+            st = w.stream_table
+            qs = ctx.prepare(w.spec, stune)
+            late_s = w.late_columns(stune)
+            scols = [(c, ptr, arr.itemsize, (t, c) in late_s) for t, c, ptr, arr, _ in pinned if t == st]
+            srows = next(arr.shape[0] for t, _, _, arr, _ in pinned if t == st)
+
+            def stream_step():
+                for tname, cname, ptr, arr, _ in pinned:
+                    if tname != st:
+                        _lib.check(lib.gpudb_upload_column(ctx.handle, tname.encode(), cname.encode(),
+                                                           C.c_void_p(ptr), arr.shape[0], arr.itemsize), ctx.handle)
+                r, _ = ctx.run_streamed(qs, st, scols, srows, args.e2e_chunk_rows)
+                return r
+
+            for _ in range(2):
+                r = stream_step()
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(e_steps):
+                r = stream_step()
+            ctx.synchronize()
+            s_ms = (time.perf_counter() - t0) / e_steps * 1e3
+            if pg:
+                s_ms = replicas.max_over_ranks(pg, [s_ms], "cuda")[0]
+            s_ok = None if verified is None else w.matches(r)
+            if verified is not None:
+                verified = verified and s_ok
+            e2e.update({"value": rows_total / (s_ms / 1e3), "ms_per_step": s_ms, "unstreamed_ms_per_step": e_ms,
+                        "streamed": {"table": st, "chunk_rows": args.e2e_chunk_rows, "tune": stune,
+                                     "in_place_columns": sorted(c for c, _, _, ip in scols if ip),
+                                     "verified": s_ok}})
+        # device copies of every column again before the host buffers go
         for tname, cname, ptr, arr, in_place in pinned:
-            if in_place:
-                ctx.upload_column(tname, cname, arr)
+            ctx.upload_column(tname, cname, arr)
         ctx.synchronize()
         for _, _, ptr, _, _ in pinned:
             lib.gpudb_host_free(C.c_void_p(ptr))
@@ -1034,6 +1090,8 @@ def main():
                                                    'tunings) or "search" (the full autotuner search)')
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-chunk-rows", type=int, default=4_000_000,
+                    help="rows per chunk of the end-to-end streamed run (0: no streamed run)")
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
     ap.add_argument("--no-extras", action="store_true",

@@ -42,6 +42,10 @@ class PhaseDesc(C.Structure):
                 ("nbindings", C.c_int)]
 
 
+class StreamColumn(C.Structure):
+    _fields_ = [("column", C.c_char_p), ("host", C.c_void_p), ("elem_bytes", C.c_int32), ("in_place", C.c_int32)]
+
+
 class Timing(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("nphases", C.c_int), ("phase_ms", C.c_double * MAX_PHASES),
                 ("phase_grid", C.c_int * MAX_PHASES), ("phase_block", C.c_int * MAX_PHASES),
@@ -137,6 +141,8 @@ _SIGNATURES = [
     ("gpudb_query_algorithmic_bytes", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]),
     ("gpudb_query_run", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p),
                                   C.POINTER(Timing)]),
+    ("gpudb_query_run_streamed", C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_uint64,
+                                           C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(Timing)]),
     ("gpudb_query_enqueue", C.c_int, [C.c_void_p, C.c_void_p]),
     ("gpudb_ctx_sync", C.c_int, [C.c_void_p, C.POINTER(C.c_uint)]),
     ("gpudb_result_shape", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),

@@ -533,6 +533,31 @@ int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gp
     })
 }
 
+int gpudb_query_run_streamed(gpudb_ctx* ctx, gpudb_query* q, const char* table, const gpudb_stream_column* cols,
+                             int ncols, uint64_t rows, uint64_t chunk_rows, gpudb_result** result,
+                             gpudb_timing* timing) {
+    if (!ctx || !q || !table || ncols < 0 || (ncols && !cols) || chunk_rows == 0)
+        return fail(ctx, GPUDB_E_INVALID, "bad argument");
+    if (result) *result = nullptr;
+    std::vector<gpudb::StreamColumn> sc;
+    for (int i = 0; i < ncols; i++) {
+        if (!cols[i].column || (!cols[i].host && rows) || cols[i].elem_bytes <= 0)
+            return fail(ctx, GPUDB_E_INVALID, "bad stream column");
+        sc.push_back({cols[i].column, cols[i].host, (size_t)cols[i].elem_bytes, cols[i].in_place != 0});
+    }
+    GPUDB_GUARD(ctx, {
+        cudaSetDevice(ctx->qc->ex.device());
+        gpudb::ExecutionResult r;
+        std::string err;
+        ctx->qc->ex.setSkipZeroInit(false);
+        const int rc = gpudb::runStreamed(*ctx->qc, *q->q, table, sc, rows, chunk_rows, result != nullptr, r, err);
+        fillTiming(r, timing);
+        if (rc != 0) return fail(ctx, mapStatus(rc), err);
+        if (result) *result = new gpudb_result{std::move(r.result)};
+        return GPUDB_OK;
+    })
+}
+
 int gpudb_query_collect(gpudb_ctx* ctx, gpudb_query* q, gpudb_result** result) {
     if (!ctx || !q || !result) return fail(ctx, GPUDB_E_INVALID, "bad argument");
     *result = nullptr;

@@ -151,6 +151,11 @@ void CudaGenericExecutor::registerHostColumn(const std::string& column, const st
     registerTableRowCount(table, rows);
 }
 
+void CudaGenericExecutor::registerStreamChunk(const std::string& column, const void* dptr, size_t rows,
+                                              size_t elemBytes, bool host) {
+    columns_[column] = {dptr, rows, elemBytes, ++generationCounter_, host};
+}
+
 size_t CudaGenericExecutor::tableRows(const std::string& table) const {
     auto it = tableRows_.find(table);
     if (it != tableRows_.end()) return it->second;

@@ -71,6 +71,18 @@ public:
     void registerHostColumn(const std::string& column, const std::string& table, const void* host, size_t rows,
                             size_t elemBytes);
 
+    // Chunked streaming (the reference's chunk loop, codegen_main.cpp:686-808):
+    // `dptr` holds one chunk of `rows` rows of a streamed column (device
+    // memory, or the mapped device address of pinned host memory when
+    // `host`, then read in place by late-materialised bindings only).
+    // Neither call touches the table's row-count symbol, so size
+    // expressions keep seeing the whole table while setScanRows() sets the
+    // extent the scanning phases walk.
+    void registerStreamChunk(const std::string& column, const void* dptr, size_t rows, size_t elemBytes, bool host);
+    void setScanRows(const std::string& table, size_t rows) { tableRows_[table] = rows; }
+    // Drop a column registration (a streamed chunk must not outlive its run).
+    void forgetColumn(const std::string& column) { columns_.erase(column); }
+
     // --- execution -----------------------------------------------------------
     // Run phases [first, last) (last < 0 = all) `warmup` + `measured` times.
     // Returns 0, or a negative status with `error` filled.

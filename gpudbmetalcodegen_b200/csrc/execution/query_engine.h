@@ -29,10 +29,21 @@ struct PreparedQuery {
     bool maxKeyColumnsFound = false;
 };
 
+// Device chunk buffers, copy stream and events of chunked streaming runs
+// (created on first use, reused by later runs).
+struct StreamRing {
+    static constexpr int kSlots = 3;  // chunks in flight: copying, waiting, being scanned
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ready[kSlots] = {}, consumed[kSlots] = {};
+    std::map<std::string, std::pair<void*, size_t>> buf[kSlots];  // column -> (device buffer, bytes)
+    ~StreamRing();
+};
+
 // Everything that lives as long as a gpudb_ctx.
 struct QueryContext {
     explicit QueryContext(int device) : ex(device) {}
     CudaGenericExecutor ex;
+    std::unique_ptr<StreamRing> ring;  // destroyed before the executor
     struct MaxKeyEntry {
         uint64_t generation;
         long long max;
@@ -58,6 +69,26 @@ long long registerMaxKey(QueryContext& qc, const std::string& column);
 // status with `err` set; GPUDB_E_DEVICE-style status -7 on device errors.
 int runQuery(QueryContext& qc, PreparedQuery& q, int warmup, int measured, bool collect, ExecutionResult& out,
              std::string& err);
+
+// One column of a table streamed from host memory.
+struct StreamColumn {
+    std::string column;
+    const void* host = nullptr;  // its row 0, in pinned host memory
+    size_t elemBytes = 0;
+    bool inPlace = false;        // read in place over the host link (mapped), not copied per chunk
+};
+
+// Chunked streaming run (the reference's chunked path, codegen_main.cpp:
+// 686-808): the phases before the first phase that scans `table` run
+// once (with their sizing steps), the phases that scan it run once per
+// chunk of `chunkRows` rows, accumulating (zero fills on the first chunk
+// only), and the remaining phases run once after the last chunk. Copied
+// columns move host -> device on a copy stream into a ring of device
+// chunk buffers while the previous chunks are scanned. Size expressions
+// see the whole table (`rows`); no phase outside the streamed ones may
+// read the table. Returns like runQuery.
+int runStreamed(QueryContext& qc, PreparedQuery& q, const std::string& table, const std::vector<StreamColumn>& cols,
+                uint64_t rows, uint64_t chunkRows, bool collect, ExecutionResult& out, std::string& err);
 
 std::string describePlan(const PreparedQuery& q);
 

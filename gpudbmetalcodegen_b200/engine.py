@@ -333,6 +333,35 @@ class Context:
                 self._lib.gpudb_result_free(res)
         return out, timing
 
+    def run_streamed(self, spec_or_query, table: str, columns: Sequence[tuple], rows: int, chunk_rows: int,
+                     tune: str = "", collect: bool = True, arrays: bool = False) -> tuple:
+        """Chunked streaming run of a query whose scans of `table` read it
+        from host memory: `columns` are (column, host pointer, element
+        bytes, in_place) tuples over pinned host memory (in_place columns
+        stay on the host and are read over the link by the rows that reach
+        them; the rest are copied a chunk at a time, overlapping the
+        kernels of earlier chunks). Returns (Result|None, Timing)."""
+        q = spec_or_query if isinstance(spec_or_query, Query) else self.prepare(spec_or_query, tune)
+        cols = (_lib.StreamColumn * max(1, len(columns)))()
+        keep = []
+        for i, (name, ptr, elem, in_place) in enumerate(columns):
+            keep.append(name.encode())
+            cols[i] = _lib.StreamColumn(keep[-1], C.c_void_p(ptr), int(elem), int(bool(in_place)))
+        res = C.c_void_p()
+        t = _lib.Timing()
+        st = self._lib.gpudb_query_run_streamed(self.handle, q.handle, table.encode(), cols, len(columns), rows,
+                                                chunk_rows, C.byref(res) if collect else None, C.byref(t))
+        timing = Timing.from_c(t)
+        if st != 0:
+            raise GpudbError(st, _lib.last_error(self.handle))
+        out = None
+        if collect:
+            try:
+                out = _arrays_from_c(res) if arrays else _result_from_c(res)
+            finally:
+                self._lib.gpudb_result_free(res)
+        return out, timing
+
     def collect(self, query: "Query") -> Result:
         """The result the last execution of `query` left in the buffers
         (e.g. the last of many enqueued graph replays), without running it."""

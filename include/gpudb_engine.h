@@ -51,6 +51,32 @@ int gpudb_query_algorithmic_bytes(gpudb_ctx* ctx, gpudb_query* q, long long* byt
 int gpudb_query_run(gpudb_ctx* ctx, gpudb_query* q, int warmup, int measured, gpudb_result** result,
                     gpudb_timing* timing);
 
+/* Chunked streaming execution from host memory (reference: the chunked
+ * path of runCodegenQuery, codegen/codegen_main.cpp:686-808, with
+ * ChunkedColbinTable::loadChunk, registerTableBuffer,
+ * registerTableRowCount and setSkipZeroInit per chunk). The phases before
+ * the first one that scans `table` run once; the phases that scan it run
+ * once per chunk of `chunk_rows` rows and accumulate (zero fills on the
+ * first chunk only); the remaining phases run once after the last chunk.
+ * Copied columns move host -> device on a copy stream into a ring of three
+ * device chunk buffers while earlier chunks are scanned, so the copies
+ * overlap the kernels; in-place columns (pinned, mapped memory) are read
+ * over the host link by late-materialised bindings. Size expressions see
+ * all `rows` rows. No phase outside the streamed ones may read `table`
+ * (stream the unsplit join plan, split=0), and no counter-driven sizing
+ * step may depend on the streamed phases (GPUDB_E_PLAN otherwise). The
+ * streamed columns are unregistered when the call returns. Timing covers
+ * the phases outside the stream. */
+typedef struct gpudb_stream_column {
+    const char* column; /* a column of `table` read by the streamed phases */
+    const void* host;   /* its row 0, in pinned host memory (gpudb_host_alloc) */
+    int32_t elem_bytes;
+    int32_t in_place;   /* 1: read in place over the host link; 0: copied per chunk */
+} gpudb_stream_column;
+int gpudb_query_run_streamed(gpudb_ctx* ctx, gpudb_query* q, const char* table, const gpudb_stream_column* cols,
+                             int ncols, uint64_t rows, uint64_t chunk_rows, gpudb_result** result,
+                             gpudb_timing* timing);
+
 /* Enqueue one execution on the context's stream and return without
  * waiting for it: no timing, no collection. Sizing passes that need a
  * host round trip still wait at their counter reads; a plan without them
