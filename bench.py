@@ -774,9 +774,14 @@ def run_aggmodes(args):
             return {"impl": "reference", "unavailable": "a measurement of the engine's own aggregation strategies only"}
         return None
     torch.cuda.set_device(local)
-    rows = args.zprobe_rows // 2
+    rows = args.agg_rows or args.zprobe_rows // 2
     tables = B.MixTables(rows=rows, zipf_s=(W.ZIPF_S,), nranks=W.MIX_NRANKS, dim_rows=1_000_000, seed=W.SEED)
-    table = autotune.measure_agg_modes(tables, rows)
+    kw = {}
+    if args.agg_cards:
+        kw["cards"] = tuple(int(c) for c in args.agg_cards.split(","))
+    if args.agg_keys:
+        kw["keys"] = tuple(args.agg_keys.split(","))
+    table = autotune.measure_agg_modes(tables, rows, **kw)
     if rank == 0:
         return ({"metric": "group_stage_ms_per_strategy", "value": None, "unit": "ms", "n_gpus": 1,
                           "steps": 3, "warmup": 1, "higher_is_better": False, "dtype": "int64",
@@ -1090,7 +1095,7 @@ def main():
                                                    'tunings) or "search" (the full autotuner search)')
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-chunk-rows", type=int, default=4_000_000,
+    ap.add_argument("--e2e-chunk-rows", type=int, default=8_000_000,
                     help="rows per chunk of the end-to-end streamed run (0: no streamed run)")
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
@@ -1110,6 +1115,9 @@ def main():
     ap.add_argument("--extras-sizer-epochs", type=int, default=30)
     ap.add_argument("--extras-serve-queries", type=int, default=600)
     ap.add_argument("--plain-passes", type=int, default=1)
+    ap.add_argument("--agg-rows", type=int, default=0, help="aggmodes: rows of the query (default half of --zprobe-rows)")
+    ap.add_argument("--agg-cards", default="", help="aggmodes: comma-separated key cardinalities")
+    ap.add_argument("--agg-keys", default="", help="aggmodes: comma-separated key columns (m_rank_u, m_rank_z)")
     ap.add_argument("--batch-tune", default="", help='batch kernels\' launch shape, e.g. "block=512;tile_rows=65536"')
     ap.add_argument("--serve-rows", type=int, default=120_000_000)
     ap.add_argument("--serve-dim-rows", type=int, default=30_000_000)

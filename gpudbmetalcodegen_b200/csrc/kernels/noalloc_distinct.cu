@@ -1,8 +1,7 @@
 // Allocation-free distinct count: gpudb_distinct_count_noalloc().
 //
 // Who needs it: callers that must not allocate device memory on the call
-// path — code that runs while a CUDA graph is being captured (an allocation
-// would break the capture), hosts that hand the GPU to a strict memory
+// path — hosts that hand the GPU to a strict memory
 // budget or their own pool (database buffer managers, JNI/cgo hosts whose
 // allocator owns all device memory), and latency-critical loops where a
 // cudaMalloc/cudaFree round trip (and its implicit synchronisation) is not
@@ -26,8 +25,7 @@
 //     overlap on the GPU (different streams, or different host threads)
 //     race on it and produce wrong counts.
 //   * the first call on a device looks up the scratch array's device
-//     address (cudaGetSymbolAddress) with that device current; make that
-//     first call before starting any stream capture. The address is kept
+//     address (cudaGetSymbolAddress) with that device current. The address is kept
 //     until the process exits: a device reset (cudaDeviceReset, or a
 //     destroyed primary context) leaves it stale, so after one this entry
 //     point must not be called on that device again.

@@ -205,8 +205,8 @@ void gpudb_host_free(void* p);
 
 /* ---- allocation-free distinct count ---------------------------------- */
 /* No counterpart in the reference: an entry point for callers that cannot
- * allocate device memory on the call path (inside CUDA-graph capture, or
- * hosts whose allocator owns all device memory). Counts the distinct values
+ * allocate device memory on the call path (hosts whose own allocator owns
+ * all device memory, strict memory budgets). Counts the distinct values
  * of key[i] % card over rows with filter[i] < thr and writes the count to
  * *out_count (device pointer). For non-negative keys that is the result of
  * the "distinct" pipeline; a negative key is skipped here, where that
@@ -216,8 +216,8 @@ void gpudb_host_free(void* p);
  * static device array sized for card <= 2^22 (512 KiB, held by every GPU
  * that loads the library). card outside [1, 2^22] -> GPUDB_E_INVALID.
  * n = 0 writes 0. Calls share the scratch: calls that overlap on the GPU
- * race. The first call on a device resolves the scratch address and should
- * come before any stream capture; that address is kept for the life of the
+ * race. The first call on a device resolves the scratch address; that
+ * address is kept for the life of the
  * process, so a device reset (cudaDeviceReset, or destroying the primary
  * context) invalidates this entry point for that device. Asynchronous:
  * read *out_count after the stream has completed. */

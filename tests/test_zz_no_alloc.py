@@ -1,9 +1,8 @@
 """Allocation-free distinct count, called through the C-ABI.
 
 Some callers of this library cannot allocate device memory on their call
-path: code that runs while a CUDA graph is being captured, or a host (a
-database buffer manager, a JNI/cgo embedding) whose own allocator owns all
-device memory. For them gpudb_distinct_count_noalloc keeps its scratch
+path: a host (a database buffer manager, a JNI/cgo embedding) whose own
+allocator owns all device memory. For them gpudb_distinct_count_noalloc keeps its scratch
 bitmap in a static device array instead of allocating. This test checks it
 against the allocating "distinct" pipeline (gpudb_query_run) on the same
 device columns, on two calls in a row, and checks that a cardinality above
