@@ -731,7 +731,10 @@ def run_serve(args, pg=None):
         ok_alone = fps[:n_plain] == plain_fp
         ok_all = fps == exact_fp
         verified = verified and ok_alone and ok_all
-        _, prep, _ = S.serve_plain(plain, trace[:n_plain], service_s=service)
+        # the baseline served live, one query at a time, on the same arrivals
+        live_res, prep = S.serve_plain_live(plain, trace[:n_plain])
+        verified = verified and [B.result_fingerprint(r) for r in live_res] == plain_fp
+        del live_res
         launches += 7 * rep.batches
         per_rate.append({"offered_per_s": rate, "ours": rep.summary(),
                          f"plain_one_at_a_time_first_{n_plain}": prep.summary(),

@@ -134,6 +134,28 @@ __device__ __forceinline__ void loadFilters(const int* __restrict__ filter, long
     for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
 }
 
+// Words of rows b, b + step, ... (kUnroll of them) whatever the filter
+// says; rows at or past r1 read as 0.
+template <typename T>
+__device__ __forceinline__ void loadAhead(const T* __restrict__ col, long long b, long long step, long long r1,
+                                          T (&x)[kUnroll]) {
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) x[u] = b + u * step < r1 ? __ldcs(col + b + u * step) : (T)0;
+}
+
+// A warp whose first kUnroll x 32 rows of a work item pass the filter at
+// least one time in four reads its dependent columns unconditionally, one
+// iteration ahead with the filter words: at that selectivity nearly every
+// 32-byte sector of those columns is needed anyway (each holds 4-8 rows),
+// and the loads no longer wait for the filter. Sparser warps keep
+// filter-guarded loads. Called by whole warps.
+__device__ __forceinline__ bool denseWarp(const int (&f)[kUnroll], int thr) {
+    int pass = 0;
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) pass += __popc(__ballot_sync(0xffffffffu, f[u] < thr));
+    return 4 * pass >= 32 * kUnroll;
+}
+
 // CTA-wide work pull; returns -1 when the list is exhausted.
 __device__ __forceinline__ long long pullWork(unsigned long long* counter, long long total, long long* s_item) {
     __syncthreads();
@@ -249,7 +271,38 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
         // the current rows' dependent loads are in flight
         int fn[kUnroll];
         loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
-        if (q.tmpl == GPUDB_TPL_JOIN) {
+        const bool dense = denseWarp(fn, thr);
+        if (q.tmpl == GPUDB_TPL_JOIN && dense) {
+            // most rows pass: fk and value ride along with the filter words
+            const int* __restrict__ fk = q.fk;
+            const unsigned* __restrict__ bm = q.bitmap;
+            const long long words = q.bitmap_words;
+            int kn[kUnroll];
+            long long vn[kUnroll];
+            loadAhead(fk, r0 + threadIdx.x, step, r1, kn);
+            loadAhead(value, r0 + threadIdx.x, step, r1, vn);
+            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
+                int f[kUnroll], key[kUnroll];
+                long long v[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    f[u] = fn[u];
+                    key[u] = kn[u];
+                    v[u] = vn[u];
+                }
+                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
+                loadAhead(fk, b + kUnroll * step, step, r1, kn);
+                loadAhead(value, b + kUnroll * step, step, r1, vn);
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const long long k = key[u];
+                    if (f[u] < thr && k >= 0 && (k >> 5) < words && gpudb_bitmap_test(bm, k)) {
+                        ++c;
+                        s += v[u];
+                    }
+                }
+            }
+        } else if (q.tmpl == GPUDB_TPL_JOIN) {
             const int* __restrict__ fk = q.fk;
             const unsigned* __restrict__ bm = q.bitmap;
             const long long words = q.bitmap_words;
@@ -269,6 +322,26 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
                         s += __ldcs(value + b + u * step);
                     }
                 }
+            }
+        } else if (dense) {
+            long long vn[kUnroll];
+            loadAhead(value, r0 + threadIdx.x, step, r1, vn);
+            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
+                int f[kUnroll];
+                long long v[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    f[u] = fn[u];
+                    v[u] = vn[u];
+                }
+                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
+                loadAhead(value, b + kUnroll * step, step, r1, vn);
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u)
+                    if (f[u] < thr) {
+                        ++c;
+                        s += v[u];
+                    }
             }
         } else {
             for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
@@ -349,28 +422,40 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const int log2cap = q.log2cap;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
-        int fn[kUnroll];
+        int fn[kUnroll], kn[kUnroll];
         loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
+        const bool dense = denseWarp(fn, thr);
+        if (dense) loadAhead(keyc, r0 + threadIdx.x, step, r1, kn);
         for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
             int f[kUnroll], kr[kUnroll];
             long long v[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
             loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
+            if (dense) {
+                // most rows pass: the keys were loaded with the filter words,
+                // the values go out together with the next ones
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                const bool p = f[u] < thr;
-                kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
-                v[u] = p ? __ldcs(value + b + u * step) : 0;
+                for (int u = 0; u < kUnroll; ++u) kr[u] = kn[u];
+                loadAhead(value, b, step, r1, v);
+                loadAhead(keyc, b + kUnroll * step, step, r1, kn);
+            } else {
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const bool p = f[u] < thr;
+                    kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
+                    v[u] = p ? __ldcs(value + b + u * step) : 0;
+                }
             }
             unsigned enc[kUnroll];
             bool live[kUnroll];
-            unsigned long long c[kUnroll], val[kUnroll];
+            unsigned c[kUnroll];  // rows a lane adds for its group: at most a warp's
+            unsigned long long val[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
                 live[u] = f[u] < thr;
                 enc[u] = live[u] ? encKey(keyMod(kr[u], q), card) : 0u;
-                c[u] = 1ull;
+                c[u] = 1u;
                 val[u] = (unsigned long long)v[u];
             }
             if (mode == GPUDB_AGG_SHARED_DIRECT) {
@@ -392,50 +477,50 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                     if (!live[u]) continue;
                     const unsigned am = __activemask();
                     const unsigned peers = __match_any_sync(am, enc[u]);
-                    c[u] = (unsigned long long)__popc(peers);  // every peer is one live row
+                    c[u] = (unsigned)__popc(peers);  // every peer is one live row
                     val[u] = gpudb_peer_sum(am, peers, val[u]);
                     live[u] = (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
                 }
             }
             if (mode == GPUDB_AGG_SHARED) {
+                // the shared table first; what it cannot hold goes on below
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
                     if (!live[u]) continue;
                     unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], 11);
-                    bool done = false;
 #pragma unroll 1
                     for (int p = 0; p < kSmemProbe; ++p) {
                         unsigned cur = vKey[h];
                         if (cur == 0u) cur = atomicCAS(&sKey[h], 0u, enc[u]) == 0u ? enc[u] : vKey[h];
                         if (cur == enc[u]) {
-                            gpudb_red_add_shared_u32(&sCnt[h], (unsigned)c[u]);
+                            gpudb_red_add_shared_u32(&sCnt[h], c[u]);
                             gpudb_red_add_shared_u64(&sSum[h], val[u]);
-                            done = true;
+                            live[u] = false;
                             break;
                         }
                         h = (h + 1u) & (kSmemSlots - 1);
                     }
-                    if (!done) globalAdd(q, true, enc[u], c[u], val[u]);
                 }
-            } else {
-                unsigned long long s0[kUnroll];
-                unsigned cur[kUnroll];
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    s0[u] = gpudb_hash_slot((unsigned long long)enc[u], log2cap);
-                    cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
-                }
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
-                        gpudb_red_add_u32(&ht[s0[u]].count, (unsigned)c[u]);
-                        gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
-                        live[u] = false;
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
             }
+            // the global table: the home-slot key words of a thread's rows
+            // are loaded together, so an existing group costs one L2 round
+            // trip per kUnroll rows, then fire-and-forget reductions
+            unsigned s0[kUnroll], cur[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                s0[u] = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], log2cap);
+                cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
+                    gpudb_red_add_u32(&ht[s0[u]].count, c[u]);
+                    gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
+                    live[u] = false;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
         }
         if (mode == GPUDB_AGG_SHARED || mode == GPUDB_AGG_SHARED_DIRECT) heldQ = qd;
     }

@@ -213,6 +213,30 @@ class Server:
         return results, rep
 
 
+def serve_plain_live(plain: B.PlainRunner, trace: Sequence[Request]):
+    """The one-query-at-a-time baseline, live: one server thread replays
+    `trace` in real time, each request waiting for its arrival and for the
+    request before it, then running alone through the plain engine path.
+    Latency = completion - arrival on the host clock."""
+    import torch
+    n = len(trace)
+    results, done = [], np.zeros(n)
+    t0 = time.perf_counter()
+    for k, r in enumerate(trace):
+        wait = r.arrival - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        results.append(plain.run(r.query))
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+        done[k] = time.perf_counter() - t0
+    lat = done - np.array([r.arrival for r in trace])
+    rate = n / trace[-1].arrival if n and trace[-1].arrival > 0 else 0.0
+    rep = ServeReport(rate=rate, requests=n, wall_s=float(done.max()) if n else 0.0, latencies_s=lat,
+                      batches=n, batch_sizes=[1] * n)
+    return results, rep
+
+
 def serve_plain(plain: B.PlainRunner, trace: Sequence[Request], service_s: Optional[np.ndarray] = None):
     """The one-query-at-a-time baseline: every request runs alone through
     the plain engine path, in arrival order behind one FIFO queue. Service

@@ -37,3 +37,20 @@ def test_fifo_queue_of_the_plain_baseline():
     assert np.allclose(rep.latencies_s, [0.15, 0.20, 0.25, 0.05])
     s = rep.summary()
     assert s["requests"] == 4 and s["p50_ms"] == pytest.approx(175.0)
+
+
+def test_live_plain_baseline_waits_for_arrivals_and_queues():
+    import time
+
+    class Slow:  # a plain path whose every query takes 30 ms
+        def run(self, q):
+            time.sleep(0.03)
+            return ("scalar", 1, q.thr)
+
+    qs = [B.MixQuery("agg", 0, 0, 10, t) for t in (1, 2, 3)]
+    tr = [S.Request(i, q, a) for i, (q, a) in enumerate(zip(qs, [0.0, 0.01, 0.2]))]
+    res, rep = S.serve_plain_live(Slow(), tr)
+    assert [r[2] for r in res] == [1, 2, 3]  # arrival order
+    lat = rep.latencies_s
+    # the second request queues behind the first; the third arrives to an idle server
+    assert 0.03 <= lat[0] < 0.06 and 0.05 <= lat[1] < 0.09 and 0.03 <= lat[2] < 0.06
