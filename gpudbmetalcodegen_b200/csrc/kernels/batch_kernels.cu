@@ -422,30 +422,21 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const int log2cap = q.log2cap;
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
-        int fn[kUnroll], kn[kUnroll];
+        // (the dense-warp loads of kAgg measured no faster here: this
+        // kernel's time goes to the aggregation, and the extra registers spill)
+        int fn[kUnroll];
         loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
-        const bool dense = denseWarp(fn, thr);
-        if (dense) loadAhead(keyc, r0 + threadIdx.x, step, r1, kn);
         for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
             int f[kUnroll], kr[kUnroll];
             long long v[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
             loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
-            if (dense) {
-                // most rows pass: the keys were loaded with the filter words,
-                // the values go out together with the next ones
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) kr[u] = kn[u];
-                loadAhead(value, b, step, r1, v);
-                loadAhead(keyc, b + kUnroll * step, step, r1, kn);
-            } else {
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    const bool p = f[u] < thr;
-                    kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
-                    v[u] = p ? __ldcs(value + b + u * step) : 0;
-                }
+            for (int u = 0; u < kUnroll; ++u) {
+                const bool p = f[u] < thr;
+                kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
+                v[u] = p ? __ldcs(value + b + u * step) : 0;
             }
             unsigned enc[kUnroll];
             bool live[kUnroll];
@@ -483,11 +474,11 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 }
             }
             if (mode == GPUDB_AGG_SHARED) {
-                // the shared table first; what it cannot hold goes on below
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
                     if (!live[u]) continue;
                     unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], 11);
+                    bool done = false;
 #pragma unroll 1
                     for (int p = 0; p < kSmemProbe; ++p) {
                         unsigned cur = vKey[h];
@@ -495,32 +486,35 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                         if (cur == enc[u]) {
                             gpudb_red_add_shared_u32(&sCnt[h], c[u]);
                             gpudb_red_add_shared_u64(&sSum[h], val[u]);
-                            live[u] = false;
+                            done = true;
                             break;
                         }
                         h = (h + 1u) & (kSmemSlots - 1);
                     }
+                    // (spills one at a time: batching their home-slot loads
+                    // as the global path does measured slower, its extra
+                    // registers spilling)
+                    if (!done) globalAdd(q, true, enc[u], c[u], val[u]);
                 }
-            }
-            // the global table: the home-slot key words of a thread's rows
-            // are loaded together, so an existing group costs one L2 round
-            // trip per kUnroll rows, then fire-and-forget reductions
-            unsigned s0[kUnroll], cur[kUnroll];
+            } else {
+                unsigned long long s0[kUnroll];
+                unsigned cur[kUnroll];
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                s0[u] = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], log2cap);
-                cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
-                    gpudb_red_add_u32(&ht[s0[u]].count, c[u]);
-                    gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
-                    live[u] = false;
+                for (int u = 0; u < kUnroll; ++u) {
+                    s0[u] = gpudb_hash_slot((unsigned long long)enc[u], log2cap);
+                    cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
+                for (int u = 0; u < kUnroll; ++u) {
+                    if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
+                        gpudb_red_add_u32(&ht[s0[u]].count, c[u]);
+                        gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
+                        live[u] = false;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
+            }
         }
         if (mode == GPUDB_AGG_SHARED || mode == GPUDB_AGG_SHARED_DIRECT) heldQ = qd;
     }
