@@ -703,6 +703,10 @@ def run_serve(args, pg=None):
         compile_s.append(time.perf_counter() - t)
     plain_res, _, service = S.serve_plain(plain, S.poisson_trace(qs[:n_plain], rate=rates[0], seed=11))
     plain_fp = [B.result_fingerprint(r) for r in plain_res]
+    # the answers hold pinned buffers of the shared pool: hand them back
+    # before serving, or the server's first large results would have to
+    # page-lock fresh memory (tens of ms) while requests wait
+    del plain_res
     # every served answer is also checked against one exact-sized batch of all queries
     ex = B.BatchRunner(tables, sizing="exact", plain=plain)
     exact_res, _ = ex.run(qs)
@@ -784,7 +788,7 @@ def run_aggmodes(args):
         kw["cards"] = tuple(int(c) for c in args.agg_cards.split(","))
     if args.agg_keys:
         kw["keys"] = tuple(args.agg_keys.split(","))
-    table = autotune.measure_agg_modes(tables, rows, **kw)
+    table = autotune.measure_agg_modes(tables, rows, tuning=batch_tuning(args), **kw)
     if rank == 0:
         return ({"metric": "group_stage_ms_per_strategy", "value": None, "unit": "ms", "n_gpus": 1,
                           "steps": 3, "warmup": 1, "higher_is_better": False, "dtype": "int64",

@@ -178,6 +178,7 @@ _SIGNATURES = [
     ("gpudb_batch_set_groups", C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
     ("gpudb_batch_set_agg_mode", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("gpudb_batch_set_tuning", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("gpudb_batch_set_option", C.c_int, [C.c_void_p, C.c_char_p, C.c_longlong]),
     ("gpudb_batch_execute", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     ("gpudb_batch_exact_stats", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
     ("gpudb_batch_features", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),

@@ -74,6 +74,7 @@ BATCH_SPACE = {
     "block": [512, 256, 1024],
     "tile_rows": [16384, 4096, 65536, 262144],
     "warp_aggregate": [True, False],
+    "group_rows": [4, 2],
 }
 
 
@@ -271,7 +272,8 @@ def tune_batch(runner_factory: Callable[[dict], object], queries, space: Optiona
 
 
 def measure_agg_modes(tables, rows: int, cards=(16, 256, 1024, 8192, 65536, 524288, 4194304),
-                      keys=("m_rank_u", "m_rank_z"), thr: int = 5000, reps: int = 3) -> List[dict]:
+                      keys=("m_rank_u", "m_rank_z"), thr: int = 5000, reps: int = 3,
+                      tuning: Optional[dict] = None) -> List[dict]:
     """Device time of the batched group-by stage for one query of `rows`
     rows per aggregation strategy, over key cardinalities and key skew
     (uniform m_rank_u / Zipf m_rank_z): the measurements behind the
@@ -288,6 +290,8 @@ def measure_agg_modes(tables, rows: int, cards=(16, 256, 1024, 8192, 65536, 5242
             for mode, name in modes:
                 b = B.Batch()
                 try:
+                    if tuning:
+                        b.set_tuning(**tuning)
                     b.set_queries([tables.query_struct(q)])
                     _, d, _ = b.exact_stats()
                     b.set_groups(0, max(1, int(d[0])))

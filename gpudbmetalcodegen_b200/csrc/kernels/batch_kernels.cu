@@ -128,10 +128,11 @@ __device__ __forceinline__ int findQuery(const WorkList& wl, long long w) {
 
 // Filter words of rows b, b + step, ... (kUnroll of them); rows at or past
 // r1 read as `thr`, which no row passes.
+template <int N>
 __device__ __forceinline__ void loadFilters(const int* __restrict__ filter, long long b, long long step, long long r1,
-                                            int thr, int (&f)[kUnroll]) {
+                                            int thr, int (&f)[N]) {
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
+    for (int u = 0; u < N; ++u) f[u] = b + u * step < r1 ? __ldcs(filter + b + u * step) : thr;
 }
 
 // Words of rows b, b + step, ... (kUnroll of them) whatever the filter
@@ -364,14 +365,18 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
 // ---- GROUPBY / TOPK: filter -> key % card -> hash table (count, sum) -------
 // Per query, the strategy the host picked from the expected group count and
 // the sample's key repetition:
-//   SHARED      warp aggregation, then the CTA's shared-memory table (flushed
-//               to the global table at the end of the work item);
+//   SHARED_DIRECT the CTA's shared table indexed by the key itself;
+//   SHARED      warp aggregation, then the CTA's hashed shared table;
 //   GLOBAL_WARP warp aggregation, then the global table;
 //   GLOBAL      the global table directly.
-// On the global path the home-slot key words of a thread's kUnroll rows are
-// loaded together, so an existing group costs one L2 round trip per
-// kUnroll rows, then fire-and-forget atomics.
-__global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
+// A CTA keeps its shared table across a query's work items and flushes it
+// into the query's global table when it moves to another query or runs out
+// of work. On the global path the home-slot key words of a thread's U rows
+// are loaded together, so an existing group costs one L2 round trip per U
+// rows, then fire-and-forget reductions. U = 4 rows per thread, or U = 2 at
+// a 42-register cap and 1.5x the resident threads (blocks of <= 512).
+template <int U>
+__global__ void __launch_bounds__(U == 2 ? 512 : 1024, U == 2 ? 3 : 1) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
                                                unsigned long long* counter) {
     __shared__ long long s_item;
     __shared__ unsigned sKey[kSmemSlots];
@@ -424,26 +429,26 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
         const long long step = (long long)blockDim.x;
         // (the dense-warp loads of kAgg measured no faster here: this
         // kernel's time goes to the aggregation, and the extra registers spill)
-        int fn[kUnroll];
+        int fn[U];
         loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
-        for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
-            int f[kUnroll], kr[kUnroll];
-            long long v[kUnroll];
+        for (long long b = r0 + threadIdx.x; b < r1; b += U * step) {
+            int f[U], kr[U];
+            long long v[U];
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
-            loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
+            for (int u = 0; u < U; ++u) f[u] = fn[u];
+            loadFilters(filter, b + U * step, step, r1, thr, fn);
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const bool p = f[u] < thr;
                 kr[u] = p ? __ldcs(keyc + b + u * step) : 0;
                 v[u] = p ? __ldcs(value + b + u * step) : 0;
             }
-            unsigned enc[kUnroll];
-            bool live[kUnroll];
-            unsigned c[kUnroll];  // rows a lane adds for its group: at most a warp's
-            unsigned long long val[kUnroll];
+            unsigned enc[U];
+            bool live[U];
+            unsigned c[U];  // rows a lane adds for its group: at most a warp's
+            unsigned long long val[U];
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
+            for (int u = 0; u < U; ++u) {
                 live[u] = f[u] < thr;
                 enc[u] = live[u] ? encKey(keyMod(kr[u], q), card) : 0u;
                 c[u] = 1u;
@@ -455,7 +460,7 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                 // (same-slot lanes of one warp serialise in the shared
                 // atomic unit, cheaper than a match and two peer sums)
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     if (!live[u]) continue;
                     gpudb_red_add_shared_u32(&sCnt[enc[u] - 1u], 1u);
                     gpudb_red_add_shared_u64(&sSum[enc[u] - 1u], val[u]);
@@ -464,7 +469,7 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
             }
             if (mode != GPUDB_AGG_GLOBAL) {
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     if (!live[u]) continue;
                     const unsigned am = __activemask();
                     const unsigned peers = __match_any_sync(am, enc[u]);
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
             }
             if (mode == GPUDB_AGG_SHARED) {
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     if (!live[u]) continue;
                     unsigned h = (unsigned)gpudb_hash_slot((unsigned long long)enc[u], 11);
                     bool done = false;
@@ -497,15 +502,15 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                     if (!done) globalAdd(q, true, enc[u], c[u], val[u]);
                 }
             } else {
-                unsigned long long s0[kUnroll];
-                unsigned cur[kUnroll];
+                unsigned long long s0[U];
+                unsigned cur[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     s0[u] = gpudb_hash_slot((unsigned long long)enc[u], log2cap);
                     cur[u] = live[u] ? *((volatile unsigned*)&ht[s0[u]].key) : 0u;
                 }
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     if (live[u] && cur[u] == enc[u]) {  // the group exists in its home slot
                         gpudb_red_add_u32(&ht[s0[u]].count, c[u]);
                         gpudb_red_add_u64(&ht[s0[u]].sum, val[u]);
@@ -513,7 +518,7 @@ __global__ void __launch_bounds__(1024) kGroup(const QDesc* __restrict__ qs, Wor
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
+                for (int u = 0; u < U; ++u) globalAddFrom(q, live[u], enc[u], s0[u], cur[u], c[u], val[u]);
             }
         }
         if (mode == GPUDB_AGG_SHARED || mode == GPUDB_AGG_SHARED_DIRECT) heldQ = qd;
@@ -833,6 +838,7 @@ struct gpudb_batch {
     cudaStream_t stream = nullptr;
     int numSMs = 148;
     int block = 512, maxProbe = 128, warpAgg = 1;
+    int groupRows = 4;  // rows in flight per thread of the group-by kernel (4, or 2 at twice the occupancy)
     long long tile = 16384;
     std::vector<gpudb_batch_query> queries;
     std::vector<QDesc> desc;
@@ -1046,8 +1052,12 @@ int enqueue(gpudb_batch* b, bool stages) {
     }
     mark(3);
     if (b->wlGroup.nq) {
-        kGroup<<<gridFor(b, (const void*)kGroup, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlGroup, b->tile,
-                                                                                      b->counters + 2);
+        if (b->groupRows == 2 && b->block <= 512)  // the 2-row form is built for blocks of <= 512
+            kGroup<2><<<gridFor(b, (const void*)kGroup<2>, b->block), b->block, 0, b->stream>>>(
+                b->dDesc, b->wlGroup, b->tile, b->counters + 2);
+        else
+            kGroup<4><<<gridFor(b, (const void*)kGroup<4>, b->block), b->block, 0, b->stream>>>(
+                b->dDesc, b->wlGroup, b->tile, b->counters + 2);
         launches++;
     }
     mark(4);
@@ -1194,6 +1204,22 @@ int gpudb_batch_set_agg_mode(gpudb_batch* b, int qi, int mode) {
         b->dirty = true;
     }
     return GPUDB_OK;
+}
+
+int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value) {
+    if (!b || !name) return GPUDB_E_INVALID;
+    const std::string n(name);
+    if (n == "group_rows") {
+        if (value != 2 && value != 4) {
+            gpudb::setThreadError("group_rows must be 2 or 4");
+            return GPUDB_E_INVALID;
+        }
+        b->groupRows = (int)value;
+        b->dirty = true;
+        return GPUDB_OK;
+    }
+    gpudb::setThreadError("unknown batch option '" + n + "'");
+    return GPUDB_E_INVALID;
 }
 
 int gpudb_batch_set_tuning(gpudb_batch* b, int block, int tile_rows, int warp_aggregate, int max_probe) {
