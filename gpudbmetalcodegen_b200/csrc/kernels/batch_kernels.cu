@@ -373,10 +373,11 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
 // into the query's global table when it moves to another query or runs out
 // of work. On the global path the home-slot key words of a thread's U rows
 // are loaded together, so an existing group costs one L2 round trip per U
-// rows, then fire-and-forget reductions. U = 4 rows per thread, or U = 2 at
-// a 42-register cap and 1.5x the resident threads (blocks of <= 512).
+// rows, then fire-and-forget reductions. U = 2 rows per thread at a
+// 42-register cap (the default), U = 4 at 64 registers, U = 1 at 32
+// registers (U < 4: blocks of at most 512 threads).
 template <int U>
-__global__ void __launch_bounds__(U == 2 ? 512 : 1024, U == 2 ? 3 : 1) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
+__global__ void __launch_bounds__(U == 4 ? 1024 : 512, U == 4 ? 1 : (U == 2 ? 3 : 4)) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
                                                unsigned long long* counter) {
     __shared__ long long s_item;
     __shared__ unsigned sKey[kSmemSlots];
@@ -838,7 +839,10 @@ struct gpudb_batch {
     cudaStream_t stream = nullptr;
     int numSMs = 148;
     int block = 512, maxProbe = 128, warpAgg = 1;
-    int groupRows = 4;  // rows in flight per thread of the group-by kernel (4, or 2 at twice the occupancy)
+    // rows in flight per thread of the group-by kernel: 2 (measured fastest:
+    // its latency-bound aggregation gains more from 1.5x the resident
+    // threads than it loses to a few spilled registers), 4 or 1
+    int groupRows = 2;
     long long tile = 16384;
     std::vector<gpudb_batch_query> queries;
     std::vector<QDesc> desc;
@@ -1052,8 +1056,12 @@ int enqueue(gpudb_batch* b, bool stages) {
     }
     mark(3);
     if (b->wlGroup.nq) {
-        if (b->groupRows == 2 && b->block <= 512)  // the 2-row form is built for blocks of <= 512
+        // the 1- and 2-row forms are built for blocks of at most 512 threads
+        if (b->groupRows == 2 && b->block <= 512)
             kGroup<2><<<gridFor(b, (const void*)kGroup<2>, b->block), b->block, 0, b->stream>>>(
+                b->dDesc, b->wlGroup, b->tile, b->counters + 2);
+        else if (b->groupRows == 1 && b->block <= 512)
+            kGroup<1><<<gridFor(b, (const void*)kGroup<1>, b->block), b->block, 0, b->stream>>>(
                 b->dDesc, b->wlGroup, b->tile, b->counters + 2);
         else
             kGroup<4><<<gridFor(b, (const void*)kGroup<4>, b->block), b->block, 0, b->stream>>>(
@@ -1210,8 +1218,8 @@ int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value) {
     if (!b || !name) return GPUDB_E_INVALID;
     const std::string n(name);
     if (n == "group_rows") {
-        if (value != 2 && value != 4) {
-            gpudb::setThreadError("group_rows must be 2 or 4");
+        if (value != 1 && value != 2 && value != 4) {
+            gpudb::setThreadError("group_rows must be 1, 2 or 4");
             return GPUDB_E_INVALID;
         }
         b->groupRows = (int)value;
