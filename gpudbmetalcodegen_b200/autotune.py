@@ -74,7 +74,7 @@ BATCH_SPACE = {
     "block": [512, 256, 1024],
     "tile_rows": [16384, 4096, 65536, 262144],
     "warp_aggregate": [True, False],
-    "group_rows": [2, 4, 1],
+    "group_rows": [1, 2, 4],
 }
 
 

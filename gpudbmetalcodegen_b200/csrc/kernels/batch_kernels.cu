@@ -373,9 +373,9 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
 // into the query's global table when it moves to another query or runs out
 // of work. On the global path the home-slot key words of a thread's U rows
 // are loaded together, so an existing group costs one L2 round trip per U
-// rows, then fire-and-forget reductions. U = 2 rows per thread at a
-// 42-register cap (the default), U = 4 at 64 registers, U = 1 at 32
-// registers (U < 4: blocks of at most 512 threads).
+// rows, then fire-and-forget reductions. U = 1 row per thread at a
+// 32-register cap (the default: every thread slot of the SM resident),
+// U = 2 at 42 registers, U = 4 at 64 (U < 4: blocks of at most 512).
 template <int U>
 __global__ void __launch_bounds__(U == 4 ? 1024 : 512, U == 4 ? 1 : (U == 2 ? 3 : 4)) kGroup(const QDesc* __restrict__ qs, WorkList wl, long long tile,
                                                unsigned long long* counter) {
@@ -839,10 +839,11 @@ struct gpudb_batch {
     cudaStream_t stream = nullptr;
     int numSMs = 148;
     int block = 512, maxProbe = 128, warpAgg = 1;
-    // rows in flight per thread of the group-by kernel: 2 (measured fastest:
-    // its latency-bound aggregation gains more from 1.5x the resident
-    // threads than it loses to a few spilled registers), 4 or 1
-    int groupRows = 2;
+    // rows in flight per thread of the group-by kernel: 1 (measured fastest
+    // on the mixed batch: its latency-bound aggregation gains more from
+    // twice the resident threads than it loses to a few spilled
+    // registers), 2 or 4
+    int groupRows = 1;
     long long tile = 16384;
     std::vector<gpudb_batch_query> queries;
     std::vector<QDesc> desc;

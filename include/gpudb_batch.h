@@ -108,8 +108,8 @@ int gpudb_batch_set_agg_mode(gpudb_batch* b, int q, int agg_mode);
  * aggregation (0 turns GLOBAL_WARP into GLOBAL), hash probe bound. */
 int gpudb_batch_set_tuning(gpudb_batch* b, int block, int tile_rows, int warp_aggregate, int max_probe);
 /* Named tuning options beyond those: "group_rows" = rows in flight per
- * thread of the group-by kernel: 2 (default; a 42-register cap), 4 (64
- * registers) or 1 (32 registers); blocks of more than 512 threads use 4.
+ * thread of the group-by kernel: 1 (default; a 32-register cap), 2 (42
+ * registers) or 4 (64 registers); blocks of more than 512 threads use 4.
  * GPUDB_E_INVALID for an unknown name or value. */
 int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value);
 /* Run every query; per-query device error words go to errors[n] (bit
