@@ -75,6 +75,7 @@ BATCH_SPACE = {
     "tile_rows": [16384, 4096, 65536, 262144],
     "warp_aggregate": [True, False],
     "group_rows": [1, 2, 4],
+    "agg_rows": [4, 2],
 }
 
 

@@ -380,9 +380,10 @@ class Batch:
         check(self._lib.gpudb_batch_set_agg_mode(self.handle, i, int(mode)))
 
     def set_tuning(self, block: int = 512, tile_rows: int = 16384, warp_aggregate: bool = True,
-                   max_probe: int = 128, group_rows: int = 1) -> None:
+                   max_probe: int = 128, group_rows: int = 1, agg_rows: int = 4) -> None:
         check(self._lib.gpudb_batch_set_tuning(self.handle, block, tile_rows, int(warp_aggregate), max_probe))
         check(self._lib.gpudb_batch_set_option(self.handle, b"group_rows", group_rows))
+        check(self._lib.gpudb_batch_set_option(self.handle, b"agg_rows", agg_rows))
 
     def execute(self, use_graph: bool = True) -> Tuple[float, np.ndarray]:
         ms = C.c_double()

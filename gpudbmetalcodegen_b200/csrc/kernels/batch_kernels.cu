@@ -137,11 +137,11 @@ __device__ __forceinline__ void loadFilters(const int* __restrict__ filter, long
 
 // Words of rows b, b + step, ... (kUnroll of them) whatever the filter
 // says; rows at or past r1 read as 0.
-template <typename T>
+template <typename T, int N>
 __device__ __forceinline__ void loadAhead(const T* __restrict__ col, long long b, long long step, long long r1,
-                                          T (&x)[kUnroll]) {
+                                          T (&x)[N]) {
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) x[u] = b + u * step < r1 ? __ldcs(col + b + u * step) : (T)0;
+    for (int u = 0; u < N; ++u) x[u] = b + u * step < r1 ? __ldcs(col + b + u * step) : (T)0;
 }
 
 // A warp whose first kUnroll x 32 rows of a work item pass the filter at
@@ -150,11 +150,12 @@ __device__ __forceinline__ void loadAhead(const T* __restrict__ col, long long b
 // 32-byte sector of those columns is needed anyway (each holds 4-8 rows),
 // and the loads no longer wait for the filter. Sparser warps keep
 // filter-guarded loads. Called by whole warps.
-__device__ __forceinline__ bool denseWarp(const int (&f)[kUnroll], int thr) {
+template <int N>
+__device__ __forceinline__ bool denseWarp(const int (&f)[N], int thr) {
     int pass = 0;
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) pass += __popc(__ballot_sync(0xffffffffu, f[u] < thr));
-    return 4 * pass >= 32 * kUnroll;
+    for (int u = 0; u < N; ++u) pass += __popc(__ballot_sync(0xffffffffu, f[u] < thr));
+    return 4 * pass >= 32 * N;
 }
 
 // CTA-wide work pull; returns -1 when the list is exhausted.
@@ -255,7 +256,8 @@ __global__ void __launch_bounds__(1024) kJoinBuild(const QDesc* __restrict__ qs,
 }
 
 // ---- AGG / JOIN probe: filter [-> semi-join] -> count + sum ---------------
-__global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkList wl, long long tile, unsigned long long* counter) {
+template <int U>
+__global__ void __launch_bounds__(U == 4 ? 1024 : 512, U == 4 ? 1 : 4) kAgg(const QDesc* __restrict__ qs, WorkList wl, long long tile, unsigned long long* counter) {
     __shared__ long long s_item;
     __shared__ long long red[64];
     const long long total = __ldg(wl.prefix + wl.nq);
@@ -268,9 +270,9 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
         const long long r0 = (w - __ldg(wl.prefix + qi)) * tile, r1 = min(q.rows, r0 + tile);
         const long long step = (long long)blockDim.x;
         long long c = 0, s = 0;
-        // the filter words of a thread's next kUnroll rows are loaded while
+        // the filter words of a thread's next U rows are loaded while
         // the current rows' dependent loads are in flight
-        int fn[kUnroll];
+        int fn[U];
         loadFilters(filter, r0 + threadIdx.x, step, r1, thr, fn);
         const bool dense = denseWarp(fn, thr);
         if (q.tmpl == GPUDB_TPL_JOIN && dense) {
@@ -278,24 +280,24 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
             const int* __restrict__ fk = q.fk;
             const unsigned* __restrict__ bm = q.bitmap;
             const long long words = q.bitmap_words;
-            int kn[kUnroll];
-            long long vn[kUnroll];
+            int kn[U];
+            long long vn[U];
             loadAhead(fk, r0 + threadIdx.x, step, r1, kn);
             loadAhead(value, r0 + threadIdx.x, step, r1, vn);
-            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
-                int f[kUnroll], key[kUnroll];
-                long long v[kUnroll];
+            for (long long b = r0 + threadIdx.x; b < r1; b += U * step) {
+                int f[U], key[U];
+                long long v[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     f[u] = fn[u];
                     key[u] = kn[u];
                     v[u] = vn[u];
                 }
-                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
-                loadAhead(fk, b + kUnroll * step, step, r1, kn);
-                loadAhead(value, b + kUnroll * step, step, r1, vn);
+                loadFilters(filter, b + U * step, step, r1, thr, fn);
+                loadAhead(fk, b + U * step, step, r1, kn);
+                loadAhead(value, b + U * step, step, r1, vn);
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     const long long k = key[u];
                     if (f[u] < thr && k >= 0 && (k >> 5) < words && gpudb_bitmap_test(bm, k)) {
                         ++c;
@@ -307,16 +309,16 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
             const int* __restrict__ fk = q.fk;
             const unsigned* __restrict__ bm = q.bitmap;
             const long long words = q.bitmap_words;
-            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
-                int f[kUnroll];
+            for (long long b = r0 + threadIdx.x; b < r1; b += U * step) {
+                int f[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
-                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
-                int key[kUnroll];
+                for (int u = 0; u < U; ++u) f[u] = fn[u];
+                loadFilters(filter, b + U * step, step, r1, thr, fn);
+                int key[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) key[u] = f[u] < thr ? __ldcs(fk + b + u * step) : -1;
+                for (int u = 0; u < U; ++u) key[u] = f[u] < thr ? __ldcs(fk + b + u * step) : -1;
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     const long long k = key[u];
                     if (k >= 0 && (k >> 5) < words && gpudb_bitmap_test(bm, k)) {
                         ++c;
@@ -325,33 +327,33 @@ __global__ void __launch_bounds__(1024) kAgg(const QDesc* __restrict__ qs, WorkL
                 }
             }
         } else if (dense) {
-            long long vn[kUnroll];
+            long long vn[U];
             loadAhead(value, r0 + threadIdx.x, step, r1, vn);
-            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
-                int f[kUnroll];
-                long long v[kUnroll];
+            for (long long b = r0 + threadIdx.x; b < r1; b += U * step) {
+                int f[U];
+                long long v[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     f[u] = fn[u];
                     v[u] = vn[u];
                 }
-                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
-                loadAhead(value, b + kUnroll * step, step, r1, vn);
+                loadFilters(filter, b + U * step, step, r1, thr, fn);
+                loadAhead(value, b + U * step, step, r1, vn);
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
+                for (int u = 0; u < U; ++u)
                     if (f[u] < thr) {
                         ++c;
                         s += v[u];
                     }
             }
         } else {
-            for (long long b = r0 + threadIdx.x; b < r1; b += kUnroll * step) {
-                int f[kUnroll];
+            for (long long b = r0 + threadIdx.x; b < r1; b += U * step) {
+                int f[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) f[u] = fn[u];
-                loadFilters(filter, b + kUnroll * step, step, r1, thr, fn);
+                for (int u = 0; u < U; ++u) f[u] = fn[u];
+                loadFilters(filter, b + U * step, step, r1, thr, fn);
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
+                for (int u = 0; u < U; ++u)
                     if (f[u] < thr) {
                         ++c;
                         s += __ldcs(value + b + u * step);
@@ -844,6 +846,7 @@ struct gpudb_batch {
     // twice the resident threads than it loses to a few spilled
     // registers), 2 or 4
     int groupRows = 1;
+    int aggRows = 4;  // rows in flight per thread of the agg / join kernel: 4 (64 registers) or 2 (32)
     long long tile = 16384;
     std::vector<gpudb_batch_query> queries;
     std::vector<QDesc> desc;
@@ -1051,8 +1054,12 @@ int enqueue(gpudb_batch* b, bool stages) {
     }
     mark(2);
     if (b->wlAgg.nq) {
-        kAgg<<<gridFor(b, (const void*)kAgg, b->block), b->block, 0, b->stream>>>(b->dDesc, b->wlAgg, b->tile,
-                                                                                  b->counters + 1);
+        if (b->aggRows == 2 && b->block <= 512)  // the 2-row form is built for blocks of <= 512
+            kAgg<2><<<gridFor(b, (const void*)kAgg<2>, b->block), b->block, 0, b->stream>>>(
+                b->dDesc, b->wlAgg, b->tile, b->counters + 1);
+        else
+            kAgg<4><<<gridFor(b, (const void*)kAgg<4>, b->block), b->block, 0, b->stream>>>(
+                b->dDesc, b->wlAgg, b->tile, b->counters + 1);
         launches++;
     }
     mark(3);
@@ -1224,6 +1231,15 @@ int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value) {
             return GPUDB_E_INVALID;
         }
         b->groupRows = (int)value;
+        b->dirty = true;
+        return GPUDB_OK;
+    }
+    if (n == "agg_rows") {
+        if (value != 2 && value != 4) {
+            gpudb::setThreadError("agg_rows must be 2 or 4");
+            return GPUDB_E_INVALID;
+        }
+        b->aggRows = (int)value;
         b->dirty = true;
         return GPUDB_OK;
     }
