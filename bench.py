@@ -703,9 +703,6 @@ def run_serve(args, pg=None):
         compile_s.append(time.perf_counter() - t)
     plain_res, _, service = S.serve_plain(plain, S.poisson_trace(qs[:n_plain], rate=rates[0], seed=11))
     plain_fp = [B.result_fingerprint(r) for r in plain_res]
-    # the answers hold pinned buffers of the shared pool: hand them back
-    # before serving, or the server's first large results would have to
-    # page-lock fresh memory (tens of ms) while requests wait
     del plain_res
     # every served answer is also checked against one exact-sized batch of all queries
     ex = B.BatchRunner(tables, sizing="exact", plain=plain)

@@ -72,10 +72,10 @@ SEEDS = {
 }
 BATCH_SPACE = {
     "block": [512, 256, 1024],
-    "tile_rows": [16384, 4096, 65536, 262144],
+    "tile_rows": [32768, 16384, 65536, 4096],
     "warp_aggregate": [True, False],
     "group_rows": [1, 2, 4],
-    "agg_rows": [4, 2],
+    "agg_rows": [2, 4],
 }
 
 

@@ -846,8 +846,11 @@ struct gpudb_batch {
     // twice the resident threads than it loses to a few spilled
     // registers), 2 or 4
     int groupRows = 1;
-    int aggRows = 4;  // rows in flight per thread of the agg / join kernel: 4 (64 registers) or 2 (32)
-    long long tile = 16384;
+    // rows in flight per thread of the agg / join kernel: 2 (32 registers,
+    // every thread slot resident; measured 9.9 ms against 10.6 ms per
+    // mixed batch) or 4 (64 registers)
+    int aggRows = 2;
+    long long tile = 32768;  // rows per work item (measured: 16K 5.31k, 32K 5.45k mixed queries/s)
     std::vector<gpudb_batch_query> queries;
     std::vector<QDesc> desc;
     DeviceBuf arena;  // zero-initialised per execution

@@ -110,8 +110,8 @@ int gpudb_batch_set_tuning(gpudb_batch* b, int block, int tile_rows, int warp_ag
 /* Named tuning options beyond those: "group_rows" = rows in flight per
  * thread of the group-by kernel: 1 (default; a 32-register cap), 2 (42
  * registers) or 4 (64 registers); blocks of more than 512 threads use 4.
- * "agg_rows" = the same for the agg / join kernel: 4 (default) or 2 (32
- * registers, blocks of at most 512).
+ * "agg_rows" = the same for the agg / join kernel: 2 (default; 32
+ * registers, blocks of at most 512) or 4 (64 registers).
  * GPUDB_E_INVALID for an unknown name or value. */
 int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value);
 /* Run every query; per-query device error words go to errors[n] (bit
