@@ -203,9 +203,12 @@ def coordinate_descent(space: Dict[str, Sequence], measure: Callable[[dict], Opt
 
 def tune_query(ctx, spec: str, rows: int, template: Optional[str] = None, space: Optional[dict] = None,
                reps: int = 10, warmup: int = 3, rounds: int = 2, cache: Optional[TuneCache] = None,
-               log: Optional[List[dict]] = None) -> Tuple[str, float, float]:
+               log: Optional[List[dict]] = None, flush: Optional[Callable[[], None]] = None) -> Tuple[str, float, float]:
     """Tune one plan on the tables registered in `ctx`; returns (tune
-    string, best ms, default ms) and stores the winner in `cache`."""
+    string, best ms, default ms) and stores the winner in `cache`. With
+    `flush` (which must order its work before the context's next run, e.g.
+    on the context's stream), it runs before every timed repetition: inputs
+    that L2 could partly hold are then timed from DRAM, as in the bench."""
     from .engine import GpudbError
 
     template = template or dict(kv.split("=", 1) for kv in spec.split(";") if "=" in kv).get("template", spec)
@@ -228,6 +231,8 @@ def tune_query(ctx, spec: str, rows: int, template: Optional[str] = None, space:
                 ctx.run(q, collect=False)
             ts = []
             for _ in range(reps):
+                if flush is not None:
+                    flush()
                 _, t = ctx.run(q, collect=False)
                 ts.append(sum(t.phase_ms))
             ts.sort()

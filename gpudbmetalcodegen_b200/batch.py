@@ -380,10 +380,11 @@ class Batch:
         check(self._lib.gpudb_batch_set_agg_mode(self.handle, i, int(mode)))
 
     def set_tuning(self, block: int = 512, tile_rows: int = 32768, warp_aggregate: bool = True,
-                   max_probe: int = 128, group_rows: int = 1, agg_rows: int = 2) -> None:
+                   max_probe: int = 128, group_rows: int = 1, agg_rows: int = 2, shared_warp: int = 1) -> None:
         check(self._lib.gpudb_batch_set_tuning(self.handle, block, tile_rows, int(warp_aggregate), max_probe))
         check(self._lib.gpudb_batch_set_option(self.handle, b"group_rows", group_rows))
         check(self._lib.gpudb_batch_set_option(self.handle, b"agg_rows", agg_rows))
+        check(self._lib.gpudb_batch_set_option(self.handle, b"shared_warp", shared_warp))
 
     def execute(self, use_graph: bool = True) -> Tuple[float, np.ndarray]:
         ms = C.c_double()

@@ -73,6 +73,7 @@ struct QDesc {
     Slot* ht;
     int log2cap, maxProbe;
     int aggMode;  // GPUDB_AGG_SHARED / _GLOBAL_WARP / _GLOBAL / _SHARED_DIRECT
+    int sharedWarp;  // SHARED: warp aggregation before the shared table
     unsigned* slots;
     long long* tk_part;  // [tk_chunks][kTopK] of (value, key)
     long long tk_chunks;
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(U == 4 ? 1024 : 512, U == 4 ? 1 : (U == 2 ? 3 
                 }
                 continue;
             }
-            if (mode != GPUDB_AGG_GLOBAL) {
+            if (mode == GPUDB_AGG_GLOBAL_WARP || (mode == GPUDB_AGG_SHARED && q.sharedWarp)) {
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     if (!live[u]) continue;
@@ -846,6 +847,7 @@ struct gpudb_batch {
     // twice the resident threads than it loses to a few spilled
     // registers), 2 or 4
     int groupRows = 1;
+    int sharedWarp = 1;  // SHARED strategy: warp aggregation before the shared table (1) or not (0)
     // rows in flight per thread of the agg / join kernel: 2 (32 registers,
     // every thread slot resident; measured 9.9 ms against 10.6 ms per
     // mixed batch) or 4 (64 registers)
@@ -944,6 +946,7 @@ int plan(gpudb_batch* b) {
         if (!b->warpAgg && d.aggMode == GPUDB_AGG_GLOBAL_WARP) d.aggMode = GPUDB_AGG_GLOBAL;
         // the direct table holds the 2 card - 1 encoded keys of (-card, card)
         if (d.aggMode == GPUDB_AGG_SHARED_DIRECT && 2 * d.card - 1 > kSmemSlots) d.aggMode = GPUDB_AGG_SHARED;
+        d.sharedWarp = b->sharedWarp;
         char* p = zb + zOff[i];
         d.agg = reinterpret_cast<unsigned long long*>(p);
         d.topk_n = d.agg + 3;
@@ -1234,6 +1237,15 @@ int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value) {
             return GPUDB_E_INVALID;
         }
         b->groupRows = (int)value;
+        b->dirty = true;
+        return GPUDB_OK;
+    }
+    if (n == "shared_warp") {
+        if (value != 0 && value != 1) {
+            gpudb::setThreadError("shared_warp must be 0 or 1");
+            return GPUDB_E_INVALID;
+        }
+        b->sharedWarp = (int)value;
         b->dirty = true;
         return GPUDB_OK;
     }

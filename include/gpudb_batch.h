@@ -112,6 +112,8 @@ int gpudb_batch_set_tuning(gpudb_batch* b, int block, int tile_rows, int warp_ag
  * registers) or 4 (64 registers); blocks of more than 512 threads use 4.
  * "agg_rows" = the same for the agg / join kernel: 2 (default; 32
  * registers, blocks of at most 512) or 4 (64 registers).
+ * "shared_warp" = 1 (default): the SHARED strategy aggregates each warp's
+ * equal keys before the shared table; 0: every row goes to it directly.
  * GPUDB_E_INVALID for an unknown name or value. */
 int gpudb_batch_set_option(gpudb_batch* b, const char* name, long long value);
 /* Run every query; per-query device error words go to errors[n] (bit

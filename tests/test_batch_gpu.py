@@ -72,7 +72,7 @@ def test_batch_exact_sizing_matches_oracle(tables, use_graph):
 @pytest.mark.parametrize("tuning", [dict(block=256, tile_rows=4096, warp_aggregate=False, max_probe=64),
                                     dict(block=1024, tile_rows=65536, warp_aggregate=True, max_probe=256),
                                     dict(block=512, tile_rows=16384, group_rows=2, agg_rows=4),
-                                    dict(block=512, tile_rows=16384, group_rows=4)])
+                                    dict(block=512, tile_rows=16384, group_rows=4, shared_warp=0)])
 def test_batch_tunings_and_bound_sizing(tables, tuning):
     qs = mixed(tables, 32, seed=2)
     r = B.BatchRunner(tables, sizing="bound", tuning=tuning)
