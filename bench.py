@@ -1115,8 +1115,19 @@ def run_extras(args, pg, world, rank, local) -> dict:
     form (config 3: learned / exact / plain queries per second, checked
     against the oracle), and serving (config 4: p50 / p99 at two offered
     rates). Each part reports its own wall time and, if it fails, why."""
+    import gc
+
     import torch
+
+    def release():
+        # each part starts from the device memory the previous one held
+        # handed back (its tables, arenas and pinned pools)
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
     out = {}
+    release()
     for which in ("q1", "q6"):
         t0 = time.perf_counter()
         try:
@@ -1130,7 +1141,7 @@ def run_extras(args, pg, world, rank, local) -> dict:
                 out[which]["wall_s"] = time.perf_counter() - t0
         except Exception as e:  # a failed part is reported, the headline stands
             out[which] = {"error": f"{type(e).__name__}: {e}"[:500]}
-        torch.cuda.empty_cache()
+        release()
     t0 = time.perf_counter()
     try:
         line = run_mixed(sub_args(args, workload="mixed", steps=5, train_executions=args.extras_train_executions,
@@ -1140,7 +1151,7 @@ def run_extras(args, pg, world, rank, local) -> dict:
             out["mixed"] = line
     except Exception as e:
         out["mixed"] = {"error": f"{type(e).__name__}: {e}"[:500]}
-    torch.cuda.empty_cache()
+    release()
     t0 = time.perf_counter()
     try:
         line = run_serve(sub_args(args, workload="serve", train_executions=args.extras_train_executions,
