@@ -451,6 +451,26 @@ __device__ __forceinline__ long long gpudb_ht_insert64(unsigned long long* keys,
     return -1;
 }
 
+// Best-effort insert into a small table: the slot holding `key` or one it
+// claimed within `max_probe` probes, else -1 (no error: the caller then
+// uses its main table). The sentinel key is never placed here.
+__device__ __forceinline__ long long gpudb_ht_try_insert64(unsigned long long* keys, int log2cap,
+                                                           unsigned long long key, unsigned max_probe) {
+    if (key == GPUDB_EMPTY64) return -1;
+    const unsigned long long mask = (1ull << log2cap) - 1ull;
+    unsigned long long s = gpudb_hash_slot(key, log2cap);
+    for (unsigned p = 0; p < max_probe; ++p) {
+        const unsigned long long cur = keys[s];
+        if (cur == key) return (long long)s;
+        if (cur == GPUDB_EMPTY64) {
+            const unsigned long long prev = atomicCAS(keys + s, GPUDB_EMPTY64, key);
+            if (prev == GPUDB_EMPTY64 || prev == key) return (long long)s;
+        }
+        s = (s + 1ull) & mask;
+    }
+    return -1;
+}
+
 // Packed group-by slots of 2^stride_log2 u64 words: word 0 holds ~key
 // (0 = empty; the all-ones key stays reserved as in the other layouts) and
 // the aggregates follow in the same sector. Returns the slot index, as

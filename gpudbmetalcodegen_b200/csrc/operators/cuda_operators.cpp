@@ -1345,6 +1345,36 @@ CudaHashInit::CudaHashInit(const std::string& tableName, const std::string& keyT
     : table_(tableName), keyType_(keyType), layout_(layout), aggs_(aggNames), groups_(groupsExpr), bound_(boundExpr),
       counters_(counters) {}
 
+// Insert `keyVar` into a group-by's main table and add `vals` to its
+// aggregates. slotList: 0 none; 1 record created groups in the CTA's
+// shared buffer (_gl_buf / _gl_n, overflow straight to the list); 2 append
+// created groups to the global list directly.
+static void emitHashMainUpdate(CudaCodegen& cg, const std::string& table, const std::string& keys, const KeyOps& ko, bool packed,
+                        int strideLog2, HashLayout layout, int maxProbe, const std::vector<std::string>& aggs,
+                        const std::string& keyVar, const std::vector<std::string>& vals, int slotList) {
+    constexpr int kSlotBuf = 1024;
+    const std::string list = table + "_slotlist", nlist = table + "_nslots";
+    if (slotList) cg.addLine("bool _gnew = false;");
+    cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + (packed ? S(strideLog2) + ", " : "") + table +
+               "_log2cap, " + ko.cast + keyVar + ", " + S(probeArg(layout, maxProbe)) + "u, gpudb_err" +
+               (slotList ? ", &_gnew" : "") + ");");
+    cg.addBlock("if (_gslot >= 0)", [&]() {
+        for (size_t j = 0; j < aggs.size(); j++) {
+            const std::string dst = packed ? keys + " + ((unsigned long long)_gslot << " + S(strideLog2) + ") + " + S(1 + j)
+                                           : table + "_" + aggs[j] + " + _gslot";
+            cg.addLine("atomicAdd(" + dst + ", (unsigned long long)" + vals[j] + ");");
+        }
+        if (slotList == 1)
+            cg.addBlock("if (_gnew)", [&]() {  // group created
+                cg.addLine("const unsigned _gp = atomicAdd(_gl_n, 1u);");
+                cg.addLine("if (_gp < " + S(kSlotBuf) + "u) _gl_buf[_gp] = (unsigned)_gslot;");
+                cg.addLine("else " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;");
+            });
+        else if (slotList == 2)
+            cg.addLine("if (_gnew) " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;");
+    });
+}
+
 void CudaHashInit::produce(CudaCodegen& cg, ConsumerFn consume) {
     const KeyOps ko = keyOps(keyType_, layout_);
     const std::string cap = hashSlotsExpr(bound_);
@@ -1422,24 +1452,36 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
         cg.addLine("if (threadIdx.x == 0) *_gl_n = 0u;");
         cg.addLine("__syncthreads();");
     }
+    std::vector<std::string> aggNames;
+    for (const auto& a : aggs_) aggNames.push_back(a.name);
+    auto mainUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
+        emitHashMainUpdate(cg, table_, keys, ko, packed, strideLog2, layout_, maxProbe_, aggNames, keyVar, vals,
+                           slotList_ ? 1 : 0);
+    };
+    const bool warm = warmLog2_ > 0;
+    if (warm) {
+        if (dev || ko.store != "unsigned long long")
+            throw std::runtime_error("CudaHashGroupBy: the warm tier needs 64-bit keys and a host-sized table");
+        cg.addHashMapParam(table_ + "_wkeys", "unsigned long long", S(1ll << warmLog2_));
+        for (const auto& a : aggs_) cg.addAtomicBufferParam(table_ + "_w" + a.name, "unsigned long long", S(1ll << warmLog2_));
+    }
+    // the warm tier first (an L2-resident table of the first keys to reach
+    // it), the main table for the keys it cannot place
     auto globalUpdate = [&](const std::string& keyVar, const std::vector<std::string>& vals) {
-        if (slotList_) cg.addLine("bool _gnew = false;");
-        cg.addLine("const long long _gslot = " + ko.ins + "(" + keys + ", " + (packed ? S(strideLog2) + ", " : "") +
-                   table_ + "_log2cap, " + ko.cast + keyVar + ", " + S(probeArg(layout_, maxProbe_)) + "u, gpudb_err" +
-                   (slotList_ ? ", &_gnew" : "") + ");");
-        cg.addBlock("if (_gslot >= 0)", [&]() {
-            for (int j = 0; j < na; j++) {
-                const std::string dst = packed ? keys + " + ((unsigned long long)_gslot << " + S(strideLog2) + ") + " + S(1 + j)
-                                               : table_ + "_" + aggs_[j].name + " + _gslot";
-                cg.addLine("atomicAdd(" + dst + ", (unsigned long long)" + vals[j] + ");");
-            }
-            if (slotList_)
-                cg.addBlock("if (_gnew)", [&]() {  // group created
-                    cg.addLine("const unsigned _gp = atomicAdd(_gl_n, 1u);");
-                    cg.addLine("if (_gp < " + S(kSlotBuf) + "u) _gl_buf[_gp] = (unsigned)_gslot;");
-                    cg.addLine("else " + list + "[atomicAdd(" + nlist + ", 1ull)] = (unsigned)_gslot;");
-                });
-        });
+        if (!warm) {
+            mainUpdate(keyVar, vals);
+            return;
+        }
+        cg.addLine("const long long _gws = gpudb_ht_try_insert64(" + table_ + "_wkeys, " + S(warmLog2_) +
+                   ", (unsigned long long)" + keyVar + ", " + S(warmProbe_) + "u);");
+        cg.addBlock("if (_gws >= 0)", [&]() {
+            for (int j = 0; j < na; j++)
+                cg.addLine("atomicAdd(" + table_ + "_w" + aggs_[j].name + " + _gws, (unsigned long long)" + vals[j] + ");");
+        }, " else {");
+        cg.increaseIndent();
+        mainUpdate(keyVar, vals);
+        cg.decreaseIndent();
+        cg.addLine("}");
     };
     child_->produce(cg, [&]() {
         cg.addLine("const long long _gk = (long long)(" + keyExpr_ + ");");
@@ -1510,7 +1552,51 @@ void CudaHashGroupBy::produce(CudaCodegen& cg, ConsumerFn consume) {
 std::string CudaHashGroupBy::describe() const {
     return "HashGroupBy(" + table_ + ", key=" + keyExpr_ +
            (layout_ == HashLayout::Bucket8 ? ", bucket8" : layout_ == HashLayout::Packed ? ", packed" : ", linear") +
-           (warpAgg_ ? ", warp-agg" : "") + (smemLog2_ ? ", smem-preagg" : "") + ") <- " + describeChain();
+           (warpAgg_ ? ", warp-agg" : "") + (smemLog2_ ? ", smem-preagg" : "") +
+           (warmLog2_ ? ", warm tier " + S(1ll << warmLog2_) : "") + ") <- " + describeChain();
+}
+
+CudaHashWarmFlush::CudaHashWarmFlush(const std::string& tableName, const std::string& capacityExpr, HashLayout layout,
+                                     int maxProbe, const std::vector<std::string>& aggNames, int warmLog2,
+                                     bool slotList)
+    : table_(tableName), capExpr_(capacityExpr), layout_(layout), maxProbe_(maxProbe), aggs_(aggNames),
+      warmLog2_(warmLog2), slotList_(slotList) {}
+
+void CudaHashWarmFlush::produce(CudaCodegen& cg, ConsumerFn consume) {
+    const KeyOps ko = keyOps("long long", layout_, true);
+    const std::string cap = hashSlotsExpr(capExpr_);
+    const bool packed = layout_ == HashLayout::Packed;
+    int strideLog2 = 0;
+    while ((1 << strideLog2) < 1 + (int)aggs_.size()) ++strideLog2;
+    const std::string keys = packed ? table_ + "_slots" : table_ + "_keys";
+    // the main table as the group-by phase left it: no fill here
+    if (packed) {
+        cg.addBufferParam(keys, "unsigned long long", "(" + cap + ") * " + S(1 << strideLog2), false, 0);
+    } else {
+        cg.addBufferParam(keys, ko.store, cap, false, 0);
+        for (const auto& a : aggs_) cg.addBufferParam(table_ + "_" + a, "unsigned long long", cap, false, 0);
+    }
+    cg.addSizeScalarParam(table_ + "_log2cap", "int", hashLog2Expr(capExpr_));
+    if (slotList_) {
+        cg.addBufferParam(table_ + "_slotlist", "unsigned", cap, false, 0);
+        cg.addBufferParam(table_ + "_nslots", "unsigned long long", "1", false, 0);
+    }
+    cg.addReadBufferParam(table_ + "_wkeys", "unsigned long long");
+    for (const auto& a : aggs_) cg.addReadBufferParam(table_ + "_w" + a, "unsigned long long");
+    cg.addComment("every warm entry into the main table");
+    cg.addBlock("for (long long _w = tid; _w < " + S(1ll << warmLog2_) + "ll; _w += tpg)", [&]() {
+        cg.addLine("const unsigned long long _wk = " + table_ + "_wkeys[_w];");
+        cg.addLine("if (_wk == GPUDB_EMPTY64) continue;");
+        std::vector<std::string> vals;
+        for (const auto& a : aggs_) vals.push_back(table_ + "_w" + a + "[_w]");
+        emitHashMainUpdate(cg, table_, keys, ko, packed, strideLog2, layout_, maxProbe_, aggs_, "(long long)_wk", vals,
+                           slotList_ ? 2 : 0);
+    });
+    consume();
+}
+
+std::string CudaHashWarmFlush::describe() const {
+    return "HashWarmFlush(" + table_ + ", " + S(1ll << warmLog2_) + " warm slots)";
 }
 
 // ===================================================================

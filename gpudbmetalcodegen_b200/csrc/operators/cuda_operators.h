@@ -516,6 +516,15 @@ public:
     // CudaHashInit phase with the same arguments must run first.
     void setDeviceCapacity(const std::string& groupsExpr, const std::string& boundExpr,
                            const std::vector<std::string>& counters);
+    // A warm tier between the shared-memory table and the main table: a
+    // global table of 2^log2Slots slots (small enough to stay in L2) that
+    // keeps the first keys to reach it, `probe` probes each; keys it cannot
+    // place go to the main table. A CudaHashWarmFlush phase must follow to
+    // add the warm entries into the main table (64-bit keys, host-sized).
+    void setWarmTier(int log2Slots, int probe = 4) {
+        warmLog2_ = log2Slots;
+        warmProbe_ = probe;
+    }
     void produce(CudaCodegen& cg, ConsumerFn consume) override;
     std::string describe() const override;
 
@@ -530,9 +539,28 @@ private:
     bool warpAgg_ = true;
     int smemLog2_ = 0;
     int smemProbe_ = 8;
+    int warmLog2_ = 0, warmProbe_ = 4;
     bool slotList_ = false;
     std::string devGroups_, devBound_;
     std::vector<std::string> devCounters_;
+};
+
+// The warm tier's flush: every key the warm table of a CudaHashGroupBy
+// holds is added into its main table (its own phase, after the group-by's).
+class CudaHashWarmFlush : public CudaOperator {
+public:
+    CudaHashWarmFlush(const std::string& tableName, const std::string& capacityExpr, HashLayout layout, int maxProbe,
+                      const std::vector<std::string>& aggNames, int warmLog2, bool slotList);
+    void produce(CudaCodegen& cg, ConsumerFn consume) override;
+    std::string describe() const override;
+
+private:
+    std::string table_, capExpr_;
+    HashLayout layout_;
+    int maxProbe_;
+    std::vector<std::string> aggs_;
+    int warmLog2_;
+    bool slotList_;
 };
 
 // Initialises the slots a device-sized group-by table will use (keys

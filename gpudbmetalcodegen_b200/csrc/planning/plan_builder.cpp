@@ -112,7 +112,7 @@ std::string TuneConfig::toString() const {
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
       << ";split=" << (splitJoin ? 1 : 0) << ";sprobe=" << smemProbe << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
-      << ";bvec=" << buildVectorRows << ";htf=" << hashFill;
+      << ";bvec=" << buildVectorRows << ";htf=" << hashFill << ";warm=" << warmLog2 << ";wprobe=" << warmProbe;
     return o.str();
 }
 
@@ -153,6 +153,8 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "bbs") t.buildBlockSize = std::stoi(v);
         else if (k == "bvec") t.buildVectorRows = std::stoi(v);
         else if (k == "htf") t.hashFill = std::stoi(v);
+        else if (k == "warm") t.warmLog2 = std::stoi(v);
+        else if (k == "wprobe") t.warmProbe = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -161,6 +163,9 @@ TuneConfig TuneConfig::parse(const std::string& s) {
     if (t.scan.prefetchRows < 0 || t.scan.prefetchRows > 16) throw std::runtime_error("tune: pf must be in [0,16]");
     if (t.smemCarveout < -1 || t.smemCarveout > 100) throw std::runtime_error("tune: carve must be -1 or in [0,100]");
     if (t.hashFill < 100 || t.hashFill > 800) throw std::runtime_error("tune: htf must be in [100,800] (percent)");
+    if (t.warmLog2 != 0 && (t.warmLog2 < 8 || t.warmLog2 > 22))
+        throw std::runtime_error("tune: warm must be 0 or in [8,22] (log2 of the warm table's slots)");
+    if (t.warmProbe < 1 || t.warmProbe > 64) throw std::runtime_error("tune: wprobe must be in [1,64]");
     if (t.buildBlockSize != 0 && (t.buildBlockSize < 64 || t.buildBlockSize > 1024 || t.buildBlockSize % 32))
         throw std::runtime_error("tune: bbs must be 0 or a multiple of 32 in [64,1024]");
     return t;
@@ -681,7 +686,14 @@ CudaQueryPlan buildGroupBy(Spec& s, const TuneConfig& tune) {
     gb->addAggregate("sum", "z_value[i]");
     gb->setWarpAggregate(tune.warpAggregate);
     gb->setSharedPreAgg(tune.smemPreAggLog2, tune.smemProbe);
+    if (tune.warmLog2) gb->setWarmTier(tune.warmLog2, tune.warmProbe);
     appendPhase(plan, "GB_aggregate", std::move(gb), tune);
+    if (tune.warmLog2)
+        appendPhase(plan, "GB_warm_flush",
+                    std::make_unique<CudaHashWarmFlush>("zg", hashCapacity(groupsExpr, tune), tune.hashLayout,
+                                                        tune.maxProbe, std::vector<std::string>{"count", "sum"},
+                                                        tune.warmLog2, false),
+                    tune);
     return plan;
 }
 

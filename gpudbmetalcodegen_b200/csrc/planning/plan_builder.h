@@ -120,6 +120,11 @@ struct TuneConfig {
     // table is requested for twice the groups, then rounded up to a power of
     // two). Lower fills keep a large table inside L2.
     int hashFill = 200;
+    // Warm tier of a group-by table (log2 of its slots, 0 = none) and its
+    // probe count: an L2-resident table between the shared-memory one and
+    // the main table.
+    int warmLog2 = 0;
+    int warmProbe = 4;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
     // join_topk: the probe lists matched rows and later phases aggregate
     // them, sized on the device (split=0: probe and group-by in one kernel,

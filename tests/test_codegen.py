@@ -153,3 +153,12 @@ def test_hash_fill_sizes_the_table():
     assert "(n_zbuild) * 125 / 100" in join
     with pytest.raises(GpudbError):
         engine.Query("template=groupby", "htf=50")
+
+
+def test_warm_tier_adds_a_flush_phase():
+    q = engine.Query("template=groupby", "smem=8;warm=16;wprobe=4")
+    assert "GB_warm_flush: HashWarmFlush(zg, 65536 warm slots)" in q.plan
+    assert "gpudb_ht_try_insert64(zg_wkeys, 16," in q.source
+    assert "zg_wkeys  [65536]  fill=255" in q.plan
+    with pytest.raises(GpudbError):
+        engine.Query("template=groupby", "warm=4")

@@ -45,7 +45,8 @@ def _same(res, expect):
 
 
 @pytest.mark.parametrize("tune", ["", "layout=bucket8", "layout=packed", "smem=0", "sprobe=4",
-                                  "bs=256;stages=2;smem=8;sprobe=4;warp=0"])
+                                  "bs=256;stages=2;smem=8;sprobe=4;warp=0",
+                                  "bs=256;stages=2;smem=8;sprobe=4;warp=0;warm=16"])
 def test_groupby_full_size(ctx, zipf_full, tune):
     _, zp, gb, _ = zipf_full
     ctx.upload_table("zprobe", zp)

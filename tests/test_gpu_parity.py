@@ -279,7 +279,11 @@ def test_join_topk_full_size(ctx):
 # ---------------------------------------------------------------------------
 GB_TUNES = ["", "layout=bucket8", "smem=10", "smem=12;layout=bucket8", "warp=0", "scan=direct;warp=0;smem=0",
             "vec=4", "vec=2;smem=0", "layout=packed", "layout=packed;smem=8;warp=0", "layout=packed;smem=0;warp=1",
-            "smem=8;sprobe=4;warp=0", "sprobe=1"]
+            "smem=8;sprobe=4;warp=0", "sprobe=1",
+            # the L2-resident warm tier: small (most keys spill past it), its
+            # own probe lengths, the packed layout, no shared table
+            "smem=8;warp=0;warm=8;wprobe=2", "smem=8;sprobe=4;warp=0;warm=14", "layout=packed;warm=12",
+            "smem=0;warp=1;warm=16;wprobe=8"]
 
 
 @pytest.fixture(scope="module")
