@@ -46,7 +46,7 @@ SPACES = {
     "join_topk": {**SCAN_SPACE, "warp": ["1", "0"], "split": ["1", "0"], "bbs": ["0", "256"], "bvec": ["0", "4"]},
     "groupby": {**SCAN_SPACE, **HASH_SPACE},
     "hashjoin": {**SCAN_SPACE, "layout": ["linear", "bucket8"], "probe": ["128", "64", "256"],
-                 "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"]},
+                 "smem": ["10", "0", "8"], "warp": ["1", "0"], "sprobe": ["0", "4", "1"], "vec": ["0", "2", "4"]},
 }
 # Joint moves coordinate descent cannot make one parameter at a time (a
 # shallower TMA ring frees the shared memory that a higher occupancy needs):
@@ -70,9 +70,11 @@ SEEDS = {
                 {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "sprobe": "4"}],
     # ... and the probe's latency-bound table lookups gain from every
     # thread slot resident (256-thread CTAs, 512-row tiles, 8 per SM):
-    # 1.93 ms against 2.14 ms per step
+    # 1.93 ms against 2.14 ms per step; reading the staged rows four at a
+    # time: 1.84 ms
     "hashjoin": [{"stages": "2"}, {"smem": "0", "warp": "1"}, {"stages": "2", "smem": "8", "warp": "0"},
-                 {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "occ": "8", "tile": "512"}],
+                 {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "occ": "8", "tile": "512"},
+                 {"bs": "256", "stages": "2", "smem": "8", "warp": "0", "occ": "8", "tile": "512", "vec": "4"}],
 }
 BATCH_SPACE = {
     "block": [512, 256, 1024],
