@@ -740,6 +740,8 @@ class BatchReport:
     stats_ms: float = 0.0
     execute_ms: float = 0.0
     collect_ms: float = 0.0
+    plan_ms: float = 0.0     # host: describing the batch (arena plan, descriptor upload)
+    unpack_ms: float = 0.0   # host: turning the collected rows into per-query results
     overflowed: List[int] = field(default_factory=list)
     fallback_s: float = 0.0
     wall_s: float = 0.0
@@ -798,10 +800,12 @@ class BatchRunner:
         report = BatchReport(self.sizing, len(queries))
         key = tuple(queries)
         b = self.batch
+        tp = time.perf_counter()
         if key != self._key:
             self._arr = self.tables.query_array(queries)
             b.set_queries(self._arr)
             self._key, self._groups = key, None
+        report.plan_ms = (time.perf_counter() - tp) * 1e3
         self._features = None
         groups = self.size(queries, report)
         modes = [(self.agg_mode if self.agg_mode is not None else
@@ -809,17 +813,21 @@ class BatchRunner:
                  if q.grouped else AGG_AUTO
                  for i, (g, q) in enumerate(zip(groups, queries))]
         if (groups, modes) != self._groups:
+            tp = time.perf_counter()
             self._arr["groups"] = groups
             self._arr["agg_mode"] = modes
             b.set_queries(self._arr)  # one call re-plans the arena
             self._groups = (groups, modes)
+            report.plan_ms += (time.perf_counter() - tp) * 1e3
         report.table_slots = sum(1 << max(4, math.ceil(math.log2(2 * g))) for g, q in zip(groups, queries)
                                  if q.grouped)
         report.execute_ms, err = b.execute(self.use_graph)
         report.launches = b.last_launches()
         rows, packed, report.collect_ms = b.collect()
         report.result_bytes = int(packed.nbytes)
+        tu = time.perf_counter()
         results = unpack_results(queries, rows, packed, copy=copy)
+        report.unpack_ms = (time.perf_counter() - tu) * 1e3
         err = [int(e) for e in err]
         bad = [i for i, e in enumerate(err) if e & DEVERR_HASH_OVERFLOW]
         other = [i for i, e in enumerate(err) if e & ~DEVERR_HASH_OVERFLOW]

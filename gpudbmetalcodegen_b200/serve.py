@@ -113,7 +113,7 @@ class Server:
         state = {"next": 0, "arrived": 0, "completed": 0, "reserved": 0, "peak": 0, "inflight": 0,
                  "overlap": 0.0, "mark": None, "batches": [], "overflowed": 0, "error": None,
                  "busy": {"batch_wall": 0.0, "execute": 0.0, "features": 0.0, "predict": 0.0, "collect": 0.0,
-                          "fallback": 0.0}}
+                          "plan": 0.0, "unpack": 0.0, "fallback": 0.0}}
         cost = [query_hbm_bytes(r.query, self.tables.dim_max_key) for r in trace]
         t0 = time.perf_counter()
 
@@ -180,6 +180,8 @@ class Server:
                     bz["features"] += rep.features_ms / 1e3
                     bz["predict"] += rep.predict_ms / 1e3
                     bz["collect"] += rep.collect_ms / 1e3
+                    bz["plan"] += rep.plan_ms / 1e3
+                    bz["unpack"] += rep.unpack_ms / 1e3
                     bz["fallback"] += rep.fallback_s
                     state["inflight"] -= 1
                     if state["inflight"] < 2 and state["mark"] is not None:
