@@ -112,7 +112,8 @@ std::string TuneConfig::toString() const {
       << ";warp=" << (warpAggregate ? 1 : 0) << ";keyed=" << keyedStrategy << ";probe=" << maxProbe
       << ";late=" << (lateMaterialize ? 1 : 0) << ";occ=" << minBlocksPerSM << ";pf=" << scan.prefetchRows << ";vec=" << scan.vectorRows << ";l2pf=" << scan.l2Prefetch
       << ";split=" << (splitJoin ? 1 : 0) << ";sprobe=" << smemProbe << ";carve=" << smemCarveout << ";bbs=" << buildBlockSize
-      << ";bvec=" << buildVectorRows << ";htf=" << hashFill << ";warm=" << warmLog2 << ";wprobe=" << warmProbe;
+      << ";bvec=" << buildVectorRows << ";htf=" << hashFill << ";warm=" << warmLog2 << ";wprobe=" << warmProbe
+      << ";tkb=" << topkBlocks;
     return o.str();
 }
 
@@ -155,6 +156,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
         else if (k == "htf") t.hashFill = std::stoi(v);
         else if (k == "warm") t.warmLog2 = std::stoi(v);
         else if (k == "wprobe") t.warmProbe = std::stoi(v);
+        else if (k == "tkb") t.topkBlocks = std::stoi(v);
         else throw std::runtime_error("tune: unknown key '" + k + "'");
     }
     if (t.blockSize < 32 || t.blockSize > 1024 || t.blockSize % 32)
@@ -166,6 +168,7 @@ TuneConfig TuneConfig::parse(const std::string& s) {
     if (t.warmLog2 != 0 && (t.warmLog2 < 8 || t.warmLog2 > 22))
         throw std::runtime_error("tune: warm must be 0 or in [8,22] (log2 of the warm table's slots)");
     if (t.warmProbe < 1 || t.warmProbe > 64) throw std::runtime_error("tune: wprobe must be in [1,64]");
+    if (t.topkBlocks < 1 || t.topkBlocks > 1184) throw std::runtime_error("tune: tkb must be in [1,1184]");
     if (t.buildBlockSize != 0 && (t.buildBlockSize < 64 || t.buildBlockSize > 1024 || t.buildBlockSize % 32))
         throw std::runtime_error("tune: bbs must be 0 or a multiple of 32 in [64,1024]");
     return t;
@@ -386,7 +389,7 @@ CudaQueryPlan buildJoinAgg(const JoinAggParts& jp, const TuneConfig& tune) {
         // only the slots whose groups were created (the probe's slot list)
         auto lscan = std::make_unique<CudaSlotListScan>("jg_slotlist", "jg_nslots");
         auto tk = std::make_unique<CudaTopK>(std::move(lscan), "jt_top", "(long long)(int)jg_keys[i]",
-                                             "(long long)jg_revenue[i]", (int)k);
+                                             "(long long)jg_revenue[i]", (int)k, splitTune.topkBlocks);
         auto& ph = appendPhase(plan, "JT_topk", std::move(tk), splitTune);
         ph.minBlocksPerSM = 1;  // the register-resident top-k lists must not be capped by an occupancy hint
         ph.extraBuffers.push_back({"jg_keys", "unsigned", true, false});

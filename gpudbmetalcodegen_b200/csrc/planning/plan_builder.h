@@ -125,6 +125,9 @@ struct TuneConfig {
     // the main table.
     int warmLog2 = 0;
     int warmProbe = 4;
+    // CTAs of the join's top-k phase (each keeps its own list; the last to
+    // finish merges them all)
+    int topkBlocks = 296;
     bool lateMaterialize = true;  // columns read only by surviving rows are not staged
     // join_topk: the probe lists matched rows and later phases aggregate
     // them, sized on the device (split=0: probe and group-by in one kernel,
