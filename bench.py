@@ -26,6 +26,7 @@ a barrier and the slowest rank's time is reported.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import queue
@@ -537,6 +538,11 @@ def run_mixed(args, pg=None):
 
     ctx = Context(local)
     plain = B.PlainRunner(ctx, tables)
+    # the setup's objects (the training log, the query lists) move to the
+    # collector's permanent generation, so its periodic full passes do not
+    # scan them in the middle of a timed region
+    gc.collect()
+    gc.freeze()
     # plain one-query-at-a-time path (first pass compiles / warms)
     plain_res = [plain.run(q) for q in queries]
     torch.cuda.synchronize()
@@ -666,6 +672,7 @@ def run_mixed(args, pg=None):
     learned.close()
     sizer.close()
     ctx.close()
+    gc.unfreeze()
     if own_pg and pg:
         replicas.shutdown(pg)
     return line if rank == 0 else None
@@ -737,6 +744,10 @@ def run_serve(args, pg=None):
     srv = S.Server(tables, sizer, plain=plain, workers=args.serve_workers, hbm_budget=150e9,
                    max_batch=args.serve_max_batch)
     srv.serve(S.poisson_trace(qs, rate=rates[-1], seed=12))  # warm the workers, their arenas and pools
+    # the setup's objects out of the collector's periodic full passes (a
+    # pass over the training log stalls every serving thread)
+    gc.collect()
+    gc.freeze()
     per_rate, verified, clocks = [], True, None
     launches = 0
     for rate in rates:
@@ -773,6 +784,7 @@ def run_serve(args, pg=None):
                          f"plain_one_at_a_time_first_{n_plain}": prep.summary(),
                          "bit_exact_vs_alone": ok_alone, "bit_exact_vs_exact_batch": ok_all})
     srv.close()
+    gc.unfreeze()
     top = per_rate[-1]["ours"]
     if rank == 0:
         line = {"metric": "serve_queries_per_s", "value": top["queries_per_s"], "unit": "queries/s",
@@ -1128,8 +1140,6 @@ def run_extras(args, pg, world, rank, local) -> dict:
     form (config 3: learned / exact / plain queries per second, checked
     against the oracle), and serving (config 4: p50 / p99 at two offered
     rates). Each part reports its own wall time and, if it fails, why."""
-    import gc
-
     import torch
 
     def release():
