@@ -164,6 +164,95 @@ MetalQueryPlan groupbyPlan() {
     return plan;
 }
 
+// The reference's anti-join operators (Q22 / Q21 use AntiBitmapProbe,
+// metal_operators.cpp:157-165): probe rows whose key is NOT in the build
+// side's qualifying set, binned by discount (ComputeExpr) into a float sum
+// of price and a count per bin (AtomicAgg + AtomicCount).
+MetalQueryPlan antiPlan() {
+    MetalQueryPlan plan;
+    plan.name = "ANTI";
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("dim", "row", "i");
+        scan->addColumn("b_key", "int");
+        scan->addColumn("b_order_day", "int");
+        scan->addColumn("b_segment", "char");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "b_segment[i] == 1 && b_order_day[i] < 1170");
+        auto bm = std::make_unique<MetalBitmapBuild>(std::move(sel), "d_ab_bitmap", "b_key[i]", "(maxKey + 31) / 32");
+        plan.phases.push_back(makePhase("ANTI_build_bitmap", std::move(bm), 256));
+    }
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("probe", "row", "i");
+        scan->addColumn("p_fk", "int");
+        scan->addColumn("p_ship_day", "int");
+        scan->addColumn("p_price", "float");
+        scan->addColumn("p_discount", "int");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "p_ship_day[i] > 1170");
+        auto ap = std::make_unique<MetalAntiBitmapProbe>(std::move(sel), "d_ab_bitmap", "p_fk[i]");
+        auto bin = std::make_unique<MetalComputeExpr>(std::move(ap), "_bin", "int", "p_discount[i]");
+        auto sum = std::make_unique<MetalAtomicAgg>(std::move(bin), "d_a_sum", "_bin", "p_price[i]", "11",
+                                                    "atomic_float", "float");
+        auto cnt = std::make_unique<MetalAtomicCount>(std::move(sum), "d_a_cnt", "_bin", "11");
+        plan.phases.push_back(makePhase("ANTI_probe_bins", std::move(cnt), 1024));
+    }
+    return plan;
+}
+
+// The reference's count histogram (Q13: AtomicCount per key, then per
+// build row an ArrayLookup of its key's count into AtomicCount bins,
+// metal_plan_builder.cpp:1244-1299).
+MetalQueryPlan histPlan() {
+    MetalQueryPlan plan;
+    plan.name = "HIST";
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("probe", "row", "i");
+        scan->addColumn("p_fk", "int");
+        scan->addColumn("p_ship_day", "int");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "p_ship_day[i] > 1170");
+        auto cnt = std::make_unique<MetalAtomicCount>(std::move(sel), "d_h_cnt", "p_fk[i]", "maxKey");
+        plan.phases.push_back(makePhase("HIST_count", std::move(cnt), 1024));
+    }
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("dim", "row", "i");
+        scan->addColumn("b_key", "int");
+        auto lk = std::make_unique<MetalArrayLookup>(std::move(scan), "d_h_cnt", "b_key[i]", "_c", "int", -1);
+        auto hist = std::make_unique<MetalAtomicCount>(std::move(lk), "d_h_hist", "_c", "256");
+        plan.phases.push_back(makePhase("HIST_bins", std::move(hist), 256));
+    }
+    return plan;
+}
+
+// The reference's direct-address join (Q3: ArrayStore of the qualifying
+// build keys' order_day, then the probe's ArrayLookup and AtomicAgg,
+// metal_plan_builder.cpp:1189-1236).
+MetalQueryPlan directPlan() {
+    MetalQueryPlan plan;
+    plan.name = "DIRECT";
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("dim", "row", "i");
+        scan->addColumn("b_key", "int");
+        scan->addColumn("b_order_day", "int");
+        scan->addColumn("b_segment", "char");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "b_segment[i] == 1 && b_order_day[i] < 1170");
+        auto st = std::make_unique<MetalArrayStore>(std::move(sel), "d_d_day", "b_key[i]", "b_order_day[i]", "int",
+                                                    "maxKey");
+        plan.phases.push_back(makePhase("DIRECT_build_map", std::move(st), 256));
+    }
+    {
+        auto scan = std::make_unique<MetalGridStrideScan>("probe", "row", "i");
+        scan->addColumn("p_fk", "int");
+        scan->addColumn("p_ship_day", "int");
+        scan->addColumn("p_price", "float");
+        scan->addColumn("p_discount", "float");
+        auto sel = std::make_unique<MetalSelection>(std::move(scan), "p_ship_day[i] > 1170");
+        auto lk = std::make_unique<MetalArrayLookup>(std::move(sel), "d_d_day", "p_fk[i]", "_od", "int", -1);
+        auto agg = std::make_unique<MetalAtomicAgg>(std::move(lk), "d_d_rev", "p_fk[i]",
+                                                    "p_price[i] * (1.0f - p_discount[i])", "maxKey", "atomic_float",
+                                                    "float");
+        plan.phases.push_back(makePhase("DIRECT_probe_aggregate", std::move(agg), 1024));
+    }
+    return plan;
+}
+
 std::string jsonEscape(const std::string& s) {
     std::string o;
     for (char c : s) {
@@ -296,7 +385,10 @@ int main(int argc, char** argv) {
     emitPlan(joinPlan(), out, manifest, false);
     emitPlan(joinRowsPlan(), out, manifest, false);
     emitPlan(groupbyPlan(), out, manifest, false);
+    emitPlan(antiPlan(), out, manifest, false);
+    emitPlan(histPlan(), out, manifest, false);
+    emitPlan(directPlan(), out, manifest, false);
     manifest << "\n}\n";
-    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,JOINROWS,GROUPBY}.cpp and manifest.json\n";
+    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,JOINROWS,GROUPBY,ANTI,HIST,DIRECT}.cpp and manifest.json\n";
     return 0;
 }

@@ -80,6 +80,33 @@ def main():
                          "ref": {"keys": [int(k) for k in keys], "count": [int(b["d_cnt"][k]) for k in keys],
                                  "sum": [float(b["d_sum"][k]) for k in keys]}})
 
+    # the anti-join, the count histogram and the direct-address join: the
+    # reference's AntiBitmapProbe / AtomicCount + ArrayLookup / ArrayStore +
+    # ArrayLookup chains over the same seeded build and probe tables
+    nd, npr, seed = 20_000, 80_000, 6
+    d, p = join_inputs(nd, npr, seed)
+    cs = checksum(list(d.values()) + list(p.values()))
+    price = (p["p_price"] / 100.0).astype(np.float32)
+    cols = {"b_key": d["b_key"], "b_order_day": d["b_order_day"], "b_segment": d["b_segment"].view(np.int8),
+            "p_fk": p["p_fk"], "p_ship_day": p["p_ship_day"], "p_price": price,
+            "p_discount": p["p_discount"].astype(np.int32)}
+    b = rk.run("ANTI", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    bins = [k for k in range(11) if b["d_a_cnt"][k]]
+    out["cases"].append({"plan": "ANTI", "dim_rows": nd, "probe_rows": npr, "seed": seed, "input_checksum": cs,
+                         "ref": {"bin": bins, "count": [int(b["d_a_cnt"][k]) for k in bins],
+                                 "sum_price": [float(b["d_a_sum"][k]) for k in bins]}})
+    b = rk.run("HIST", {"p_fk": p["p_fk"], "p_ship_day": p["p_ship_day"], "b_key": d["b_key"]},
+               {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    bins = [k for k in range(256) if b["d_h_hist"][k]]
+    out["cases"].append({"plan": "HIST", "dim_rows": nd, "probe_rows": npr, "seed": seed, "input_checksum": cs,
+                         "ref": {"bin": bins, "keys": [int(b["d_h_hist"][k]) for k in bins]}})
+    cols["p_discount"] = (p["p_discount"] / 100.0).astype(np.float32)
+    b = rk.run("DIRECT", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    rev = b["d_d_rev"]
+    keys = np.nonzero(rev > 0)[0]
+    out["cases"].append({"plan": "DIRECT", "dim_rows": nd, "probe_rows": npr, "seed": seed, "input_checksum": cs,
+                         "ref": {"keys": [int(k) for k in keys], "revenue": [float(rev[k]) for k in keys]}})
+
     path = Path(__file__).resolve().parent / "ref_pinning.json"
     path.write_text(json.dumps(out, separators=(",", ":")) + "\n")
     print(f"wrote {path} ({path.stat().st_size} bytes, {len(out['cases'])} cases)")

@@ -133,6 +133,48 @@ def test_oracle_matches_reference_groupby(case):
     check_groupby(case["ref"], m, case["thr"], case["card"])
 
 
+def join_case(case):
+    d = W.gen_dim(case["dim_rows"], seed=case["seed"])
+    p = W.gen_probe(case["probe_rows"], dim_rows=case["dim_rows"], seed=case["seed"])
+    assert checksum(list(d.values()) + list(p.values())) == case["input_checksum"]
+    return d, p
+
+
+def check_anti(ref, d, p):
+    """The reference's anti-join (BitmapBuild, AntiBitmapProbe, per-discount
+    AtomicCount and float AtomicAgg of the price): the same non-empty bins
+    and counts as the oracle, the float price sums within the golden
+    tolerance of the exact cent sums."""
+    exp = O.anti_join(d, p)
+    assert ref["bin"] == [b for b, _, _ in exp]
+    assert ref["count"] == [c for _, c, _ in exp]
+    for a, (_, _, s) in zip(ref["sum_price"], exp):
+        assert close(a, s / 100)
+
+
+@pytest.mark.parametrize("case", cases("ANTI"), ids=lambda c: f"p{c['probe_rows']}")
+def test_oracle_matches_reference_anti(case):
+    check_anti(case["ref"], *join_case(case))
+
+
+@pytest.mark.parametrize("case", cases("HIST"), ids=lambda c: f"p{c['probe_rows']}")
+def test_oracle_matches_reference_histogram(case):
+    """The reference's count histogram (AtomicCount per key, ArrayLookup of
+    each build key's count, AtomicCount into bins): exact."""
+    d, p = join_case(case)
+    exp = O.histogram(d, p)
+    assert case["ref"]["bin"] == [c for c, _ in exp]
+    assert case["ref"]["keys"] == [k for _, k in exp]
+
+
+@pytest.mark.parametrize("case", cases("DIRECT"), ids=lambda c: f"p{c['probe_rows']}")
+def test_oracle_matches_reference_direct(case):
+    """The reference's direct-address join (ArrayStore of the qualifying build
+    keys' order day, ArrayLookup per probe row, float AtomicAgg per key)
+    yields the hash join's groups and revenues."""
+    check_join(case["ref"], *join_case(case))
+
+
 # ---------------------------------------------------------------------------
 # live: the reference's kernels on fresh seeds (only where the harness exists)
 # ---------------------------------------------------------------------------
@@ -167,6 +209,17 @@ def test_live_reference_matches_oracle():
     rows = sorted(zip(b["d_jr_row"][:n].tolist(), b["d_jr_key"][:n].tolist(), b["d_jr_rev"][:n].tolist()))
     check_join_rows({"row": [r for r, _, _ in rows], "key": [k for _, k, _ in rows],
                      "revenue": [float(v) for _, _, v in rows]}, d, p)
+    b = rk.run("DIRECT", cols, {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    keys = np.nonzero(b["d_d_rev"] > 0)[0]
+    check_join({"keys": [int(k) for k in keys], "revenue": [float(b["d_d_rev"][k]) for k in keys]}, d, p)
+    b = rk.run("ANTI", dict(cols, p_discount=p["p_discount"].astype(np.int32)), {"dim": nd, "probe": npr},
+               {"maxKey": int(d["b_key"].max()) + 1})
+    bins = [k for k in range(11) if b["d_a_cnt"][k]]
+    check_anti({"bin": bins, "count": [int(b["d_a_cnt"][k]) for k in bins],
+                "sum_price": [float(b["d_a_sum"][k]) for k in bins]}, d, p)
+    b = rk.run("HIST", {"p_fk": p["p_fk"], "p_ship_day": p["p_ship_day"], "b_key": d["b_key"]},
+               {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
+    assert [(c, int(b["d_h_hist"][c])) for c in range(256) if b["d_h_hist"][c]] == O.histogram(d, p)
     m = W.gen_mix(40_000, nranks=1 << 20, dim_rows=1000, seed=404)
     cols = {"m_rank_u": m["m_rank_u"], "m_filter": m["m_filter"], "m_value": m["m_value"].astype(np.float32)}
     b = rk.run("GROUPBY", cols, {"mix": 40_000}, {"card": 500}, scalars={"thr": 7000, "card": 500})
