@@ -30,7 +30,7 @@ REF_SOURCES = [
     "codegen/core/metal_param_binding.cpp",
 ]
 REF_INCLUDES = ["codegen/planning", "codegen/operators", "codegen/core"]
-PLANS = ["Q1", "Q6", "JOIN", "JOINROWS", "GROUPBY", "ANTI", "HIST", "DIRECT"]
+PLANS = ["Q1", "Q6", "JOIN", "JOINROWS", "GROUPBY", "ANTI", "HIST", "DIRECT", "Q5"]
 
 
 def available() -> bool:

@@ -21,6 +21,10 @@
 //         configuration's columns
 //   GROUPBY the reference's AtomicAgg + AtomicCount (Q18 / Q13 operators)
 //         grouping by rank % card
+//   ANTI / HIST / DIRECT  the reference's Q22 anti-join, Q13 count histogram
+//         and Q3 direct-address join chains over the join configuration
+//   Q5  buildMetalPlan(empty analysis, "Q5"): the reference's own five-phase
+//         multi-join (metal_plan_builder.cpp:894-1015), reached by name
 #include <fstream>
 #include <iostream>
 #include <regex>
@@ -376,8 +380,9 @@ int main(int argc, char** argv) {
     manifest << "{\n";
     auto q1 = buildMetalPlan(q1Query(), "Q1");
     auto q6 = buildMetalPlan(q6Query(), "Q6");
-    if (!q1 || !q6) {
-        std::cerr << "reference planner did not accept the Q1/Q6 shapes\n";
+    auto q5 = buildMetalPlan(AnalyzedQuery{}, "Q5");
+    if (!q1 || !q6 || !q5) {
+        std::cerr << "reference planner did not accept the Q1/Q6/Q5 shapes\n";
         return 1;
     }
     emitPlan(*q1, out, manifest, true);
@@ -388,7 +393,9 @@ int main(int argc, char** argv) {
     emitPlan(antiPlan(), out, manifest, false);
     emitPlan(histPlan(), out, manifest, false);
     emitPlan(directPlan(), out, manifest, false);
+    q5->name = "Q5";
+    emitPlan(*q5, out, manifest, false);
     manifest << "\n}\n";
-    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,JOINROWS,GROUPBY,ANTI,HIST,DIRECT}.cpp and manifest.json\n";
+    std::cout << "wrote " << out << "/ref_{Q1,Q6,JOIN,JOINROWS,GROUPBY,ANTI,HIST,DIRECT,Q5}.cpp and manifest.json\n";
     return 0;
 }

@@ -117,3 +117,29 @@ def fact_as_reference(fact: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
             "l_tax": (fact["f_tax"] / 100.0).astype(np.float32),
             "l_returnflag": fact["f_flag_a"].view(np.int8),
             "l_linestatus": fact["f_flag_b"].view(np.int8)}
+
+
+def snow_as_reference(snow: Dict[str, Dict[str, np.ndarray]], day_ge: int = 730, day_lt: int = 1095):
+    """The multi-join snowflake in the reference's Q5 schema (nation,
+    customer, supplier, orders, lineitem; metal_plan_builder.cpp:894-1015).
+    The reference's Q5 plan filters o_orderdate on yyyymmdd literals
+    [19940101, 19950101); the day numbers are mapped onto that scale by a
+    monotone map that sends [day_ge, day_lt) exactly onto it, so the same
+    orders qualify. Returns (columns, rows, symbols)."""
+    nat, cust, supp, ords, line = (snow[t] for t in ("nation", "cust", "supp", "ord", "line"))
+    d = ords["o_day"].astype(np.int64)
+    date = np.where(d < day_ge, 19930000 + d - day_ge,
+                    np.where(d < day_lt, 19940101 + d - day_ge, 19950101 + d - day_lt))
+    cols = {"n_nationkey": nat["n_key"].astype(np.int32), "n_regionkey": nat["n_region"].astype(np.int32),
+            "c_custkey": cust["c_key"], "c_nationkey": cust["c_nation"],
+            "s_suppkey": supp["s_key"], "s_nationkey": supp["s_nation"],
+            "o_orderkey": ords["o_key"], "o_custkey": ords["o_cust"], "o_orderdate": date.astype(np.int32),
+            "l_orderkey": line["l_okey"], "l_suppkey": line["l_supp"],
+            "l_extendedprice": (line["l_price"] / 100.0).astype(np.float32),
+            "l_discount": (line["l_discount"] / 100.0).astype(np.float32)}
+    rows = {"nation": 25, "customer": len(cust["c_key"]), "supplier": len(supp["s_key"]),
+            "orders": len(ords["o_key"]), "lineitem": len(line["l_okey"])}
+    top = lambda *a: int(max(int(x.max(initial=0)) for x in a)) + 1  # noqa: E731
+    syms = {"maxCustkey": top(cust["c_key"], ords["o_cust"]), "maxSuppkey": top(supp["s_key"], line["l_supp"]),
+            "maxOrderkey": top(ords["o_key"], line["l_okey"])}
+    return cols, rows, syms

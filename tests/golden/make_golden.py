@@ -107,6 +107,17 @@ def main():
     out["cases"].append({"plan": "DIRECT", "dim_rows": nd, "probe_rows": npr, "seed": seed, "input_checksum": cs,
                          "ref": {"keys": [int(k) for k in keys], "revenue": [float(rev[k]) for k in keys]}})
 
+    # the multi-join through the reference's own Q5 plan (buildMetalPlan by name)
+    nc, ns, no, nl, seed = 3_000, 200, 30_000, 120_000, 8
+    snow = W.gen_snowflake(nc, ns, no, nl, seed=seed)
+    cols, rows, syms = R.snow_as_reference(snow)
+    b = rk.run("Q5", cols, rows, syms, scalars={"asia_rk": 2})
+    rev = b["d_nation_revenue"]
+    nations = [n for n in range(25) if rev[n]]
+    out["cases"].append({"plan": "Q5", "sizes": [nc, ns, no, nl], "seed": seed,
+                         "input_checksum": checksum([a for t in snow.values() for a in t.values()]),
+                         "ref": {"nation": nations, "revenue": [float(rev[n]) for n in nations]}})
+
     path = Path(__file__).resolve().parent / "ref_pinning.json"
     path.write_text(json.dumps(out, separators=(",", ":")) + "\n")
     print(f"wrote {path} ({path.stat().st_size} bytes, {len(out['cases'])} cases)")

@@ -175,6 +175,24 @@ def test_oracle_matches_reference_direct(case):
     check_join(case["ref"], *join_case(case))
 
 
+def check_multi_join(ref, snow):
+    """The reference's Q5 plan (nation bitmap, customer / supplier / orders
+    nation maps, same-nation probe with float AtomicAgg per nation): the
+    oracle's nations, its exact revenues within the golden tolerance."""
+    exp = O.multi_join(snow)
+    assert ref["nation"] == [n for n, _ in exp]
+    for a, (_, v) in zip(ref["revenue"], exp):
+        assert close(a, v / 1e4)
+
+
+@pytest.mark.parametrize("case", cases("Q5"), ids=lambda c: f"l{c['sizes'][3]}")
+def test_oracle_matches_reference_multi_join(case):
+    snow = W.gen_snowflake(*case["sizes"], seed=case["seed"])
+    assert checksum([a for t in snow.values() for a in t.values()]) == case["input_checksum"]
+    assert len(case["ref"]["nation"]) == 5
+    check_multi_join(case["ref"], snow)
+
+
 # ---------------------------------------------------------------------------
 # live: the reference's kernels on fresh seeds (only where the harness exists)
 # ---------------------------------------------------------------------------
@@ -220,6 +238,10 @@ def test_live_reference_matches_oracle():
     b = rk.run("HIST", {"p_fk": p["p_fk"], "p_ship_day": p["p_ship_day"], "b_key": d["b_key"]},
                {"dim": nd, "probe": npr}, {"maxKey": int(d["b_key"].max()) + 1})
     assert [(c, int(b["d_h_hist"][c])) for c in range(256) if b["d_h_hist"][c]] == O.histogram(d, p)
+    snow = W.gen_snowflake(2_000, 150, 20_000, 90_000, seed=505)
+    cols, rows, syms = R.snow_as_reference(snow)
+    rev = rk.run("Q5", cols, rows, syms, scalars={"asia_rk": 2})["d_nation_revenue"]
+    check_multi_join({"nation": [n for n in range(25) if rev[n]], "revenue": [float(v) for v in rev if v]}, snow)
     m = W.gen_mix(40_000, nranks=1 << 20, dim_rows=1000, seed=404)
     cols = {"m_rank_u": m["m_rank_u"], "m_filter": m["m_filter"], "m_value": m["m_value"].astype(np.float32)}
     b = rk.run("GROUPBY", cols, {"mix": 40_000}, {"card": 500}, scalars={"thr": 7000, "card": 500})
