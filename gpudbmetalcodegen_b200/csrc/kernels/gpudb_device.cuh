@@ -706,11 +706,61 @@ __device__ __forceinline__ void gpudb_topk_warp_merge_rounds(const long long (&v
     }
 }
 
+// Sort one entry per lane of a warp into (value desc, key asc) order, best
+// at lane 0: a 32-wide bitonic sorting network of shuffles. Full warp.
+__device__ __forceinline__ void gpudb_topk_warp_sort32(long long& v, long long& k) {
+    const int lane = (int)(threadIdx.x & 31u);
+#pragma unroll
+    for (int w = 2; w <= 32; w <<= 1) {
+#pragma unroll
+        for (int j = w >> 1; j > 0; j >>= 1) {
+            const long long pv = __shfl_xor_sync(0xffffffffu, v, j), pk = __shfl_xor_sync(0xffffffffu, k, j);
+            const bool better = gpudb_topk_better(v, k, pv, pk);
+            // descending runs keep the better entry at the lower lane
+            const bool keep = (((lane & j) == 0) == ((lane & w) == 0)) ? better : !better;
+            if (!keep) {
+                v = pv;
+                k = pk;
+            }
+        }
+    }
+}
+
+// Merge a second sorted list (ov, ok: lane j holds its j-th best) into the
+// warp's sorted list (rv, rk). Lane j takes the better of its own entry
+// and the other list's (31-j)-th: of two descending sequences that keeps
+// the best 32 of both as a bitonic sequence, which five half-cleaner
+// stages sort. Lanes K..31 end as "none". Full warp.
+template <int K>
+__device__ __forceinline__ void gpudb_topk_warp_merge_list(long long& rv, long long& rk, long long ov, long long ok) {
+    const int lane = (int)(threadIdx.x & 31u);
+    long long v = rv, k = rk;
+    {
+        const long long bv = __shfl_sync(0xffffffffu, ov, 31 - lane), bk = __shfl_sync(0xffffffffu, ok, 31 - lane);
+        if (gpudb_topk_better(bv, bk, v, k)) {
+            v = bv;
+            k = bk;
+        }
+    }
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const long long pv = __shfl_xor_sync(0xffffffffu, v, j), pk = __shfl_xor_sync(0xffffffffu, k, j);
+        // the lower lane of each pair keeps the better entry, the upper the worse
+        if (((lane & j) == 0) == gpudb_topk_better(pv, pk, v, k)) {
+            v = pv;
+            k = pk;
+        }
+    }
+    rv = lane < K ? v : GPUDB_TOPK_NONE_VAL;
+    rk = lane < K ? k : GPUDB_TOPK_NONE_KEY;
+}
+
 // A warp's best K (K <= 32) held one entry per lane: lane j holds the
-// j-th best. Offer one entry per lane: a ballot keeps those better than
-// the current K-th best, and each is inserted by one more ballot (its rank
-// = the entries better than it) and a shift of the lanes below it. Returns
-// the ballot of offered entries that beat the K-th best. Full warp.
+// j-th best, lanes K..31 hold "none". Offer one entry per lane: a ballot
+// keeps those better than the current K-th best. A few are inserted one
+// at a time (one more ballot gives each its rank, the lanes below it
+// shift); more are sorted by a bitonic network and merged as a list.
+// Returns the ballot of offered entries that beat the K-th best. Full warp.
 template <int K>
 __device__ __forceinline__ unsigned gpudb_topk_warp_offer(long long& rv, long long& rk, long long cv, long long ck) {
     static_assert(K >= 1 && K <= 32, "a warp holds at most 32 entries");
@@ -719,26 +769,16 @@ __device__ __forceinline__ unsigned gpudb_topk_warp_offer(long long& rv, long lo
     const unsigned any = __ballot_sync(0xffffffffu, gpudb_topk_better(cv, ck, tv, tk));
     if (!any) return 0u;
     const long long hv = __shfl_sync(0xffffffffu, rv, 0), hk = __shfl_sync(0xffffffffu, rk, 0);
-    if (hv == GPUDB_TOPK_NONE_VAL && hk == GPUDB_TOPK_NONE_KEY && __popc(any) > 2) {
-        // empty list, several entries: a bitonic sort of the 32 offered
-        // entries (best first) gives the list at once
-        long long v = cv, k = ck;
-#pragma unroll
-        for (int w = 2; w <= 32; w <<= 1) {
-#pragma unroll
-            for (int j = w >> 1; j > 0; j >>= 1) {
-                const long long pv = __shfl_xor_sync(0xffffffffu, v, j), pk = __shfl_xor_sync(0xffffffffu, k, j);
-                const bool better = gpudb_topk_better(v, k, pv, pk);
-                // descending runs keep the better entry at the lower lane
-                const bool keep = (((lane & j) == 0) == ((lane & w) == 0)) ? better : !better;
-                if (!keep) {
-                    v = pv;
-                    k = pk;
-                }
-            }
+    const bool empty = hv == GPUDB_TOPK_NONE_VAL && hk == GPUDB_TOPK_NONE_KEY;
+    if (__popc(any) > (empty ? 2 : 4)) {
+        long long v = (any >> lane) & 1u ? cv : GPUDB_TOPK_NONE_VAL, k = (any >> lane) & 1u ? ck : GPUDB_TOPK_NONE_KEY;
+        gpudb_topk_warp_sort32(v, k);
+        if (empty) {
+            rv = lane < K ? v : GPUDB_TOPK_NONE_VAL;
+            rk = lane < K ? k : GPUDB_TOPK_NONE_KEY;
+        } else {
+            gpudb_topk_warp_merge_list<K>(rv, rk, v, k);
         }
-        rv = lane < K ? v : GPUDB_TOPK_NONE_VAL;
-        rk = lane < K ? k : GPUDB_TOPK_NONE_KEY;
         return any;
     }
     unsigned m = any;

@@ -1699,9 +1699,6 @@ void CudaTopK::produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, Co
     const std::string& i = list.indexVar();
     // highest full-list floor of all blocks, as value ^ sign bit (0 = none)
     cg.addAtomicBufferParam(out_ + "_floor", "unsigned long long", "1");
-    cg.addLine("__shared__ unsigned long long _ts_floor;");
-    cg.addLine("if (threadIdx.x == 0) _ts_floor = 0ull;");
-    cg.addLine("__syncthreads();");
     cg.addLine("const int _tl = (int)(threadIdx.x & 31u);");
     cg.addLine("long long _tr_v = GPUDB_TOPK_NONE_VAL, _tr_k = GPUDB_TOPK_NONE_KEY;");
     cg.addLine("const long long _tl_n = " + n + ";");
@@ -1716,32 +1713,25 @@ void CudaTopK::produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, Co
         });
         cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tc_v, _tc_k);");
     });
-    cg.addLine("__shared__ long long _ts_v[32 * " + K + "], _ts_k[32 * " + K + "];");
+    cg.addLine("__shared__ long long _ts_v[32 * 32], _ts_k[32 * 32];");
     cg.addLine("__shared__ bool _t_last;");
     // (the biased floor of a full list, or 0)
     const std::string fullFloor = "(_tl == " + S(k_ - 1) + " && !(_tr_k == GPUDB_TOPK_NONE_KEY && _tr_v == "
                                   "GPUDB_TOPK_NONE_VAL) ? ((unsigned long long)_tr_v ^ 0x8000000000000000ull) : 0ull)";
-    // every warp's list -> warp 0 holds the block's best K
+    // every warp's sorted list -> warp 0 holds the block's best K: a tree of
+    // pairwise list merges through shared memory, log2(warps) levels
     auto blockMerge = [&]() {
-        cg.addBlock("if (_tl < " + K + ")", [&]() {
-            cg.addLine("_ts_v[(threadIdx.x >> 5) * " + K + " + _tl] = _tr_v;");
-            cg.addLine("_ts_k[(threadIdx.x >> 5) * " + K + " + _tl] = _tr_k;");
-            cg.addLine("const unsigned long long _fl = " + fullFloor + ";");
-            cg.addLine("if (_fl > _ts_floor) atomicMax(&_ts_floor, _fl);");
-        });
-        cg.addLine("__syncthreads();");
-        cg.addBlock("if (threadIdx.x < 32u)", [&]() {
-            cg.addLine("_tr_v = GPUDB_TOPK_NONE_VAL; _tr_k = GPUDB_TOPK_NONE_KEY;");
-            cg.addLine("const long long _tfv = (long long)(_ts_floor ^ 0x8000000000000000ull);");
-            cg.addLine("const int _tn = (int)(blockDim.x >> 5) * " + K + ";");
-            cg.addBlock("for (int _e0 = 0; _e0 < _tn; _e0 += 32)", [&]() {
-                cg.addLine("const int _e = _e0 + _tl;");
-                cg.addLine("const bool _tin = _e < _tn && _ts_v[_e] >= _tfv;");
-                cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
-                cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ts_v[_e] : GPUDB_TOPK_NONE_VAL, "
-                           "_tin ? _ts_k[_e] : GPUDB_TOPK_NONE_KEY);");
+        cg.addLine("_ts_v[threadIdx.x] = _tr_v; _ts_k[threadIdx.x] = _tr_k;");
+        cg.addBlock("for (int _ts = 1; _ts < (int)(blockDim.x >> 5); _ts <<= 1)", [&]() {
+            cg.addLine("__syncthreads();");
+            cg.addLine("const int _tw = (int)(threadIdx.x >> 5);");
+            cg.addBlock("if ((_tw & (2 * _ts - 1)) == 0 && _tw + _ts < (int)(blockDim.x >> 5))", [&]() {
+                cg.addLine("gpudb_topk_warp_merge_list<" + K + ">(_tr_v, _tr_k, _ts_v[(_tw + _ts) * 32 + _tl], "
+                           "_ts_k[(_tw + _ts) * 32 + _tl]);");
+                cg.addLine("_ts_v[threadIdx.x] = _tr_v; _ts_k[threadIdx.x] = _tr_k;");
             });
         });
+        cg.addLine("__syncthreads();");
     };
     blockMerge();
     cg.addBlock("if (threadIdx.x < 32u)", [&]() {
@@ -1760,25 +1750,27 @@ void CudaTopK::produceOverList(CudaCodegen& cg, const CudaSlotListScan& list, Co
         cg.addLine("__threadfence();");
         cg.addLine("_tr_v = GPUDB_TOPK_NONE_VAL; _tr_k = GPUDB_TOPK_NONE_KEY;");
         cg.addLine("const long long _tgf = (long long)(__ldcg(" + out_ + "_floor) ^ 0x8000000000000000ull);");
-        cg.addLine("const int _tg = (int)gridDim.x * " + K + ";");
-        // four batches' loads in flight per warp before any is offered
-        cg.addBlock("for (int _e0 = (int)(threadIdx.x & ~31u); _e0 < _tg; _e0 += 4 * (int)blockDim.x)", [&]() {
+        // each warp merges whole block lists (lane j loads a list's j-th
+        // entry), four lists' loads in flight before any merge; a list with
+        // no entry at or above the highest block floor cannot contribute
+        cg.addLine("const int _tnw = (int)(blockDim.x >> 5);");
+        cg.addBlock("for (int _b0 = (int)(threadIdx.x >> 5); _b0 < (int)gridDim.x; _b0 += 4 * _tnw)", [&]() {
             cg.addLine("long long _ev[4], _ek[4];");
             cg.addLine("#pragma unroll");
             cg.addBlock("for (int _u = 0; _u < 4; ++_u)", [&]() {
-                cg.addLine("const int _e = _e0 + _u * (int)blockDim.x + _tl;");
-                cg.addLine("_ev[_u] = _e < _tg ? __ldcg(" + out_ + "_pvals + _e) : GPUDB_TOPK_NONE_VAL;");
-                cg.addLine("_ek[_u] = _e < _tg ? __ldcg(" + out_ + "_pkeys + _e) : GPUDB_TOPK_NONE_KEY;");
+                cg.addLine("const int _b = _b0 + _u * _tnw;");
+                cg.addLine("const bool _tin = _b < (int)gridDim.x && _tl < " + K + ";");
+                cg.addLine("_ev[_u] = _tin ? __ldcg(" + out_ + "_pvals + _b * " + K + " + _tl) : GPUDB_TOPK_NONE_VAL;");
+                cg.addLine("_ek[_u] = _tin ? __ldcg(" + out_ + "_pkeys + _b * " + K + " + _tl) : GPUDB_TOPK_NONE_KEY;");
             });
             cg.addLine("#pragma unroll");
             cg.addBlock("for (int _u = 0; _u < 4; ++_u)", [&]() {
-                cg.addLine("const bool _tin = _e0 + _u * (int)blockDim.x + _tl < _tg && _ev[_u] >= _tgf;");
-                cg.addLine("if (!__any_sync(0xffffffffu, _tin)) continue;");
-                cg.addLine("gpudb_topk_warp_offer<" + K + ">(_tr_v, _tr_k, _tin ? _ev[_u] : GPUDB_TOPK_NONE_VAL, "
-                           "_tin ? _ek[_u] : GPUDB_TOPK_NONE_KEY);");
+                cg.addLine("const bool _tok = _ev[_u] >= _tgf && !(_ev[_u] == GPUDB_TOPK_NONE_VAL && "
+                           "_ek[_u] == GPUDB_TOPK_NONE_KEY);");
+                cg.addLine("if (__any_sync(0xffffffffu, _tok)) gpudb_topk_warp_merge_list<" + K +
+                           ">(_tr_v, _tr_k, _ev[_u], _ek[_u]);");
             });
         });
-        // this block's own floor stays valid: its K entries are among those offered
         blockMerge();
         cg.addBlock("if (threadIdx.x < 32u)", [&]() {
             cg.addLine("const bool _tf = _tl < " + K + " && !(_tr_k == GPUDB_TOPK_NONE_KEY && _tr_v == GPUDB_TOPK_NONE_VAL);");
