@@ -71,6 +71,22 @@ void CudaGenericExecutor::clearGraphs() {
         if (g.graph) cudaGraphDestroy(g.graph);
     }
     graphs_.clear();
+    graphOrder_.clear();
+    seenOnce_.clear();
+}
+
+void CudaGenericExecutor::evictOldestGraph() {
+    while (!graphOrder_.empty()) {
+        auto g = graphs_.find(graphOrder_.front());
+        graphOrder_.pop_front();
+        if (g == graphs_.end()) continue;
+        // a deferred replay of it may still be running on the stream
+        if (pendingErr_ && stream_) cudaStreamSynchronize(stream_);
+        if (g->second.exec) cudaGraphExecDestroy(g->second.exec);
+        if (g->second.graph) cudaGraphDestroy(g->second.graph);
+        graphs_.erase(g);
+        return;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -477,6 +493,7 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
         return -5;
     }
     const int total = warmup + measured;
+    std::map<std::string, GraphEntry>::iterator it = graphs_.end();
     if (useGraphs_) {
         // the load id: a graph captured from a module that was unloaded and
         // loaded again (same source key) must never be replayed
@@ -487,11 +504,18 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
             for (auto s : l.slots) key += "," + std::to_string(s);
         }
         for (const auto& f : fills) key += ";" + std::to_string((uintptr_t)f.ptr) + "/" + std::to_string(f.bytes);
-        auto it = graphs_.find(key);
-        if (it == graphs_.end()) {
-            // graphs of argument sets that no longer occur (columns
-            // registered elsewhere since) are dropped in bulk
-            if (graphs_.size() >= kMaxGraphs) clearGraphs();
+        it = graphs_.find(key);
+        // A launch sequence met for the first time runs eagerly, unless this
+        // call repeats it: a query run once (its constants are launch
+        // arguments) never pays for a capture or holds a cache entry.
+        if (it == graphs_.end() && total == 1 && seenOnce_.count(key) == 0) {
+            if (seenOnce_.size() >= kMaxSeen) seenOnce_.clear();
+            seenOnce_.insert(key);
+        } else if (it == graphs_.end()) {
+            seenOnce_.erase(key);
+            // the oldest graph makes room: argument sets that no longer
+            // occur (columns registered elsewhere since) age out
+            if (graphs_.size() >= kMaxGraphs) evictOldestGraph();
             GraphEntry g;
             if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 error = "cudaStreamBeginCapture failed";
@@ -510,7 +534,10 @@ int CudaGenericExecutor::execute(const RuntimeCompiler::CompiledQuery& cq,
                 return -6;
             }
             it = graphs_.emplace(key, g).first;
+            graphOrder_.push_back(key);
         }
+    }
+    if (it != graphs_.end()) {
         for (int iter = 0; iter < total; iter++) {
             const bool timed = iter >= warmup;
             if (timed) cudaEventRecord(events_[2 * nl], stream_);

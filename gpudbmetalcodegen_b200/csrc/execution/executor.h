@@ -19,10 +19,12 @@
 // ===================================================================
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <map>
 #include <memory>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../core/cuda_codegen.h"
@@ -167,12 +169,16 @@ private:
         cudaGraphExec_t exec = nullptr;
     };
     std::map<std::string, GraphEntry> graphs_;
+    std::deque<std::string> graphOrder_;          // graph keys in capture order, oldest first
+    std::unordered_set<std::string> seenOnce_;    // keys run once, eagerly, not captured yet
+    static constexpr size_t kMaxSeen = 4096;
 
     void ensureEvents(size_t n);
     bool allocateBuffers(const CudaCodegen::PhaseInfo& phase, std::string& error);
     bool buildLaunch(const RuntimeCompiler::CompiledQuery& cq, const CudaCodegen::PhaseInfo& phase, Launch& l,
                      std::string& error);
     void clearGraphs();
+    void evictOldestGraph();
 };
 
 }  // namespace gpudb

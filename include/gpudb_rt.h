@@ -190,7 +190,11 @@ int gpudb_execute(gpudb_ctx* ctx, gpudb_module* m, const gpudb_phase_desc* phase
                   int warmup, int measured, gpudb_timing* timing);
 /* setSkipZeroInit (metal_generic_executor.h:105). */
 int gpudb_set_skip_zero_init(gpudb_ctx* ctx, int skip);
-/* Replay whole iterations as CUDA graphs (captured on first use). */
+/* Replay whole iterations as CUDA graphs. A launch sequence (kernels,
+ * grids, arguments, fills) is captured when it recurs: on its second run,
+ * or at once when one call repeats it (warmup + measured > 1); its first
+ * single run is eager. A context keeps 512 graphs, the oldest dropped
+ * first. */
 int gpudb_set_use_graphs(gpudb_ctx* ctx, int on);
 
 /* ---- results / lifetime (reference: getAllocatedBuffer /

@@ -137,6 +137,27 @@ def test_batch_equals_plain_path(ctx, tables):
     r.close()
 
 
+def test_graph_cache_captures_recurring_runs_and_ages_out(ctx, tables):
+    """Graphs on, 400 plain queries whose constants are launch arguments,
+    each run twice: a launch sequence's first run is eager, its second is
+    captured and replayed, and past the 512 graphs a context keeps the
+    oldest ones are dropped (the third pass re-runs early queries whose
+    graphs aged out). Every answer equals the eager run's and, on a
+    subset, the oracle's."""
+    qs = mixed(tables, 400, seed=41)
+    plain = B.PlainRunner(ctx, tables)
+    ctx.set_use_graphs(True)
+    try:
+        first = [plain.run(q) for q in qs]
+        second = [plain.run(q) for q in qs]
+        third = [plain.run(q) for q in qs[:40]]
+    finally:
+        ctx.set_use_graphs(False)
+    assert_all_equal(second, first, qs)
+    assert_all_equal(third, first[:40], qs[:40])
+    assert_all_equal(first[:40], [oracle_result(tables, q) for q in qs[:40]], qs[:40])
+
+
 # ---------------------------------------------------------------------------
 # the sizer network
 # ---------------------------------------------------------------------------
