@@ -1,5 +1,6 @@
 #include "executor.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <stdexcept>
@@ -109,7 +110,7 @@ void CudaGenericExecutor::registerTableBuffer(const std::string& column, const v
 void CudaGenericExecutor::registerAllocatedBuffer(const std::string& name, void* dptr, size_t bytes, size_t elemBytes) {
     auto it = buffers_.find(name);
     if (it != buffers_.end() && it->second.owned && it->second.ptr) cudaFree(it->second.ptr);
-    buffers_[name] = {dptr, bytes, elemBytes ? elemBytes : 1, false};
+    buffers_[name] = {dptr, bytes, elemBytes ? elemBytes : 1, false, bytes};
     clearGraphs();
 }
 
@@ -208,22 +209,34 @@ bool CudaGenericExecutor::allocateBuffers(const CudaCodegen::PhaseInfo& phase, s
         const size_t bytes = (size_t)(count ? count : 1) * elem;
         auto it = buffers_.find(b.name);
         if (it != buffers_.end() && !it->second.owned) continue;  // caller-provided buffer
-        if (it != buffers_.end() && it->second.ptr && it->second.bytes >= bytes && it->second.elemBytes == elem) {
-            // reuse the allocation; remember the logical size for length params / fills
+        if (it != buffers_.end() && it->second.ptr && it->second.capacity >= bytes && it->second.elemBytes == elem) {
+            // reuse the allocation (its capacity stays); remember the
+            // logical size for length params / fills
             it->second.bytes = bytes;
             continue;
         }
+        // a buffer that has to grow again gets a quarter of headroom, so
+        // sizes that creep upward do not free and allocate on every run
+        size_t cap = bytes;
         if (it != buffers_.end() && it->second.ptr) {
+            if (it->second.elemBytes == elem) cap = std::max(bytes, it->second.capacity + it->second.capacity / 4);
             cudaStreamSynchronize(stream_);
             cudaFree(it->second.ptr);
+            it->second.ptr = nullptr;
         }
         void* p = nullptr;
-        const cudaError_t e = cudaMalloc(&p, bytes);
+        cudaError_t e = cudaMalloc(&p, cap);
+        if (e != cudaSuccess && cap > bytes) {
+            cudaGetLastError();  // the headroom did not fit: the exact size may
+            cap = bytes;
+            e = cudaMalloc(&p, cap);
+        }
         if (e != cudaSuccess) {
+            buffers_.erase(b.name);
             error = "cudaMalloc(" + std::to_string(bytes) + " B) for '" + b.name + "': " + cudaGetErrorString(e);
             return false;
         }
-        buffers_[b.name] = {p, bytes, elem, true};
+        buffers_[b.name] = {p, bytes, elem, true, cap};
         clearGraphs();
     }
     return true;

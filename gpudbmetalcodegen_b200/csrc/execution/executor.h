@@ -119,9 +119,10 @@ public:
 private:
     struct Buffer {
         void* ptr = nullptr;
-        size_t bytes = 0;
+        size_t bytes = 0;     // logical size of the current run (length params, fills, reads)
         size_t elemBytes = 1;
         bool owned = false;
+        size_t capacity = 0;  // bytes allocated; reused while a run's size fits
     };
     struct Column {
         const void* ptr = nullptr;

@@ -137,6 +137,31 @@ def test_batch_equals_plain_path(ctx, tables):
     r.close()
 
 
+def test_plain_path_buffers_keep_their_allocation(ctx, tables):
+    """The plain path sizes its group table per query. A large query, a
+    small one, then one in between: the later two reuse the first
+    allocation (its capacity is kept apart from each run's logical size, so
+    a smaller run does not make the next larger one free and allocate
+    again), the logical sizes follow the queries, and every answer equals
+    the oracle's."""
+    import ctypes as C
+    from gpudbmetalcodegen_b200 import _lib
+    lib = _lib.load()
+    plain = B.PlainRunner(ctx, tables)
+    qs = [B.MixQuery("groupby", 0, 0, tables.rows, 10_000, card=1 << 20),
+          B.MixQuery("groupby", 0, 5, 100_000, 10_000, card=1 << 20),
+          B.MixQuery("groupby", 0, 7, 1_000_000, 10_000, card=1 << 20)]
+    got, bufs = [], []
+    for q in qs:
+        got.append(plain.run(q))
+        p, n = C.c_void_p(), C.c_uint64()
+        assert lib.gpudb_buffer_ptr(ctx.handle, b"mg_keys", C.byref(p), C.byref(n)) == 0
+        bufs.append((p.value, n.value))
+    assert bufs[1][0] == bufs[0][0] and bufs[2][0] == bufs[0][0]
+    assert bufs[1][1] < bufs[2][1] <= bufs[0][1]
+    assert_all_equal(got, [oracle_result(tables, q) for q in qs], qs)
+
+
 def test_graph_cache_captures_recurring_runs_and_ages_out(ctx, tables):
     """Graphs on, 400 plain queries whose constants are launch arguments,
     each run twice: a launch sequence's first run is eager, its second is
