@@ -861,6 +861,52 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
             with torch.cuda.stream(stream):
                 scratch[0].zero_()
                 scratch[1].view(torch.int64).sum()
+    rot, bind = None, None
+    if flush:
+        # inputs under twice the L2: three device copies of every column,
+        # rotated from step to step, so each step reads a copy that the
+        # other two (at least twice the L2) evicted, launches still back to
+        # back (each copy's plan is its own cached graph)
+        lib = _lib.load()
+        rot, held = [], []
+        for _ in range(3):
+            binds = []
+            for tname, table in w.tables.items():
+                for cname, arr in table.items():
+                    t = torch.from_numpy(np.ascontiguousarray(arr)).to(f"cuda:{local}")
+                    held.append(t)
+                    binds.append((tname.encode(), cname.encode(), C.c_void_p(t.data_ptr()), arr.shape[0],
+                                  arr.itemsize))
+            rot.append(binds)
+
+        def bind(k):
+            for tb, cb, ptr, n, e in rot[k]:
+                lib.gpudb_register_column(ctx.handle, tb, cb, ptr, n, e)
+
+    def rotated_step_ms(qq, steps: int = 30) -> float:
+        # a candidate's step as the timed region below measures it: graph
+        # replays back to back over the rotated copies (single flushed
+        # launches also time each launch's start-up, and rank tiles
+        # differently)
+        ctx.set_use_graphs(not args.no_graphs)
+        try:
+            for i in range(6):
+                bind(i % 3)
+                ctx.enqueue(qq)
+            ctx.sync()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for i in range(steps):
+                bind(i % 3)
+                ctx.enqueue(qq)
+            b.record(stream)
+            b.synchronize()
+            ctx.sync()
+            return a.elapsed_time(b) / steps
+        finally:
+            ctx.set_use_graphs(False)
+
     tuner = None
     tune = args.tune
     if tune == "auto":
@@ -878,7 +924,7 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
             t0 = time.perf_counter()
             tlog = []
             autotune.tune_query(ctx, w.spec, rows, cache=cache, log=tlog, rounds=0 if not args.tune_search else 2,
-                                flush=flush_l2 if flush else None)
+                                flush=flush_l2 if flush else None, timer=rotated_step_ms if flush else None)
             tuner = {"tuned_s": time.perf_counter() - t0, "candidates": len(tlog) + 1,
                      "mode": "search" if args.tune_search else "seeds"}
         e = cache.data.get(cache.key(tpl, rows), {})
@@ -908,28 +954,7 @@ def measure(args, w: Workload, pg, world: int, rank: int, local: int):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
 
-    rot = None
-    if flush:
-        # inputs under twice the L2: three device copies of every column,
-        # rotated from step to step, so each step reads a copy that the
-        # other two (at least twice the L2) evicted, launches still back to
-        # back (each copy's plan is its own cached graph)
-        lib = _lib.load()
-        rot, held = [], []
-        for _ in range(3):
-            binds = []
-            for tname, table in w.tables.items():
-                for cname, arr in table.items():
-                    t = torch.from_numpy(np.ascontiguousarray(arr)).to(f"cuda:{local}")
-                    held.append(t)
-                    binds.append((tname.encode(), cname.encode(), C.c_void_p(t.data_ptr()), arr.shape[0],
-                                  arr.itemsize))
-            rot.append(binds)
-
-        def bind(k):
-            for tb, cb, ptr, n, e in rot[k]:
-                lib.gpudb_register_column(ctx.handle, tb, cb, ptr, n, e)
-
+    if rot:
         # each copy's launch sequence twice: a graph is captured when its
         # sequence recurs, so all three are captured before the timed steps
         for i in range(max(6, args.warmup)):

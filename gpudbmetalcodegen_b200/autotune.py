@@ -205,12 +205,17 @@ def coordinate_descent(space: Dict[str, Sequence], measure: Callable[[dict], Opt
 
 def tune_query(ctx, spec: str, rows: int, template: Optional[str] = None, space: Optional[dict] = None,
                reps: int = 10, warmup: int = 3, rounds: int = 2, cache: Optional[TuneCache] = None,
-               log: Optional[List[dict]] = None, flush: Optional[Callable[[], None]] = None) -> Tuple[str, float, float]:
+               log: Optional[List[dict]] = None, flush: Optional[Callable[[], None]] = None,
+               timer: Optional[Callable[[object], float]] = None) -> Tuple[str, float, float]:
     """Tune one plan on the tables registered in `ctx`; returns (tune
     string, best ms, default ms) and stores the winner in `cache`. With
     `flush` (which must order its work before the context's next run, e.g.
     on the context's stream), it runs before every timed repetition: inputs
-    that L2 could partly hold are then timed from DRAM, as in the bench."""
+    that L2 could partly hold are then timed from DRAM, as in the bench.
+    With `timer(query) -> ms`, each candidate whose answer matched is timed
+    by it instead: the caller's own regime (e.g. back-to-back launches over
+    rotated input copies), whose ranking of candidates can differ from
+    single launches'."""
     from .engine import GpudbError
 
     template = template or dict(kv.split("=", 1) for kv in spec.split(";") if "=" in kv).get("template", spec)
@@ -229,6 +234,8 @@ def tune_query(ctx, spec: str, rows: int, template: Optional[str] = None, space:
                 ref["r"] = canon(res)
             elif canon(res) != ref["r"]:
                 return None  # a tuning may never change an answer
+            if timer is not None:
+                return timer(q)
             for _ in range(warmup):
                 ctx.run(q, collect=False)
             ts = []
