@@ -51,6 +51,10 @@ struct ScanConfig {
     int prefetchRows = 0;  // rows whose probe bitmap words are loaded ahead (0 = off)
     int vectorRows = 0;    // consecutive rows per consumer thread, loaded with wide shared loads (0/1 = off)
     int l2Prefetch = 0;    // tiles beyond the ring the producer prefetches into L2 (0 = off)
+    // automatic tiles rounded down to whole rounds of the consumer threads:
+    // for consumers whose per-row work (lookups, atomics) makes a stage wait
+    // on its slowest warp; a pure streaming reduction keeps the fuller tile
+    bool wholeRounds = false;
 };
 
 // ------------------------------------------------------------------

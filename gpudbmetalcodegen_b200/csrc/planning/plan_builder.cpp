@@ -320,6 +320,9 @@ CudaQueryPlan buildJoinAgg(const JoinAggParts& jp, const TuneConfig& tune) {
         // the collector can read every slot (the device-sized table only
         // initialises the slots it uses)
         if (k <= 0) t.splitJoin = false;
+        // the split plan's build and probe consumers set bits and look them
+        // up per row: their automatic tiles hold whole consumer rounds
+        if (t.splitJoin) t.scan.wholeRounds = true;
         return t;
     }();
     {
