@@ -1,4 +1,6 @@
 """The autotuner's search and cache (no GPU)."""
+import collections
+
 from gpudbmetalcodegen_b200 import autotune as A
 
 
@@ -91,3 +93,78 @@ def test_replicas_writing_the_cache_at_once_leave_a_valid_file(tmp_path):
     for i in range(4):
         assert data[A.TuneCache.key(f"own{i}", 1000)]["tune"] == f"bs={32 * (i + 1)}"
     assert not list(tmp_path.glob("*.tmp"))
+
+
+# ---------------------------------------------------------------------------
+# tune_query against a fake context: with a caller's `timer` (the bench hands
+# it one that runs each candidate back to back over rotated input copies) the
+# timer ranks the candidates, each runs once to check its answer and never
+# for timing, and one whose answer differs from the default's is dropped
+# however fast its timer says it is
+# ---------------------------------------------------------------------------
+class FakeQuery:
+    def __init__(self, tune):
+        self.tune = tune
+
+
+class FakeResult:
+    def __init__(self, rows):
+        self.types = ["int64"]
+        self.rows = rows
+
+
+class FakeTiming:
+    def __init__(self, ms):
+        self.phase_ms = [ms]
+
+
+class FakeContext:
+    """Answers [[7]] ([[8]] for the tunes in `wrong`); each run's single
+    phase takes `run_ms[tune]` ms (1 ms when absent)."""
+
+    def __init__(self, wrong=(), run_ms=None):
+        self.wrong = set(wrong)
+        self.run_ms = run_ms or {}
+        self.runs = collections.Counter()
+
+    def prepare(self, spec, tune):
+        return FakeQuery(tune)
+
+    def run(self, q, collect=True, **kw):
+        self.runs[q.tune] += 1
+        return FakeResult([[8]] if q.tune in self.wrong else [[7]]), FakeTiming(self.run_ms.get(q.tune, 1.0))
+
+
+def test_timer_ranks_candidates_and_answers_still_gate_them():
+    space = {"bs": ["512", "256"], "tile": ["0", "448", "512"]}
+    # coordinate descent: bs first (256 beats 512 by more than its 2 %
+    # margin), then the tile at bs=256
+    times = {"bs=512;tile=0": 31.0, "bs=256;tile=0": 29.9, "bs=512;tile=448": 33.0, "bs=512;tile=512": 32.0,
+             "bs=256;tile=448": 29.0, "bs=256;tile=512": 20.0}
+    ctx = FakeContext(wrong={"bs=256;tile=512"})
+    timed = []
+
+    def timer(q):
+        timed.append(q.tune)
+        return times[q.tune]
+
+    tune, best, default = A.tune_query(ctx, "template=fake_scan", 1000, space=space, rounds=2, timer=timer)
+    # the fastest candidate returned a different answer: dropped, never timed
+    assert "bs=256;tile=512" not in timed
+    assert tune == "bs=256;tile=448" and best == 29.0 and default == 31.0
+    # with a timer, every candidate but the default (which also warms the
+    # clocks) runs exactly once: the answer check
+    assert all(n == 1 for t, n in ctx.runs.items() if t != "bs=512;tile=0")
+
+
+def test_without_a_timer_candidates_are_timed_by_their_own_runs():
+    space = {"bs": ["512", "256", "128"]}
+    ctx = FakeContext(run_ms={"bs=512": 2.0, "bs=256": 1.5, "bs=128": 1.0})
+    flushes = []
+    tune, best, default = A.tune_query(ctx, "template=fake_scan", 1000, space=space, rounds=1, reps=3,
+                                       warmup=2, flush=lambda: flushes.append(1))
+    assert (tune, best, default) == ("bs=128", 1.0, 2.0)
+    # a non-default candidate: the answer check, 2 warm-ups, 3 timed runs,
+    # each timed run after a flush
+    assert ctx.runs["bs=256"] == ctx.runs["bs=128"] == 6
+    assert len(flushes) == 3 * 3
