@@ -162,3 +162,21 @@ def test_warm_tier_adds_a_flush_phase():
     assert "zg_wkeys  [65536]  fill=255" in q.plan
     with pytest.raises(GpudbError):
         engine.Query("template=groupby", "warm=4")
+
+
+def _tiles(q):
+    import re
+    return {t: int(n) for t, n in re.findall(r"scan of (\w+): (\d+)-row tiles", q.source)}
+
+
+def test_split_join_tiles_hold_whole_consumer_rounds():
+    """The split join's automatic scan tiles are whole rounds of its consumer
+    threads (the block minus the producer warp, times the rows each takes
+    per round), so no warp takes an extra round per tile; a streaming
+    reduction keeps its power-of-two tile, and an explicit tile is kept."""
+    assert _tiles(engine.Query("template=join_topk", "bs=512;tile=0;split=1;bvec=4")) == {"dim": 1920, "probe": 1920}
+    t = _tiles(engine.Query("template=join_topk", "bs=256;tile=0;split=1;bvec=2"))
+    assert t["dim"] % (224 * 2) == 0 and t["probe"] % 224 == 0 and t["dim"] % 16 == 0
+    assert _tiles(engine.Query("template=q6", "bs=256;tile=0")) == {"fact": 1024}
+    assert _tiles(engine.Query("template=join_topk", "bs=512;tile=2048;split=1;bvec=4")) == {"dim": 2048, "probe": 2048}
+    assert _tiles(engine.Query("template=join_topk", "bs=512;tile=0;split=0")) == {"dim": 2048, "probe": 2048}
